@@ -1,0 +1,170 @@
+/*
+ * rtm3d_b200.h -- C ABI of librtm3d_b200.so, the B200 (sm_100a) time-stepping library for
+ * 3D acoustic seismic modeling and reverse-time migration.
+ *
+ * The library replaces the GPU back-end of sc4ii-cimatec/rtm3d-demo (paths below are relative
+ * to its source/rtm-3d/ directory):
+ *   - the per-step operators of the platform interface RTMPlatform (include/RTMPlatform.hpp:28-102)
+ *     and their CUDA wrappers (kernel/gpu/rtmgpu.hpp:8-65), and
+ *   - the per-shot time loops of the kernel classes: RTMFiniteDifferencesKernel::rtmModel
+ *     (src/kernel/RTMFiniteDifferencesKernel.cpp:103-246), RTMHBCKernel::rtmMigrate
+ *     (src/kernel/RTMFiniteDifferencesKernel_HBC.cpp:64-364) and RTMRBCKernel::rtmMigrate
+ *     (src/kernel/RTMFiniteDifferencesKernel_RBC.cpp:36-274).
+ *
+ * Conventions
+ *   - Volumes are FP32, padded by blen cells on every face: (nx+2*blen, ny+2*blen, nz+2*blen),
+ *     x slowest, z fastest, offset = (x*nye + y)*nze + z (include/RTMGrid.hpp:217-221).
+ *   - Source and receiver coordinates are in the UNPADDED model, as in input.json.
+ *   - A shot record is held in the reference's file layout: nt/ntstep chunks, each chunk
+ *     [receiver_count_x][receiver_count_y][ntstep] with time fastest -- exactly the
+ *     concatenation of the .seism files (include/RTMBase.hpp:131-138).
+ *   - Per-operator entry points take caller-owned DEVICE pointers (the reference's
+ *     GPUDeviceGrid ownership, src/grid/RTMGPUDeviceGrid.cpp:14-57) and are asynchronous on the
+ *     context's stream; they never synchronise the device (the reference syncs after every
+ *     launch, src/platform/gpu/RTMGPUPlatform.cpp:193-194).  *_host driver entry points take
+ *     host pointers and return after the result is in host memory.
+ *   - Every function returns an rtmb_status.  Nothing calls exit() or abort() (the reference's
+ *     CUDACHECK exits, include/RTMGPU.hpp:18-33); rtmb_last_error() describes the last failure.
+ *   - A context is bound to one device and is not thread-safe; separate contexts are.
+ */
+#ifndef RTM3D_B200_H
+#define RTM3D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RTMB_ABI_VERSION 1
+
+typedef enum rtmb_status {
+    RTMB_OK = 0,
+    RTMB_EINVAL = 1,   /* bad argument or parameter combination */
+    RTMB_ENOMEM = 2,   /* device or host allocation failed */
+    RTMB_ECUDA = 3,    /* a CUDA runtime call failed */
+    RTMB_ENAN = 4,     /* a NaN appeared in a wavefield ("Numerical Dispersion" in the reference) */
+    RTMB_ETIMEOUT = 5, /* a bounded device-side wait ran out */
+    RTMB_EIO = 6       /* a file could not be read or written */
+} rtmb_status;
+
+/* Boundary handling of a migration (getRTMBoundaryCondition, include/RTMGrid.hpp:27-57). */
+typedef enum rtmb_boundary { RTMB_BC_ABC = 1, RTMB_BC_HBC = 2, RTMB_BC_RBC = 3 } rtmb_boundary;
+
+/* Flags for rtmb_params.flags. */
+#define RTMB_FLAG_FAST_FMA      0x1u  /* contract stencil arithmetic into FMA; not bit-exact with the
+                                         reference CPU path (rel-L2 ~1e-7/step) */
+#define RTMB_FLAG_RCV_ADD       0x2u  /* backward receiver injection ADDS (reference GPU kernel,
+                                         kernel/gpu/rtmgpu_finitediff.cu:403) instead of overwriting
+                                         (reference CPU path, RTMCPUPlatform.cpp:127) */
+#define RTMB_FLAG_IMG_FULL_Z    0x4u  /* imaging covers every z (reference GPU kernel, .cu:440-458)
+                                         instead of z in [blen, nze-blen) (CPU, RTMCPUPlatform.cpp:532) */
+#define RTMB_FLAG_NO_TAPER_QUIRK 0x8u /* taper the front-right x-y edge from its own cells instead of
+                                         from x = blen (RTMCPUPlatform.cpp:901) */
+#define RTMB_FLAG_USE_GRAPH     0x10u /* capture each time loop in a CUDA graph */
+#define RTMB_FLAG_NO_TMA        0x20u /* use the plain-load step kernel even when rows are 16-byte
+                                         aligned (the TMA-pipelined kernel is the default then) */
+
+/* The input.json parameters on the path (include/RTMParam.hpp:188-249). */
+typedef struct rtmb_params {
+    uint32_t nx, ny, nz;          /* unpadded model size */
+    uint32_t blen;                /* border cells on every face */
+    uint32_t nt, ntstep;          /* time steps; record chunk length (nt % ntstep == 0) */
+    uint32_t stencil_order;       /* even, 2..16 */
+    float dx, dy, dz, dt;
+    float fpeak;                  /* Ricker peak frequency */
+    float taper_factor;
+    uint32_t receiver_start_x, receiver_start_y, receiver_depth_z;
+    uint32_t receiver_distance_x, receiver_distance_y;
+    uint32_t receiver_count_x, receiver_count_y;
+    int32_t boundary;             /* rtmb_boundary, used by the migration drivers */
+    uint32_t flags;               /* RTMB_FLAG_* */
+    int32_t device;               /* CUDA device ordinal; -1 = current device */
+} rtmb_params;
+
+typedef struct rtmb_ctx rtmb_ctx;
+
+/* ------------------------------------------------------------------ context */
+/* Replaces RTMGPUPlatform::initRTMPlatform (src/platform/gpu/RTMGPUPlatform.cpp:22-57) without its
+ * cudaDeviceReset; allocates the stencil, taper and Ricker tables on the device. */
+int rtmb_create(const rtmb_params *params, rtmb_ctx **out);
+/* Replaces RTMGPUPlatform::destroyRTMPlatform (:16-21); frees every context-owned buffer. */
+int rtmb_destroy(rtmb_ctx *ctx);
+const char *rtmb_last_error(const rtmb_ctx *ctx);
+/* Run subsequent work on this cudaStream_t (NULL = the context's own stream). */
+int rtmb_set_stream(rtmb_ctx *ctx, void *cuda_stream);
+int rtmb_sync(rtmb_ctx *ctx);
+int rtmb_abi_version(void);
+/* Count of this library's kernel launches since the context was created. */
+uint64_t rtmb_launch_count(const rtmb_ctx *ctx);
+
+/* ------------------------------------------------------------------ host-side tables
+ * Bit-identical to the reference's host computations; usable without a GPU. */
+/* RTMStencil::setStencilCoefficients (include/RTMGrid.hpp:433-446) with laplacian_coefs / makeo2
+ * (src/misc/Misc.cpp:106-176).  out: [3][order+1] for x, y, z. */
+int rtmb_stencil_coefs(uint32_t order, float dx, float dy, float dz, float *out);
+/* RTMTaperFunction::inittaper (include/RTMSeismic.hpp:294-305).  out: blen floats. */
+int rtmb_taper_vector(uint32_t blen, float taper_factor, float *out);
+/* RTMSeismicSource::loadSamples / ricker (include/RTMSeismic.hpp:135-144, 191-198). */
+int rtmb_ricker(uint32_t nt, float dt, float fpeak, float *out);
+/* RTMCube::extendBorders + initBorders (src/grid/RTMGrid.cpp:47-86, 371-714) on the host.
+ * bc: 0 none (border left zero), RTMB_BC_ABC, RTMB_BC_HBC, RTMB_BC_RBC.  The random border uses
+ * libc rand() in the reference's single-thread order after srand(seed); seed < 0 skips srand. */
+int rtmb_prepare_velocity(const float *v, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t blen,
+                          int32_t bc, int64_t seed, float *ve);
+/* Grid::power2 then multiplyBy(dt*dt) (src/controller/RTMController.cpp:110-111), in place. */
+int rtmb_v2dt2_host(float *ve, size_t n, float dt);
+
+/* ------------------------------------------------------------------ per-step operators
+ * Device pointers, padded volumes sized by the context's parameters. */
+/* RTMPlatform::rtmStep (include/RTMPlatform.hpp:50-51), RTMSTEP_WRAPPER (kernel/gpu/rtmgpu.hpp:8-11):
+ * PP <- 2P - PP + v2dt2 * lap(P) on [h, n-h)^3, h = order/2; PP updated in place. */
+int rtmb_step(rtmb_ctx *ctx, const float *P, float *PP, const float *v2dt2);
+/* RTMPlatform::rtmTaperAllBorders / rtmTaperUpperBorders (RTMPlatform.hpp:35-42),
+ * RTMTAPER_WRAPPER (rtmgpu.hpp:27-30); CPU taper semantics (RTMCPUPlatform.cpp:566-920). */
+int rtmb_taper_all_borders(rtmb_ctx *ctx, float *P);
+int rtmb_taper_upper_borders(rtmb_ctx *ctx, float *P);
+/* RTMPlatform::rtmApplySource (RTMPlatform.hpp:70), RTMSOURCE_WRAPPER (rtmgpu.hpp:21-25):
+ * PP[sx+b, sy+b, sz+b] += wavelet[it] (the context's Ricker table). */
+int rtmb_apply_source(rtmb_ctx *ctx, float *PP, uint32_t sx, uint32_t sy, uint32_t sz, uint32_t it);
+/* RTMPlatform::rtmSaveReceiverData / rtmRestoreReceiverData (RTMPlatform.hpp:75-80),
+ * RTMSEISM_WRAPPER (rtmgpu.hpp:13-19).  rec: one chunk [rcx][rcy][ntstep]; lt < ntstep. */
+int rtmb_save_receiver_data(rtmb_ctx *ctx, const float *PP, float *rec, uint32_t lt);
+int rtmb_restore_receiver_data(rtmb_ctx *ctx, float *PP, const float *rec, uint32_t lt);
+/* RTMPlatform::rtmSaveUpperBorder / rtmRestoreUpperBorder (RTMPlatform.hpp:85-90),
+ * RTMWUPB_WRAPPER (rtmgpu.hpp:32-33).  upb: [ntstep][nxe][nye][order/2], 64-bit offsets. */
+int rtmb_save_upper_border(rtmb_ctx *ctx, const float *P, float *upb, uint32_t lt);
+int rtmb_restore_upper_border(rtmb_ctx *ctx, float *P, const float *upb, uint32_t lt);
+/* RTMPlatform::rtmImageCondition (RTMPlatform.hpp:65), RTMIMG_WRAPPER (rtmgpu.hpp:35-37):
+ * IMG += PS * PR. */
+int rtmb_image_condition(rtmb_ctx *ctx, float *img, const float *ps, const float *pr);
+/* Image finalisation of the controller (src/controller/RTMAcousticController.cpp:244-249):
+ * order-2 Laplacian filter (src/grid/RTMGrid.cpp:226-300) then removeBorders (:129-166).
+ * img: padded device volume; out: nx*ny*nz device volume. */
+int rtmb_image_finalize(rtmb_ctx *ctx, const float *img, float *out);
+/* RTMCube::stack / stackRegion over the whole cube (src/grid/RTMGrid.cpp:168-223): acc += img. */
+int rtmb_image_stack(rtmb_ctx *ctx, float *acc, const float *img);
+
+/* ------------------------------------------------------------------ per-shot drivers
+ * The extended squared-slowness-times-dt^2 volume (v2dt2, padded) must be loaded first.
+ * (sx, sy, sz) is the shot position in the unpadded model (RTMController.cpp:145-147). */
+int rtmb_load_v2dt2(rtmb_ctx *ctx, const float *v2dt2, int from_host);
+/* RTMFiniteDifferencesKernel::rtmModel: taper every face, step, inject, sample receivers.
+ * rec: record in file layout (nt*rcx*rcy floats), device pointer. */
+int rtmb_model_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, float *rec);
+/* RTMHBCKernel::rtmMigrate / RTMRBCKernel::rtmMigrate (by params.boundary): forward pass, then the
+ * backward pass rebuilding the source wavefield and cross-correlating it with the back-propagated
+ * receiver wavefield.  rec: record in file layout (device); img: padded per-shot image (device),
+ * overwritten (the reference's shotImage). */
+int rtmb_migrate_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const float *rec,
+                      float *img);
+/* Host-buffer forms: copy in, run, copy out, return when the result is on the host. */
+int rtmb_model_shot_host(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, float *rec_host);
+int rtmb_migrate_shot_host(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz,
+                           const float *rec_host, float *img_host);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RTM3D_B200_H */

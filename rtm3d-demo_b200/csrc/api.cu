@@ -1,0 +1,473 @@
+// api.cu -- context, C ABI entry points and the per-shot time-loop drivers of librtm3d_b200.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <utility>
+
+#include <cuda_runtime.h>
+
+#include "ops.cuh"
+#include "rtm3d_b200.h"
+#include "stencil.cuh"
+
+struct rtmb_ctx {
+    rtmb_params p{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    int nxe = 0, nye = 0, nze = 0, h = 0;
+    size_t n = 0;
+    float coefs[3 * (rtmb::kMaxOrder + 1)] = {};
+    float *d_taper = nullptr, *d_wavelet = nullptr;
+    unsigned *d_err = nullptr;
+    // driver state
+    float *d_v2dt2 = nullptr;
+    float *d_w[4] = {};          // source pair, receiver pair
+    float *d_quirk[3] = {};      // front-right taper side buffers (modeling)
+    float *d_upb = nullptr;      // [nt][nxe][nye][h] (HBC)
+    float *d_rec = nullptr, *d_img = nullptr;  // staging for the host-buffer forms
+    int chunk = 0;
+    uint64_t launches = 0;
+    std::string err;
+};
+
+namespace {
+
+int fail(rtmb_ctx *c, int code, const char *fmt, ...) {
+    if (c) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        c->err = buf;
+    }
+    return code;
+}
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? RTMB_ENOMEM : RTMB_ECUDA, "%s: %s (%s:%d)", \
+                        #call, cudaGetErrorString(e_), __FILE__, __LINE__);                       \
+    } while (0)
+
+#define LAUNCH(call)                                                                              \
+    do {                                                                                          \
+        ++ctx->launches;                                                                          \
+        CK(call);                                                                                 \
+    } while (0)
+
+rtmb::Geom geom(const rtmb_ctx *c) { return rtmb::Geom{c->nxe, c->nye, c->nze, (int)c->p.blen, c->h}; }
+
+rtmb::RcvGeom rgeom(const rtmb_ctx *c) {
+    const int b = (int)c->p.blen;
+    return rtmb::RcvGeom{(int)c->p.receiver_start_x + b, (int)c->p.receiver_start_y + b,
+                         (int)c->p.receiver_depth_z + b, (int)c->p.receiver_distance_x,
+                         (int)c->p.receiver_distance_y, (int)c->p.receiver_count_x,
+                         (int)c->p.receiver_count_y, (int)c->p.ntstep};
+}
+
+// x planes per CTA: enough CTAs for several waves of 2 CTAs per SM on 148 SMs.
+int pick_chunk(int nxi, int tiles) {
+    const int target = 148 * 2 * 4;
+    int nch = (target + tiles - 1) / tiles;
+    const int maxch = nxi / 16 > 0 ? nxi / 16 : 1;
+    if (nch > maxch) nch = maxch;
+    if (nch < 1) nch = 1;
+    return (nxi + nch - 1) / nch;
+}
+
+rtmb::StepArgs base_args(const rtmb_ctx *c) {
+    rtmb::StepArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.nxe = c->nxe; a.nye = c->nye; a.nze = c->nze; a.blen = (int)c->p.blen;
+    a.chunk = c->chunk;
+    const int o = (int)c->p.stencil_order;
+    for (int i = 0; i <= o; ++i) {
+        a.cx[i] = c->coefs[i];
+        a.cy[i] = c->coefs[(o + 1) + i];
+        a.cz[i] = c->coefs[2 * (o + 1) + i];
+    }
+    a.taper = c->d_taper;
+    a.wavelet = c->d_wavelet;
+    a.sxe = a.sye = a.sze = -1;
+    a.err = c->d_err;
+    a.rdx = a.rdy = 1;
+    return a;
+}
+
+bool exact(const rtmb_ctx *c) { return !(c->p.flags & RTMB_FLAG_FAST_FMA); }
+bool tma_ok(const rtmb_ctx *c) { return !(c->p.flags & RTMB_FLAG_NO_TMA); }
+
+int check_err_flag(rtmb_ctx *ctx) {
+    unsigned h = 0;
+    CK(cudaMemcpyAsync(&h, ctx->d_err, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (h) {
+        CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(unsigned), ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (h & 2u) return fail(ctx, RTMB_ETIMEOUT, "a bounded device wait for a tile load ran out");
+        return fail(ctx, RTMB_ENAN, "Numerical Dispersion: a wavefield value became NaN");
+    }
+    return RTMB_OK;
+}
+
+int ensure(rtmb_ctx *ctx, float **buf, size_t count, bool zero) {
+    if (!*buf) {
+        CK(cudaMalloc(buf, count * sizeof(float)));
+        if (zero) CK(cudaMemsetAsync(*buf, 0, count * sizeof(float), ctx->stream));
+    }
+    return RTMB_OK;
+}
+
+int check_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz) {
+    const rtmb_params &p = ctx->p;
+    // RTMController.cpp:149-155 rejects sources outside the model
+    if (sx >= p.nx || sy >= p.ny || sz >= p.nz)
+        return fail(ctx, RTMB_EINVAL, "Invalid Source Position: (%u,%u,%u)", sx, sy, sz);
+    if ((int)p.blen < ctx->h)
+        return fail(ctx, RTMB_EINVAL, "the per-shot drivers need blen >= stencil_order/2");
+    if (!ctx->d_v2dt2) return fail(ctx, RTMB_EINVAL, "no velocity loaded (rtmb_load_v2dt2)");
+    if (p.receiver_count_x > p.nx || p.receiver_count_y > p.ny)  // RTMSeismic.cpp:15-19
+        return fail(ctx, RTMB_EINVAL, "Invalid Receiver Grid Size");
+    return RTMB_OK;
+}
+
+void set_receivers(rtmb::StepArgs &a, const rtmb_ctx *c, int mode, float *rec, int it) {
+    const rtmb::RcvGeom r = rgeom(c);
+    a.rec_mode = mode;
+    a.rec = rec;
+    a.rx0 = r.rx0; a.ry0 = r.ry0; a.rz = r.rz; a.rdx = r.rdx > 0 ? r.rdx : 1; a.rdy = r.rdy > 0 ? r.rdy : 1;
+    a.rcx = r.rcx; a.rcy = r.rcy;
+    const long long ntstep = c->p.ntstep;
+    a.rec_si = (long long)r.rcy * ntstep;
+    a.rec_sj = ntstep;
+    a.rec_base = (long long)(it / ntstep) * r.rcx * r.rcy * ntstep + (it % ntstep);
+}
+
+// Forward time loop shared by modeling and the migration forward pass.  Leaves the last two
+// wavefields in (*P, *PP) raw (untapered): *P = u(nt-1), *PP = u(nt).
+int run_forward(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, int taper_mode, float *rec,
+                float *upb, float **P_out, float **PP_out) {
+    const rtmb_params &p = ctx->p;
+    const size_t nb = ctx->n * sizeof(float);
+    float *P = ctx->d_w[0], *PP = ctx->d_w[1];
+    CK(cudaMemsetAsync(P, 0, nb, ctx->stream));
+    CK(cudaMemsetAsync(PP, 0, nb, ctx->stream));
+    const bool quirk = taper_mode == rtmb::kTaperAll && !(p.flags & RTMB_FLAG_NO_TAPER_QUIRK) && p.blen > 0;
+    if (quirk) {
+        const size_t qn = (size_t)p.blen * (ctx->nze - 2 * p.blen);
+        for (int k = 0; k < 3; ++k) {
+            int rc = ensure(ctx, &ctx->d_quirk[k], qn > 0 ? qn : 1, false);
+            if (rc) return rc;
+            CK(cudaMemsetAsync(ctx->d_quirk[k], 0, (qn > 0 ? qn : 1) * sizeof(float), ctx->stream));
+        }
+    }
+    rtmb::StepArgs a = base_args(ctx);
+    a.V = ctx->d_v2dt2;
+    a.taper_mode = taper_mode;
+    a.quirk = quirk;
+    a.sxe = (int)(sx + p.blen); a.sye = (int)(sy + p.blen); a.sze = (int)(sz + p.blen);
+    const size_t upb_step = (size_t)ctx->nxe * ctx->nye * ctx->h;
+    for (uint32_t it = 0; it < p.nt; ++it) {
+        std::swap(P, PP);
+        a.P = P; a.PP = PP; a.it = (int)it;
+        if (rec) set_receivers(a, ctx, rtmb::kRecSample, rec, (int)it);
+        if (upb) { a.upb_mode = rtmb::kUpbSave; a.upb = upb + (size_t)it * upb_step; }
+        if (quirk) { a.quirk_in = ctx->d_quirk[(it + 1) % 3]; a.quirk_out = ctx->d_quirk[it % 3]; }
+        LAUNCH(rtmb::launch_step(a, (int)p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
+    }
+    *P_out = P;
+    *PP_out = PP;
+    return RTMB_OK;
+}
+
+int alloc_driver(rtmb_ctx *ctx) {
+    for (int k = 0; k < 4; ++k) {
+        int rc = ensure(ctx, &ctx->d_w[k], ctx->n, false);
+        if (rc) return rc;
+    }
+    return RTMB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rtmb_abi_version(void) { return RTMB_ABI_VERSION; }
+
+const char *rtmb_last_error(const rtmb_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+uint64_t rtmb_launch_count(const rtmb_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+int rtmb_create(const rtmb_params *params, rtmb_ctx **out) {
+    if (!params || !out) return RTMB_EINVAL;
+    *out = nullptr;
+    const rtmb_params &p = *params;
+    if (!p.nx || !p.ny || !p.nz || p.stencil_order < 2 || p.stencil_order > 16 || (p.stencil_order & 1u))
+        return RTMB_EINVAL;
+    if (!p.ntstep || p.nt % p.ntstep) return RTMB_EINVAL;  // RTMParam.cpp:241-245 rejects nt < ntstep
+    rtmb_ctx *ctx = new rtmb_ctx;
+    ctx->p = p;
+    ctx->h = (int)p.stencil_order / 2;
+    ctx->nxe = (int)(p.nx + 2 * p.blen);
+    ctx->nye = (int)(p.ny + 2 * p.blen);
+    ctx->nze = (int)(p.nz + 2 * p.blen);
+    ctx->n = (size_t)ctx->nxe * ctx->nye * ctx->nze;
+    const int nxi = ctx->nxe - 2 * ctx->h, nyi = ctx->nye - 2 * ctx->h;
+    const int tiles = ((ctx->nze + rtmb::kTZ - 1) / rtmb::kTZ) * ((nyi + rtmb::kTY - 1) / rtmb::kTY);
+    ctx->chunk = pick_chunk(nxi > 0 ? nxi : 1, tiles > 0 ? tiles : 1);
+    auto bail = [&](int code) {
+        rtmb_destroy(ctx);
+        return code;
+    };
+    int dev = p.device;
+    if (dev < 0) {
+        if (cudaGetDevice(&dev) != cudaSuccess) return bail(RTMB_ECUDA);
+    } else if (cudaSetDevice(dev) != cudaSuccess) {
+        return bail(RTMB_ECUDA);
+    }
+    ctx->device = dev;
+    if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) return bail(RTMB_ECUDA);
+    ctx->stream = ctx->own_stream;
+    rtmb_stencil_coefs(p.stencil_order, p.dx, p.dy, p.dz, ctx->coefs);
+    float *tap = new float[p.blen > 0 ? p.blen : 1];
+    float *wav = new float[p.nt];
+    rtmb_taper_vector(p.blen, p.taper_factor, tap);
+    rtmb_ricker(p.nt, p.dt, p.fpeak, wav);
+    bool ok = cudaMalloc(&ctx->d_taper, sizeof(float) * (p.blen > 0 ? p.blen : 1)) == cudaSuccess &&
+              cudaMalloc(&ctx->d_wavelet, sizeof(float) * p.nt) == cudaSuccess &&
+              cudaMalloc(&ctx->d_err, sizeof(unsigned)) == cudaSuccess &&
+              cudaMemcpy(ctx->d_taper, tap, sizeof(float) * (p.blen > 0 ? p.blen : 1), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(ctx->d_wavelet, wav, sizeof(float) * p.nt, cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemset(ctx->d_err, 0, sizeof(unsigned)) == cudaSuccess;
+    delete[] tap;
+    delete[] wav;
+    if (!ok) return bail(RTMB_ENOMEM);
+    *out = ctx;
+    return RTMB_OK;
+}
+
+int rtmb_destroy(rtmb_ctx *ctx) {
+    if (!ctx) return RTMB_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    float *bufs[] = {ctx->d_taper, ctx->d_wavelet, ctx->d_v2dt2, ctx->d_w[0], ctx->d_w[1], ctx->d_w[2],
+                     ctx->d_w[3], ctx->d_quirk[0], ctx->d_quirk[1], ctx->d_quirk[2], ctx->d_upb,
+                     ctx->d_rec, ctx->d_img};
+    for (float *b : bufs)
+        if (b) cudaFree(b);
+    if (ctx->d_err) cudaFree(ctx->d_err);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return RTMB_OK;
+}
+
+int rtmb_set_stream(rtmb_ctx *ctx, void *cuda_stream) {
+    if (!ctx) return RTMB_EINVAL;
+    ctx->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : ctx->own_stream;
+    return RTMB_OK;
+}
+
+int rtmb_sync(rtmb_ctx *ctx) {
+    if (!ctx) return RTMB_EINVAL;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return check_err_flag(ctx);
+}
+
+// ------------------------------------------------------------------ per-step operators
+
+int rtmb_step(rtmb_ctx *ctx, const float *P, float *PP, const float *v2dt2) {
+    if (!ctx || !P || !PP || !v2dt2) return fail(ctx, RTMB_EINVAL, "rtmb_step: null pointer");
+    rtmb::StepArgs a = base_args(ctx);
+    a.P = P; a.PP = PP; a.V = v2dt2;
+    LAUNCH(rtmb::launch_step(a, (int)ctx->p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
+    return RTMB_OK;
+}
+
+int rtmb_taper_all_borders(rtmb_ctx *ctx, float *P) {
+    if (!ctx || !P) return fail(ctx, RTMB_EINVAL, "rtmb_taper_all_borders: null pointer");
+    LAUNCH(rtmb::launch_taper(P, ctx->d_taper, geom(ctx), 0, !(ctx->p.flags & RTMB_FLAG_NO_TAPER_QUIRK), ctx->stream));
+    return RTMB_OK;
+}
+
+int rtmb_taper_upper_borders(rtmb_ctx *ctx, float *P) {
+    if (!ctx || !P) return fail(ctx, RTMB_EINVAL, "rtmb_taper_upper_borders: null pointer");
+    LAUNCH(rtmb::launch_taper(P, ctx->d_taper, geom(ctx), 1, 0, ctx->stream));
+    return RTMB_OK;
+}
+
+int rtmb_apply_source(rtmb_ctx *ctx, float *PP, uint32_t sx, uint32_t sy, uint32_t sz, uint32_t it) {
+    if (!ctx || !PP) return fail(ctx, RTMB_EINVAL, "rtmb_apply_source: null pointer");
+    const uint32_t b = ctx->p.blen;
+    if (sx + b >= (uint32_t)ctx->nxe || sy + b >= (uint32_t)ctx->nye || sz + b >= (uint32_t)ctx->nze || it >= ctx->p.nt)
+        return fail(ctx, RTMB_EINVAL, "rtmb_apply_source: position or time step out of range");
+    LAUNCH(rtmb::launch_source(PP, ctx->d_wavelet, (int)it, (int)(sx + b), (int)(sy + b), (int)(sz + b), geom(ctx),
+                               ctx->stream));
+    return RTMB_OK;
+}
+
+int rtmb_save_receiver_data(rtmb_ctx *ctx, const float *PP, float *rec, uint32_t lt) {
+    if (!ctx || !PP || !rec || lt >= ctx->p.ntstep) return fail(ctx, RTMB_EINVAL, "rtmb_save_receiver_data: bad argument");
+    if (ctx->p.receiver_depth_z + ctx->p.blen >= (uint32_t)ctx->nze) return fail(ctx, RTMB_EINVAL, "receiver depth out of range");
+    LAUNCH(rtmb::launch_receivers(const_cast<float *>(PP), rec, (int)lt, 1, rgeom(ctx), geom(ctx), ctx->stream));
+    return RTMB_OK;
+}
+
+int rtmb_restore_receiver_data(rtmb_ctx *ctx, float *PP, const float *rec, uint32_t lt) {
+    if (!ctx || !PP || !rec || lt >= ctx->p.ntstep) return fail(ctx, RTMB_EINVAL, "rtmb_restore_receiver_data: bad argument");
+    if (ctx->p.receiver_depth_z + ctx->p.blen >= (uint32_t)ctx->nze) return fail(ctx, RTMB_EINVAL, "receiver depth out of range");
+    const int mode = (ctx->p.flags & RTMB_FLAG_RCV_ADD) ? 3 : 2;
+    LAUNCH(rtmb::launch_receivers(PP, const_cast<float *>(rec), (int)lt, mode, rgeom(ctx), geom(ctx), ctx->stream));
+    return RTMB_OK;
+}
+
+int rtmb_save_upper_border(rtmb_ctx *ctx, const float *P, float *upb, uint32_t lt) {
+    if (!ctx || !P || !upb || lt >= ctx->p.ntstep) return fail(ctx, RTMB_EINVAL, "rtmb_save_upper_border: bad argument");
+    if ((int)ctx->p.blen < ctx->h) return fail(ctx, RTMB_EINVAL, "upper border needs blen >= stencil_order/2");
+    LAUNCH(rtmb::launch_upb(const_cast<float *>(P), upb, (int)lt, 1, geom(ctx), ctx->stream));
+    return RTMB_OK;
+}
+
+int rtmb_restore_upper_border(rtmb_ctx *ctx, float *P, const float *upb, uint32_t lt) {
+    if (!ctx || !P || !upb || lt >= ctx->p.ntstep) return fail(ctx, RTMB_EINVAL, "rtmb_restore_upper_border: bad argument");
+    if ((int)ctx->p.blen < ctx->h) return fail(ctx, RTMB_EINVAL, "upper border needs blen >= stencil_order/2");
+    LAUNCH(rtmb::launch_upb(P, const_cast<float *>(upb), (int)lt, 0, geom(ctx), ctx->stream));
+    return RTMB_OK;
+}
+
+int rtmb_image_condition(rtmb_ctx *ctx, float *img, const float *ps, const float *pr) {
+    if (!ctx || !img || !ps || !pr) return fail(ctx, RTMB_EINVAL, "rtmb_image_condition: null pointer");
+    const bool full = ctx->p.flags & RTMB_FLAG_IMG_FULL_Z;
+    const int z0 = full ? 0 : (int)ctx->p.blen, z1 = full ? ctx->nze : ctx->nze - (int)ctx->p.blen;
+    LAUNCH(rtmb::launch_image(img, ps, pr, z0, z1, geom(ctx), ctx->stream));
+    return RTMB_OK;
+}
+
+int rtmb_image_finalize(rtmb_ctx *ctx, const float *img, float *out) {
+    if (!ctx || !img || !out) return fail(ctx, RTMB_EINVAL, "rtmb_image_finalize: null pointer");
+    if (ctx->p.blen < 1) return fail(ctx, RTMB_EINVAL, "rtmb_image_finalize needs blen >= 1");
+    float c3[9];
+    rtmb_stencil_coefs(2, ctx->p.dx, ctx->p.dy, ctx->p.dz, c3);
+    LAUNCH(rtmb::launch_filter_remove(img, out, c3, geom(ctx), ctx->stream));
+    return RTMB_OK;
+}
+
+int rtmb_image_stack(rtmb_ctx *ctx, float *acc, const float *img) {
+    if (!ctx || !acc || !img) return fail(ctx, RTMB_EINVAL, "rtmb_image_stack: null pointer");
+    LAUNCH(rtmb::launch_stack(acc, img, ctx->n, ctx->stream));
+    return RTMB_OK;
+}
+
+// ------------------------------------------------------------------ drivers
+
+int rtmb_load_v2dt2(rtmb_ctx *ctx, const float *v2dt2, int from_host) {
+    if (!ctx || !v2dt2) return fail(ctx, RTMB_EINVAL, "rtmb_load_v2dt2: null pointer");
+    int rc = ensure(ctx, &ctx->d_v2dt2, ctx->n, false);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(ctx->d_v2dt2, v2dt2, ctx->n * sizeof(float),
+                       from_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return RTMB_OK;
+}
+
+int rtmb_model_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, float *rec) {
+    if (!ctx || !rec) return fail(ctx, RTMB_EINVAL, "rtmb_model_shot: null pointer");
+    int rc = check_shot(ctx, sx, sy, sz);
+    if (rc) return rc;
+    if (ctx->p.receiver_depth_z + ctx->p.blen >= (uint32_t)ctx->nze - ctx->h)
+        return fail(ctx, RTMB_EINVAL, "receiver depth outside the computed region");
+    if ((rc = alloc_driver(ctx))) return rc;
+    float *P, *PP;
+    // RTMFiniteDifferencesKernel.cpp:169-216: taper all faces, step, inject, sample.
+    if ((rc = run_forward(ctx, sx, sy, sz, rtmb::kTaperAll, rec, nullptr, &P, &PP))) return rc;
+    return check_err_flag(ctx);
+}
+
+int rtmb_migrate_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const float *rec, float *img) {
+    if (!ctx || !rec || !img) return fail(ctx, RTMB_EINVAL, "rtmb_migrate_shot: null pointer");
+    int rc = check_shot(ctx, sx, sy, sz);
+    if (rc) return rc;
+    const rtmb_params &p = ctx->p;
+    if (p.boundary != RTMB_BC_HBC && p.boundary != RTMB_BC_RBC)
+        return fail(ctx, RTMB_EINVAL, "migration boundary must be HBC or RBC");
+    if (p.receiver_depth_z + p.blen >= (uint32_t)ctx->nze - ctx->h)
+        return fail(ctx, RTMB_EINVAL, "receiver depth outside the computed region");
+    if ((rc = alloc_driver(ctx))) return rc;
+    const bool hbc = p.boundary == RTMB_BC_HBC;
+    const size_t upb_step = (size_t)ctx->nxe * ctx->nye * ctx->h;
+    if (hbc && (rc = ensure(ctx, &ctx->d_upb, upb_step * p.nt, true))) return rc;
+
+    // forward pass (HBC.cpp:96-210 / RBC.cpp:54-144)
+    float *sP, *sPP;
+    if ((rc = run_forward(ctx, sx, sy, sz, hbc ? rtmb::kTaperUpper : rtmb::kTaperNone, nullptr,
+                          hbc ? ctx->d_upb : nullptr, &sP, &sPP)))
+        return rc;
+    // snap0 is P after its last in-place taper (HBC.cpp:150, 203)
+    if (hbc) LAUNCH(rtmb::launch_taper(sP, ctx->d_taper, geom(ctx), 1, 0, ctx->stream));
+
+    // backward pass (HBC.cpp:212-364 / RBC.cpp:146-274)
+    float *rP = ctx->d_w[2], *rPP = ctx->d_w[3];
+    CK(cudaMemsetAsync(rP, 0, ctx->n * sizeof(float), ctx->stream));
+    CK(cudaMemsetAsync(rPP, 0, ctx->n * sizeof(float), ctx->stream));
+    CK(cudaMemsetAsync(img, 0, ctx->n * sizeof(float), ctx->stream));
+    const bool full = p.flags & RTMB_FLAG_IMG_FULL_Z;
+    float *s_cur = sPP, *s_prev = sP;  // it = nt-1 images snap1
+    rtmb::StepArgs src = base_args(ctx);
+    src.V = ctx->d_v2dt2;
+    if (hbc) src.upb_mode = rtmb::kUpbRestore;
+    rtmb::StepArgs rcv = base_args(ctx);
+    rcv.V = ctx->d_v2dt2;
+    rcv.taper_mode = hbc ? rtmb::kTaperUpper : rtmb::kTaperNone;
+    rcv.img = img;
+    rcv.img_z0 = full ? 0 : (int)p.blen;
+    rcv.img_z1 = full ? ctx->nze : ctx->nze - (int)p.blen;
+    const int rmode = (p.flags & RTMB_FLAG_RCV_ADD) ? rtmb::kRecAdd : rtmb::kRecOverwrite;
+    for (int it = (int)p.nt - 1; it >= 0; --it) {
+        if (it == (int)p.nt - 2) {
+            s_cur = sP;
+            s_prev = sPP;
+        } else if (it < (int)p.nt - 2) {
+            src.P = s_cur; src.PP = s_prev; src.it = it;
+            if (hbc) src.upb = ctx->d_upb + (size_t)it * upb_step;
+            LAUNCH(rtmb::launch_step(src, (int)p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
+            std::swap(s_cur, s_prev);
+        }
+        rcv.P = rP; rcv.PP = rPP; rcv.it = it;
+        rcv.ps = s_cur;
+        set_receivers(rcv, ctx, rmode, const_cast<float *>(rec), it);
+        LAUNCH(rtmb::launch_step(rcv, (int)p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
+        std::swap(rP, rPP);
+    }
+    return check_err_flag(ctx);
+}
+
+int rtmb_model_shot_host(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, float *rec_host) {
+    if (!ctx || !rec_host) return fail(ctx, RTMB_EINVAL, "rtmb_model_shot_host: null pointer");
+    const size_t nrec = (size_t)ctx->p.nt * ctx->p.receiver_count_x * ctx->p.receiver_count_y;
+    int rc = ensure(ctx, &ctx->d_rec, nrec ? nrec : 1, false);
+    if (rc) return rc;
+    if ((rc = rtmb_model_shot(ctx, sx, sy, sz, ctx->d_rec))) return rc;
+    CK(cudaMemcpyAsync(rec_host, ctx->d_rec, nrec * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return RTMB_OK;
+}
+
+int rtmb_migrate_shot_host(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const float *rec_host,
+                           float *img_host) {
+    if (!ctx || !rec_host || !img_host) return fail(ctx, RTMB_EINVAL, "rtmb_migrate_shot_host: null pointer");
+    const size_t nrec = (size_t)ctx->p.nt * ctx->p.receiver_count_x * ctx->p.receiver_count_y;
+    int rc = ensure(ctx, &ctx->d_rec, nrec ? nrec : 1, false);
+    if (rc) return rc;
+    if ((rc = ensure(ctx, &ctx->d_img, ctx->n, false))) return rc;
+    CK(cudaMemcpyAsync(ctx->d_rec, rec_host, nrec * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    if ((rc = rtmb_migrate_shot(ctx, sx, sy, sz, ctx->d_rec, ctx->d_img))) return rc;
+    CK(cudaMemcpyAsync(img_host, ctx->d_img, ctx->n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return RTMB_OK;
+}
+
+}  // extern "C"

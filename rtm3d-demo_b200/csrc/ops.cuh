@@ -1,0 +1,36 @@
+// ops.cuh -- the small per-operator kernels of librtm3d_b200 (one launch per reference operator).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace rtmb {
+
+struct Geom {
+    int nxe, nye, nze, blen, h;
+};
+
+struct RcvGeom {
+    int rx0, ry0, rz;   // padded coordinates of receiver (0, 0)
+    int rdx, rdy, rcx, rcy;
+    int ntstep;
+};
+
+// taper3D / taperUpper3D in place (RTMCPUPlatform.cpp:566-920); upper != 0 for the upper form.
+cudaError_t launch_taper(float *P, const float *taper, const Geom &g, int upper, int quirk, cudaStream_t s);
+// PP[x, y, z] += wavelet[it] (padded coordinates; RTMCPUPlatform.cpp:103-113).
+cudaError_t launch_source(float *PP, const float *wavelet, int it, int x, int y, int z, const Geom &g,
+                          cudaStream_t s);
+// mode 1: rec[i][j][lt] = PP; 2: PP = rec (CPU path); 3: PP += rec (reference GPU kernel).
+cudaError_t launch_receivers(float *PP, float *rec, int lt, int mode, const RcvGeom &r, const Geom &g,
+                             cudaStream_t s);
+// rw 1: upb[lt][x][y][k] = P[x][y][blen-h+k]; rw 0: the reverse (RTMCPUPlatform.cpp:153-189).
+cudaError_t launch_upb(float *P, float *upb, int lt, int rw, const Geom &g, cudaStream_t s);
+// img += ps * pr on all x, y and z in [z0, z1) (RTMCPUPlatform.cpp:513-540).
+cudaError_t launch_image(float *img, const float *ps, const float *pr, int z0, int z1, const Geom &g,
+                         cudaStream_t s);
+// order-2 Laplacian filter then border removal (RTMGrid.cpp:129-300); c3 = [3][3] coefficients.
+cudaError_t launch_filter_remove(const float *img, float *out, const float *c3, const Geom &g, cudaStream_t s);
+// acc += img over n floats.
+cudaError_t launch_stack(float *acc, const float *img, size_t n, cudaStream_t s);
+
+}  // namespace rtmb

@@ -1,0 +1,9 @@
+// stencil_h8.cu -- instantiations of the fused time-step kernels for stencil order 16.
+#include "stencil.cuh"
+#include "stencil_impl.cuh"
+
+namespace rtmb {
+namespace detail {
+template cudaError_t launch_h<8>(const StepArgs &, bool, bool, dim3, cudaStream_t);
+}  // namespace detail
+}  // namespace rtmb

@@ -1,0 +1,457 @@
+// stencil_tma_impl.cuh -- the TMA-pipelined form of the fused time step (sm_100a).
+//
+// Same contract and arithmetic as stencil_impl.cuh (bit-identical results); used when rows are
+// 16-byte aligned (nze % 4 == 0, 16-byte aligned base pointers).
+//
+// Pipeline.  A CTA owns a TZ x TY tile of the (y, z) plane and a chunk of x planes; its eight warps
+// compute, and thread 0 is also the producer of two rings of shared-memory slots filled by
+// cp.async.bulk.tensor (TMA) loads that complete on "full" mbarriers:
+//   * the P ring (D slots): the P tile of one plane with a y halo of H rows and a z halo of ZH
+//     columns.  A slot is needed from the plane's arrival (its centre values enter each thread's
+//     register queue of x taps) until the plane is computed H planes later (y and z taps);
+//   * the core ring (R slots): the PP and v2dt2 tiles (and PS and IMG for the imaging form) of the
+//     plane being computed.
+// One block barrier per plane keeps the warps in step (the plane loop is unrolled by the queue
+// length 2H+1 so the register queue rotates at compile time, and warps in step share the fetched
+// instructions); it also releases the slots of the previous plane, which the producer refills at
+// once, D-H-1 planes (P) and R-1 planes (core) ahead of their use.
+//
+// Every wait is bounded (about two seconds): a wait that runs out sets error bit 2 and the CTA stops,
+// after waiting, again bounded, for the copies it issued.
+#pragma once
+#include <cuda.h>
+
+#include "stencil_common.cuh"
+
+namespace rtmb {
+namespace detail {
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the completion of the phase with the given parity: false after ~2^32 cycles.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - t0 > (1ll << 32)) return false;
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0, int c1,
+                                            int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ float4 ld_f4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+
+// Tensor maps of one launch.  p: box {TZ + 2ZH, TY + 2H, 1}; the others: box {TZ, TY, 1}.
+struct TmaMaps {
+    CUtensorMap p, pp, v, ps, img;
+};
+
+template <int H, bool IMG>
+struct TmaShape {
+    static constexpr int ZH = ((H + 3) / 4) * 4;
+    static constexpr int SROWS = kTY + 2 * H;
+    static constexpr int SPITCH = kTZ + 2 * ZH;
+    static constexpr int STAGE = SROWS * SPITCH;             // floats written by one P tile load
+    static constexpr int STRIDE = ((STAGE + 31) / 32) * 32;  // P slot pitch: 128-byte aligned
+    static constexpr int CORE = kTZ * kTY;                   // floats of one core tile
+    static constexpr int NCORE = IMG ? 4 : 2;                // PP, V (, PS, IMG)
+    static constexpr int D = IMG ? H + 5 : H + 6;            // P slots
+    static constexpr int R = IMG ? 3 : 4;                    // core slots
+    static_assert(2 * H <= D && D >= H + 2, "warm-up planes and the lookahead must fit in the P ring");
+    static constexpr size_t SMEM =
+        ((size_t)D * STRIDE + (size_t)R * NCORE * CORE) * sizeof(float) + (D + R) * sizeof(uint64_t);
+};
+
+// TAPER: kTaperNone / kTaperUpper / kTaperAll.  IMG: the epilogue accumulates the image.
+template <int H, bool EXACT, int TAPER, bool IMG>
+__global__ void __launch_bounds__(kThreads, 2)
+    tma_step_kernel(const __grid_constant__ TmaMaps maps, const __grid_constant__ StepArgs a) {
+    using S = TmaShape<H, IMG>;
+    constexpr int ZH = S::ZH, SPITCH = S::SPITCH, STAGE = S::STAGE, STRIDE = S::STRIDE, D = S::D, R = S::R;
+    constexpr int CORE = S::CORE, NCORE = S::NCORE;
+    constexpr int NQ = 2 * H + 1;
+    constexpr int ZQ = kTZ / kVZ;
+    extern __shared__ __align__(128) float smem[];
+    float *pring = smem;
+    float *cring = smem + D * STRIDE;
+    uint64_t *pfull = reinterpret_cast<uint64_t *>(cring + R * NCORE * CORE);
+    uint64_t *cfull = pfull + D;
+
+    const int tid = threadIdx.x;
+    const int tz = tid % ZQ, ty = tid / ZQ;
+    const int zt0 = blockIdx.x * kTZ;
+    const int yt0 = H + blockIdx.y * kTY;
+    const int z0 = zt0 + tz * kVZ;
+    const int y = yt0 + ty;
+    const int xc0 = H + blockIdx.z * a.chunk;
+    const int xc1 = min(xc0 + a.chunk, a.nxe - H);
+    if (xc0 >= xc1) return;
+    const int n = xc1 - xc0;        // output planes, local index i <-> x = xc0 + i
+    const int nplanes = n + 2 * H;  // P planes, local index k <-> x = xc0 - H + k
+    const size_t plane = (size_t)a.nye * a.nze;
+
+    if (tid == 0) {
+        for (int s = 0; s < D; ++s) mbar_init(&pfull[s], 1);
+        for (int s = 0; s < R; ++s) mbar_init(&cfull[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    // ---- producer (thread 0): loads are issued in order, each after a block barrier has released
+    // its slot
+    int p_issued = 0, c_issued = 0;  // next P plane / next core plane to issue
+    auto issue_p = [&](int upto) {
+        for (; p_issued <= upto && p_issued < nplanes; ++p_issued) {
+            const int k = p_issued, s = k % D;
+            mbar_expect_tx(&pfull[s], STAGE * sizeof(float));
+            tma_load_3d(pring + s * STRIDE, &maps.p, &pfull[s], zt0 - ZH, yt0 - H, xc0 - H + k);
+        }
+    };
+    auto issue_c = [&](int upto) {
+        for (; c_issued <= upto && c_issued < n; ++c_issued) {
+            const int i = c_issued, s = i % R;
+            float *dst = cring + s * NCORE * CORE;
+            mbar_expect_tx(&cfull[s], NCORE * CORE * sizeof(float));
+            tma_load_3d(dst, &maps.pp, &cfull[s], zt0, yt0, xc0 + i);
+            tma_load_3d(dst + CORE, &maps.v, &cfull[s], zt0, yt0, xc0 + i);
+            if (IMG) {
+                tma_load_3d(dst + 2 * CORE, &maps.ps, &cfull[s], zt0, yt0, xc0 + i);
+                tma_load_3d(dst + 3 * CORE, &maps.img, &cfull[s], zt0, yt0, xc0 + i);
+            }
+        }
+    };
+    if (tid == 0) {
+        issue_p(D - 1);
+        issue_c(R - 1);
+    }
+    // (planes D .. D+H-1 follow once the warm-up planes 0 .. H-1 are in the queue)
+
+    // ---- per-thread constants, hoisted out of the plane loop
+    const bool row_ok = y < a.nye && z0 < a.nze;
+    const bool y_ok = y < a.nye - H;
+    unsigned vmask = 0, imask = 0, umask = 0, qmask = 0;
+#pragma unroll
+    for (int e = 0; e < kVZ; ++e) {
+        const int z = z0 + e;
+        const bool v = y_ok && z >= H && z < a.nze - H;
+        if (v) vmask |= 1u << e;
+        if (v && IMG && z >= a.img_z0 && z < a.img_z1) imask |= 1u << e;
+        if (v && a.upb_mode != kUpbNone && z >= a.blen - H && z < a.blen) umask |= 1u << e;
+        if (v && a.quirk_out && y >= a.nye - a.blen && z >= a.blen && z < a.nze - a.blen) qmask |= 1u << e;
+    }
+    const int src_e =
+        (y == a.sye && a.sze >= z0 && a.sze < z0 + kVZ && ((vmask >> (a.sze - z0)) & 1u)) ? a.sze - z0 : -1;
+    int rec_e = -1, rec_j = 0;
+    if (a.rec_mode != kRecNone && a.rz >= z0 && a.rz < z0 + kVZ && ((vmask >> (a.rz - z0)) & 1u)) {
+        const int dyr = y - a.ry0;
+        if (dyr >= 0 && dyr % a.rdy == 0 && dyr / a.rdy < a.rcy) {
+            rec_e = a.rz - z0;
+            rec_j = dyr / a.rdy;
+        }
+    }
+    const bool special = src_e >= 0 || rec_e >= 0 || umask != 0 || qmask != 0;
+    bool tile_taper_yz = false;  // does this CTA's tile touch the taper region (x border aside)?
+    if (TAPER == kTaperAll)
+        tile_taper_yz = (yt0 - H < a.blen) || (yt0 + kTY + H > a.nye - a.blen) || (zt0 - ZH < a.blen) ||
+                        (zt0 + kTZ + ZH > a.nze - a.blen);
+    if (TAPER == kTaperUpper) tile_taper_yz = (zt0 - ZH < a.blen);
+    bool pp_taper_yz = false;    // T o T needed on this thread's own PP values?
+    if (TAPER == kTaperAll)
+        pp_taper_yz = (y < a.blen) || (y >= a.nye - a.blen) || (z0 < a.blen) || (z0 + kVZ > a.nze - a.blen);
+    if (TAPER == kTaperUpper) pp_taper_yz = z0 < a.blen;
+
+    const size_t row_off = (size_t)y * a.nze + z0;
+    float *PPp = a.PP + row_off;
+    const int col = ZH + tz * kVZ;
+    const int ccol = ty * kTZ + tz * kVZ;  // this thread's offset in a core tile
+
+    bool bad_wait = false;
+    int kdone = 0;  // P planes whose wait succeeded, in order
+    auto wait_p = [&](int k) {  // warp-uniform outcome, so a warp never splits at a timeout
+        const bool ok = __all_sync(0xffffffffu, mbar_wait(&pfull[k % D], (k / D) & 1));
+        if (ok && !bad_wait) kdone = k + 1;
+        bad_wait |= !ok;
+    };
+    // taper of the tile of P plane k, in place (TAPER forms).  The pass is collective: every thread
+    // tapers a share of the tile, so it ends with a block barrier.
+    auto taper_stage = [&](int k) {
+        const int x = xc0 - H + k;
+        bool need;
+        if (TAPER == kTaperAll) need = tile_taper_yz || x < a.blen || x >= a.nxe - a.blen;
+        else need = tile_taper_yz;
+        if (!need) return;  // uniform across the CTA
+        float *st = pring + (k % D) * STRIDE;
+        for (int c = tid; c < STAGE; c += kThreads) {
+            const int r = c / SPITCH, cc = c % SPITCH;
+            const int yy = yt0 - H + r, zz = zt0 - ZH + cc;
+            if (yy >= a.nye || zz < 0 || zz >= a.nze) continue;
+            float v = st[c];
+            if (TAPER == kTaperAll && quirk_cell(x, yy, zz, a)) {
+                const float tyy = face_factor(a.taper, a.blen, a.nye, yy);
+                v = __ldg(a.P + (size_t)a.blen * plane + (size_t)yy * a.nze + zz);
+                v = v * tyy;
+                v = v * face_factor(a.taper, a.blen, a.nxe, x);
+                v = v * tyy;
+            } else {
+                v = taper_once(v, x, yy, zz, a);
+            }
+            st[c] = v;
+        }
+        __syncthreads();
+    };
+
+    float4 q[NQ];
+    float nanacc = 0.f;  // stays 0 unless a NaN or an infinity is written
+
+
+    // warm-up: P planes 0 .. 2H-1 into the queue; planes 0 .. H-1 are not computed here
+    for (int k = 0; k < 2 * H; ++k) {
+        wait_p(k);
+        if (TAPER != kTaperNone) taper_stage(k);
+    }
+#pragma unroll
+    for (int k = 0; k < 2 * H; ++k) q[k] = ld_f4(pring + (k % D) * STRIDE + (ty + H) * SPITCH + col);
+    if (__syncthreads_or(bad_wait)) goto drain;
+    if (tid == 0) issue_p(H + D - 1);  // planes 0 .. H-1 were only needed for the queue
+
+    for (int i0 = 0; i0 < n; i0 += NQ) {
+#pragma unroll
+        for (int u = 0; u < NQ; ++u) {
+            const int i = i0 + u;
+            if (i >= n) break;  // uniform
+            const int x = xc0 + i;
+            if (i > 0) {
+                // every warp is done with plane i-1: its P and core slots are free
+                if (__syncthreads_or(bad_wait)) goto drain;
+                if (tid == 0) {
+                    issue_p(i - 1 + H + D);
+                    issue_c(i - 1 + R);
+                }
+            }
+            const int kin = i + 2 * H;
+            wait_p(kin);
+            if (TAPER != kTaperNone) {
+                if (__syncthreads_or(bad_wait)) goto drain;  // the taper pass is collective
+                taper_stage(kin);
+            } else if (bad_wait) {
+                goto drain;  // a timed-out wait leaves the data undefined; stop without computing
+            }
+            q[(u + 2 * H) % NQ] = ld_f4(pring + (kin % D) * STRIDE + (ty + H) * SPITCH + col);
+            const float *s = pring + ((i + H) % D) * STRIDE;
+
+            float lap[kVZ] = {0.f, 0.f, 0.f, 0.f};
+            if (row_ok) {
+                float zr[kVZ + 2 * ZH];
+#pragma unroll
+                for (int k = 0; k < (kVZ + 2 * ZH) / 4; ++k) {
+                    const float4 t4 =
+                        (k == ZH / 4) ? q[(u + H) % NQ] : ld_f4(s + (ty + H) * SPITCH + col - ZH + 4 * k);
+                    zr[4 * k + 0] = t4.x; zr[4 * k + 1] = t4.y; zr[4 * k + 2] = t4.z; zr[4 * k + 3] = t4.w;
+                }
+                if (EXACT) {
+                    float ax[kVZ], ay[kVZ], az[kVZ];
+#pragma unroll
+                    for (int e = 0; e < kVZ; ++e) { ax[e] = 0.f; ay[e] = 0.f; az[e] = 0.f; }
+#pragma unroll
+                    for (int io = 0; io < NQ; ++io) {
+                        const float4 qx = q[(u + io) % NQ];
+                        const float4 ry = (io == H) ? q[(u + H) % NQ] : ld_f4(s + (ty + io) * SPITCH + col);
+#pragma unroll
+                        for (int e = 0; e < kVZ; ++e) {
+                            ax[e] = ax[e] + get(qx, e) * a.cx[io];
+                            ay[e] = ay[e] + get(ry, e) * a.cy[io];
+                            az[e] = az[e] + zr[ZH - H + e + io] * a.cz[io];
+                        }
+                    }
+#pragma unroll
+                    for (int e = 0; e < kVZ; ++e) lap[e] = ax[e] + ay[e] + az[e];
+                } else {
+                    const float cc = a.cx[H] + a.cy[H] + a.cz[H];
+                    const float4 qc = q[(u + H) % NQ];
+#pragma unroll
+                    for (int e = 0; e < kVZ; ++e) lap[e] = get(qc, e) * cc;
+#pragma unroll
+                    for (int io = 0; io < NQ; ++io) {
+                        if (io == H) continue;
+                        const float4 qx = q[(u + io) % NQ];
+                        const float4 ry = ld_f4(s + (ty + io) * SPITCH + col);
+#pragma unroll
+                        for (int e = 0; e < kVZ; ++e) {
+                            lap[e] = fmaf(get(qx, e), a.cx[io], lap[e]);
+                            lap[e] = fmaf(get(ry, e), a.cy[io], lap[e]);
+                            lap[e] = fmaf(zr[ZH - H + e + io], a.cz[io], lap[e]);
+                        }
+                    }
+                }
+            }
+            // core tiles of plane x
+            const int cs = i % R;
+            if (!__all_sync(0xffffffffu, mbar_wait(&cfull[cs], (i / R) & 1))) {
+                bad_wait = true;
+                goto drain;
+            }
+            const float *ct = cring + cs * NCORE * CORE + ccol;
+            const float4 pp_raw = ld_f4(ct), vv = ld_f4(ct + CORE);
+            float4 ps4 = pp_raw, im4 = pp_raw;
+            if (IMG) { ps4 = ld_f4(ct + 2 * CORE); im4 = ld_f4(ct + 3 * CORE); }
+            if (!row_ok) continue;
+
+            const float4 qc = q[(u + H) % NQ];
+            float ppv[kVZ] = {pp_raw.x, pp_raw.y, pp_raw.z, pp_raw.w};
+            if (TAPER != kTaperNone) {
+                const bool pp_taper = pp_taper_yz || (TAPER == kTaperAll && (x < a.blen || x >= a.nxe - a.blen));
+                if (pp_taper) {
+#pragma unroll
+                    for (int e = 0; e < kVZ; ++e) {
+                        if (!((vmask >> e) & 1u)) continue;
+                        const int z = z0 + e;
+                        float pp = ppv[e];
+                        if (TAPER == kTaperAll && quirk_cell(x, y, z, a)) {
+                            const float ty_ = face_factor(a.taper, a.blen, a.nye, y);
+                            pp = a.quirk_in[(size_t)(y - (a.nye - a.blen)) * (a.nze - 2 * a.blen) + (z - a.blen)];
+                            pp = pp * ty_;
+                            pp = pp * ty_;
+                            pp = pp * face_factor(a.taper, a.blen, a.nxe, x);
+                            pp = pp * ty_;
+                        } else {
+                            pp = taper_once(taper_once(pp, x, y, z, a), x, y, z, a);
+                        }
+                        ppv[e] = pp;
+                    }
+                }
+            }
+            float npp[kVZ];
+#pragma unroll
+            for (int e = 0; e < kVZ; ++e) {
+                if (EXACT) {
+                    const float two_p = 2.f * get(qc, e);
+                    const float d = two_p - ppv[e];
+                    const float vl = get(vv, e) * lap[e];
+                    npp[e] = d + vl;
+                } else {
+                    npp[e] = fmaf(get(vv, e), lap[e], 2.f * get(qc, e) - ppv[e]);
+                }
+            }
+            if (special) {  // source, receivers, upper border or taper side buffer in this thread's cells
+#pragma unroll
+                for (int e = 0; e < kVZ; ++e) {
+                    const int z = z0 + e;
+                    if (e == src_e && x == a.sxe) npp[e] = npp[e] + a.wavelet[a.it];
+                    if (e == rec_e) {
+                        const int dxr = x - a.rx0;
+                        if (dxr >= 0 && dxr % a.rdx == 0 && dxr / a.rdx < a.rcx) {
+                            float *rp = a.rec + a.rec_base + (dxr / a.rdx) * a.rec_si + rec_j * a.rec_sj;
+                            if (a.rec_mode == kRecSample) *rp = npp[e];
+                            else if (a.rec_mode == kRecOverwrite) npp[e] = *rp;
+                            else npp[e] = npp[e] + *rp;
+                        }
+                    }
+                    if ((umask >> e) & 1u) {
+                        float *up = a.upb + ((size_t)x * a.nye + y) * H + (z - (a.blen - H));
+                        if (a.upb_mode == kUpbSave) *up = npp[e];
+                        else npp[e] = *up;
+                    }
+                    if (((qmask >> e) & 1u) && x == a.blen)
+                        a.quirk_out[(size_t)(y - (a.nye - a.blen)) * (a.nze - 2 * a.blen) + (z - a.blen)] = npp[e];
+                }
+            }
+            float4 out;
+#pragma unroll
+            for (int e = 0; e < kVZ; ++e) {
+                const float o = ((vmask >> e) & 1u) ? npp[e] : get(pp_raw, e);
+                put(out, e, o);
+                nanacc = fmaf(0.f, o, nanacc);  // stays 0 unless a NaN or an infinity appears
+            }
+            *reinterpret_cast<float4 *>(PPp + (size_t)x * plane) = out;
+            if (IMG && imask) {
+                float4 im;
+#pragma unroll
+                for (int e = 0; e < kVZ; ++e) {
+                    const float acc = get(im4, e) + get(ps4, e) * get(out, e);
+                    put(im, e, ((imask >> e) & 1u) ? acc : get(im4, e));
+                }
+                *reinterpret_cast<float4 *>(a.img + row_off + (size_t)x * plane) = im;
+            }
+        }
+    }
+    if (nanacc != nanacc && a.err) atomicOr(a.err, 1u);
+    return;
+
+drain:
+    // A wait ran out: record it, then wait (bounded) for the copies thread 0 issued.
+    if (a.err) atomicOr(a.err, 2u);
+    if (tid == 0) {
+        for (int k = kdone; k < p_issued; ++k)
+            if (!mbar_wait(&pfull[k % D], (k / D) & 1)) break;
+        for (int i = (c_issued > R ? c_issued - R : 0); i < c_issued; ++i)
+            if (!mbar_wait(&cfull[i % R], (i / R) & 1)) break;
+    }
+}
+
+template <int H>
+cudaError_t launch_tma_h(const TmaMaps &maps, const StepArgs &a, bool exact, int taper, bool img, dim3 grid,
+                         cudaStream_t s) {
+    // the dynamic shared-memory opt-in, once per (variant, device)
+    static unsigned long long attr_done[12] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int variant = (exact ? 6 : 0) + (img ? 3 : 0) + taper;
+    auto run = [&](void (*kern)(TmaMaps, StepArgs), size_t smem) -> cudaError_t {
+        const unsigned long long bit = 1ull << (dev & 63);
+        if (!(attr_done[variant] & bit)) {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            attr_done[variant] |= bit;
+        }
+        kern<<<grid, kThreads, smem, s>>>(maps, a);
+        return cudaGetLastError();
+    };
+#define RTMB_TMA_CASE(EX, TP, IM) \
+    if (exact == EX && taper == TP && img == IM) return run(tma_step_kernel<H, EX, TP, IM>, TmaShape<H, IM>::SMEM);
+    RTMB_TMA_CASE(true, kTaperNone, false)
+    RTMB_TMA_CASE(true, kTaperUpper, false)
+    RTMB_TMA_CASE(true, kTaperAll, false)
+    RTMB_TMA_CASE(true, kTaperNone, true)
+    RTMB_TMA_CASE(true, kTaperUpper, true)
+    RTMB_TMA_CASE(false, kTaperNone, false)
+    RTMB_TMA_CASE(false, kTaperUpper, false)
+    RTMB_TMA_CASE(false, kTaperAll, false)
+    RTMB_TMA_CASE(false, kTaperNone, true)
+    RTMB_TMA_CASE(false, kTaperUpper, true)
+#undef RTMB_TMA_CASE
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace detail
+}  // namespace rtmb

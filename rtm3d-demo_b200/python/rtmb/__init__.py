@@ -1,0 +1,271 @@
+"""ctypes binding of librtm3d_b200.so (the C ABI declared in include/rtm3d_b200.h).
+
+The library does all the work on the GPU; this module only marshals arguments.  Device buffers are
+passed as raw pointers, so any CUDA allocator works (the tests and bench.py use torch tensors).
+Importing the module never falls back to anything: if the shared library is missing or fails to
+load, ``load()`` raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+PKG_ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), "..", ".."))
+LIB_PATH = os.path.join(PKG_ROOT, "lib", "librtm3d_b200.so")
+BIN_PATH = os.path.join(PKG_ROOT, "bin", "rtm3d_b200")
+
+RTMB_OK, RTMB_EINVAL, RTMB_ENOMEM, RTMB_ECUDA, RTMB_ENAN, RTMB_ETIMEOUT, RTMB_EIO = range(7)
+BC = {"abc": 1, "hbc": 2, "rbc": 3}
+FLAG_FAST_FMA = 0x1
+FLAG_RCV_ADD = 0x2
+FLAG_IMG_FULL_Z = 0x4
+FLAG_NO_TAPER_QUIRK = 0x8
+FLAG_USE_GRAPH = 0x10
+FLAG_NO_TMA = 0x20
+
+# every symbol include/rtm3d_b200.h declares: (name, argtypes, restype)
+_vp, _fp, _u32, _i32 = C.c_void_p, C.POINTER(C.c_float), C.c_uint32, C.c_int32
+
+
+class RtmbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"rtmb error {code}: {msg}")
+        self.code = code
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("nx", _u32), ("ny", _u32), ("nz", _u32), ("blen", _u32), ("nt", _u32), ("ntstep", _u32),
+        ("stencil_order", _u32),
+        ("dx", C.c_float), ("dy", C.c_float), ("dz", C.c_float), ("dt", C.c_float),
+        ("fpeak", C.c_float), ("taper_factor", C.c_float),
+        ("receiver_start_x", _u32), ("receiver_start_y", _u32), ("receiver_depth_z", _u32),
+        ("receiver_distance_x", _u32), ("receiver_distance_y", _u32),
+        ("receiver_count_x", _u32), ("receiver_count_y", _u32),
+        ("boundary", _i32), ("flags", _u32), ("device", _i32),
+    ]
+
+    @classmethod
+    def from_input(cls, d: dict, flags: int = 0, device: int = -1) -> "Params":
+        """Build from input.json keys (RTMParam names)."""
+        p = cls()
+        for k in ("nx", "ny", "nz", "blen", "nt", "ntstep", "stencil_order", "dx", "dy", "dz", "dt",
+                  "fpeak", "taper_factor", "receiver_start_x", "receiver_start_y", "receiver_depth_z",
+                  "receiver_distance_x", "receiver_distance_y", "receiver_count_x", "receiver_count_y"):
+            setattr(p, k, d[k])
+        p.boundary = BC.get(str(d.get("boundary_condition", "hbc")).lower(), BC["hbc"])
+        p.flags = flags
+        p.device = device
+        return p
+
+
+SYMBOLS = [
+    ("rtmb_abi_version", [], C.c_int),
+    ("rtmb_create", [C.POINTER(Params), C.POINTER(_vp)], C.c_int),
+    ("rtmb_destroy", [_vp], C.c_int),
+    ("rtmb_last_error", [_vp], C.c_char_p),
+    ("rtmb_set_stream", [_vp, _vp], C.c_int),
+    ("rtmb_sync", [_vp], C.c_int),
+    ("rtmb_launch_count", [_vp], C.c_uint64),
+    ("rtmb_stencil_coefs", [_u32, C.c_float, C.c_float, C.c_float, _fp], C.c_int),
+    ("rtmb_taper_vector", [_u32, C.c_float, _fp], C.c_int),
+    ("rtmb_ricker", [_u32, C.c_float, C.c_float, _fp], C.c_int),
+    ("rtmb_prepare_velocity", [_fp, _u32, _u32, _u32, _u32, _i32, C.c_int64, _fp], C.c_int),
+    ("rtmb_v2dt2_host", [_fp, C.c_size_t, C.c_float], C.c_int),
+    ("rtmb_step", [_vp, _vp, _vp, _vp], C.c_int),
+    ("rtmb_taper_all_borders", [_vp, _vp], C.c_int),
+    ("rtmb_taper_upper_borders", [_vp, _vp], C.c_int),
+    ("rtmb_apply_source", [_vp, _vp, _u32, _u32, _u32, _u32], C.c_int),
+    ("rtmb_save_receiver_data", [_vp, _vp, _vp, _u32], C.c_int),
+    ("rtmb_restore_receiver_data", [_vp, _vp, _vp, _u32], C.c_int),
+    ("rtmb_save_upper_border", [_vp, _vp, _vp, _u32], C.c_int),
+    ("rtmb_restore_upper_border", [_vp, _vp, _vp, _u32], C.c_int),
+    ("rtmb_image_condition", [_vp, _vp, _vp, _vp], C.c_int),
+    ("rtmb_image_finalize", [_vp, _vp, _vp], C.c_int),
+    ("rtmb_image_stack", [_vp, _vp, _vp], C.c_int),
+    ("rtmb_load_v2dt2", [_vp, _vp, C.c_int], C.c_int),
+    ("rtmb_model_shot", [_vp, _u32, _u32, _u32, _vp], C.c_int),
+    ("rtmb_migrate_shot", [_vp, _u32, _u32, _u32, _vp, _vp], C.c_int),
+    ("rtmb_model_shot_host", [_vp, _u32, _u32, _u32, _vp], C.c_int),
+    ("rtmb_migrate_shot_host", [_vp, _u32, _u32, _u32, _vp, _vp], C.c_int),
+]
+
+_LIB = None
+
+
+def build() -> None:
+    """Compile librtm3d_b200.so (and the CLI) for sm_100a."""
+    subprocess.run(["make", "-s", "-j8", "-C", PKG_ROOT], check=True)
+
+
+def load(path: str = LIB_PATH):
+    """Load the shared library and bind every declared symbol; raises if anything is missing."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is not built; run rtmb.build() (make -C rtm3d-demo_b200)")
+    lib = C.CDLL(path)
+    for name, args, res in SYMBOLS:
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _LIB = lib
+    return lib
+
+
+def _ptr(t) -> int:
+    """Device (or host) address of a torch tensor / numpy array / int."""
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    if hasattr(t, "data_ptr"):
+        return t.data_ptr()
+    return t.ctypes.data
+
+
+class Context:
+    """One rtmb_ctx: the context of one shot geometry on one device."""
+
+    def __init__(self, params: Params, stream=None):
+        self.L = load()
+        self.params = params
+        h = _vp()
+        rc = self.L.rtmb_create(C.byref(params), C.byref(h))
+        if rc != RTMB_OK:
+            raise RtmbError(rc, "rtmb_create failed")
+        self.h = h
+        if stream is not None:
+            self._check(self.L.rtmb_set_stream(self.h, _ptr(stream) if not isinstance(stream, int) else stream))
+
+    def _check(self, rc: int) -> None:
+        if rc != RTMB_OK:
+            raise RtmbError(rc, self.L.rtmb_last_error(self.h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.L.rtmb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # properties -------------------------------------------------------------
+    @property
+    def padded_shape(self):
+        p = self.params
+        return (p.nx + 2 * p.blen, p.ny + 2 * p.blen, p.nz + 2 * p.blen)
+
+    @property
+    def launches(self) -> int:
+        return int(self.L.rtmb_launch_count(self.h))
+
+    def set_stream(self, stream) -> None:
+        self._check(self.L.rtmb_set_stream(self.h, stream))
+
+    def sync(self) -> None:
+        self._check(self.L.rtmb_sync(self.h))
+
+    # per-step operators ------------------------------------------------------
+    def step(self, P, PP, V):
+        self._check(self.L.rtmb_step(self.h, _ptr(P), _ptr(PP), _ptr(V)))
+
+    def taper_all(self, P):
+        self._check(self.L.rtmb_taper_all_borders(self.h, _ptr(P)))
+
+    def taper_upper(self, P):
+        self._check(self.L.rtmb_taper_upper_borders(self.h, _ptr(P)))
+
+    def apply_source(self, PP, sx, sy, sz, it):
+        self._check(self.L.rtmb_apply_source(self.h, _ptr(PP), sx, sy, sz, it))
+
+    def save_receivers(self, PP, rec, lt):
+        self._check(self.L.rtmb_save_receiver_data(self.h, _ptr(PP), _ptr(rec), lt))
+
+    def restore_receivers(self, PP, rec, lt):
+        self._check(self.L.rtmb_restore_receiver_data(self.h, _ptr(PP), _ptr(rec), lt))
+
+    def save_upb(self, P, upb, lt):
+        self._check(self.L.rtmb_save_upper_border(self.h, _ptr(P), _ptr(upb), lt))
+
+    def restore_upb(self, P, upb, lt):
+        self._check(self.L.rtmb_restore_upper_border(self.h, _ptr(P), _ptr(upb), lt))
+
+    def image(self, img, ps, pr):
+        self._check(self.L.rtmb_image_condition(self.h, _ptr(img), _ptr(ps), _ptr(pr)))
+
+    def image_finalize(self, img, out):
+        self._check(self.L.rtmb_image_finalize(self.h, _ptr(img), _ptr(out)))
+
+    def image_stack(self, acc, img):
+        self._check(self.L.rtmb_image_stack(self.h, _ptr(acc), _ptr(img)))
+
+    # drivers -----------------------------------------------------------------
+    def load_v2dt2(self, v2dt2, from_host: bool):
+        self._check(self.L.rtmb_load_v2dt2(self.h, _ptr(v2dt2), int(from_host)))
+
+    def model_shot(self, sx, sy, sz, rec):
+        self._check(self.L.rtmb_model_shot(self.h, sx, sy, sz, _ptr(rec)))
+
+    def migrate_shot(self, sx, sy, sz, rec, img):
+        self._check(self.L.rtmb_migrate_shot(self.h, sx, sy, sz, _ptr(rec), _ptr(img)))
+
+    def model_shot_host(self, sx, sy, sz, rec_host):
+        self._check(self.L.rtmb_model_shot_host(self.h, sx, sy, sz, _ptr(rec_host)))
+
+    def migrate_shot_host(self, sx, sy, sz, rec_host, img_host):
+        self._check(self.L.rtmb_migrate_shot_host(self.h, sx, sy, sz, _ptr(rec_host), _ptr(img_host)))
+
+
+# host-side tables (no GPU needed) ----------------------------------------------
+def _np():
+    import numpy as np
+    return np
+
+
+def stencil_coefs(order, dx, dy, dz):
+    np = _np()
+    out = np.zeros(3 * (order + 1), np.float32)
+    rc = load().rtmb_stencil_coefs(order, dx, dy, dz, out.ctypes.data_as(_fp))
+    if rc:
+        raise RtmbError(rc, "rtmb_stencil_coefs")
+    return out
+
+
+def taper_vector(blen, factor):
+    np = _np()
+    out = np.zeros(max(blen, 1), np.float32)
+    load().rtmb_taper_vector(blen, factor, out.ctypes.data_as(_fp))
+    return out[:blen]
+
+
+def ricker(nt, dt, fpeak):
+    np = _np()
+    out = np.zeros(nt, np.float32)
+    load().rtmb_ricker(nt, dt, fpeak, out.ctypes.data_as(_fp))
+    return out
+
+
+def prepare_velocity(v, blen: int, bc: str, seed: int = -1):
+    """extendBorders + initBorders on the host; bc in {'none', 'abc', 'hbc', 'rbc'}."""
+    np = _np()
+    v = np.ascontiguousarray(v, np.float32)
+    nx, ny, nz = v.shape
+    ve = np.zeros((nx + 2 * blen, ny + 2 * blen, nz + 2 * blen), np.float32)
+    code = 0 if bc == "none" else BC[bc]
+    rc = load().rtmb_prepare_velocity(v.ctypes.data_as(_fp), nx, ny, nz, blen, code, seed, ve.ctypes.data_as(_fp))
+    if rc:
+        raise RtmbError(rc, "rtmb_prepare_velocity")
+    return ve
+
+
+def v2dt2(ve, dt):
+    np = _np()
+    out = np.ascontiguousarray(ve, np.float32).copy()
+    load().rtmb_v2dt2_host(out.ctypes.data_as(_fp), out.size, dt)
+    return out

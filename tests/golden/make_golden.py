@@ -1,0 +1,105 @@
+"""Generate the golden fixtures of tests/golden/ by running the REFERENCE itself.
+
+The reference CPU program (oracle/_ref/RTM3D.bin, built from the reference's sources by
+``make -C oracle ref``) is driven through its own input.json on small seeded synthetic models:
+
+  * model_abc.npz  -- modeling shot record (ABC velocity + all-face taper), reference .seism files
+  * mig_hbc.npz    -- HBC migration image (RTMIMG file) with the extended velocity it used (vpe)
+  * mig_rbc.npz    -- RBC migration image with its extended velocity
+  * ops.npz        -- per-operator vectors from the reference CPU platform (oracle/_ref/librtmref.so)
+
+Run:  python tests/golden/make_golden.py      (needs oracle/_ref, i.e. the reference sources)
+"""
+from __future__ import annotations
+
+import glob
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+from oracle import REF_BIN, Reference  # noqa: E402
+from rtm_cases import input_json, layered_model, CASES  # noqa: E402
+
+
+def run_reference(case: dict, mode: str, workdir: str, vpe_path: str | None = None):
+    """Run RTM3D.bin for one case. mode: 'model' | 'hbc' | 'rbc'. Returns output arrays."""
+    v = layered_model(case)
+    vp = os.path.join(workdir, "vel.bin")
+    v.tofile(vp)
+    d = input_json(case, vpfile=vp, workdir=workdir)
+    if mode == "model":
+        d.update(modeling=True, migration=False)
+    else:
+        d.update(modeling=False, migration=True, boundary_condition=mode,
+                 save_vpe_file=True, vpefile=vpe_path or os.path.join(workdir, f"vpe_{mode}.bin"))
+    jp = os.path.join(workdir, f"{mode}.json")
+    with open(jp, "w") as f:
+        json.dump(d, f)
+    subprocess.run([REF_BIN, jp], check=True, capture_output=True, cwd=workdir)
+    return d
+
+
+def read_record(d: dict):
+    files = glob.glob(os.path.join(d["datdir"], "RTMSEISMOGRAM_*.seism"))
+    files.sort(key=lambda f: int(f.split("NTSTART")[1].split("_")[0]))
+    n = d["nt"] // d["ntstep"]
+    assert len(files) == n, files
+    return np.concatenate([np.fromfile(f, np.float32) for f in files]).reshape(
+        n, d["receiver_count_x"], d["receiver_count_y"], d["ntstep"])
+
+
+def main():
+    if not os.path.exists(REF_BIN):
+        raise SystemExit("oracle/_ref/RTM3D.bin missing: run `make -C oracle ref` first")
+    rng = np.random.default_rng(7)
+    case = CASES["golden"]
+    with tempfile.TemporaryDirectory() as wd:
+        d = run_reference(case, "model", wd)
+        rec = read_record(d)
+        np.savez_compressed(os.path.join(HERE, "model_abc.npz"), rec=rec)
+        for bc in ("hbc", "rbc"):
+            for f in glob.glob(os.path.join(wd, "out", "RTMIMG_*")):
+                os.remove(f)
+            dm = run_reference(case, bc, wd)
+            img = np.fromfile(glob.glob(os.path.join(wd, "out", "RTMIMG_*"))[0], np.float32)
+            img = img.reshape(case["nx"], case["ny"], case["nz"])
+            vpe = np.fromfile(dm["vpefile"], np.float32).reshape(
+                case["nx"] + 2 * case["blen"], case["ny"] + 2 * case["blen"], case["nz"] + 2 * case["blen"])
+            np.savez_compressed(os.path.join(HERE, f"mig_{bc}.npz"), img=img, vpe=vpe, rec=rec)
+
+    # per-operator vectors from the reference CPU platform
+    R = Reference()
+    nx, ny, nz, b = 10, 12, 9, 6
+    shp = (nx + 2 * b, ny + 2 * b, nz + 2 * b)
+    P = rng.standard_normal(shp).astype(np.float32)
+    PP = rng.standard_normal(shp).astype(np.float32)
+    V = (rng.random(shp) * 0.1).astype(np.float32)
+    out = dict(P=P, PP=PP, V=V)
+    for order in (2, 4, 8, 12):
+        out[f"coefs{order}"] = R.stencil_coefs(order, 10.0, 12.5, 7.5)
+        out[f"step{order}"], _ = R.step(nx, ny, nz, b, order, 10.0, 12.5, 7.5, P, PP, V)
+    out["taper"] = R.taper_vector(b, 0.2)
+    out["taper_all"] = R.taper(P, nx, ny, nz, b, 0.2, upper=False)
+    out["taper_upper"] = R.taper(P, nx, ny, nz, b, 0.2, upper=True)
+    out["image"] = R.image(P, PP, V, nx, ny, nz, b)
+    out["filter"] = R.filter_remove(P, b, 10.0, 12.5, 7.5)
+    out["ricker"] = R.ricker(500, 0.001, 15.0)
+    vel = (1500 + 3000 * rng.random((nx, ny, nz))).astype(np.float32)
+    out["vel"] = vel
+    for bc in ("abc", "rbc", "hbc"):
+        out[f"borders_{bc}"] = R.extend_init_borders(vel, b, bc, seed=1234)
+    np.savez_compressed(os.path.join(HERE, "ops.npz"), **out)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

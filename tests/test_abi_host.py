@@ -1,0 +1,64 @@
+"""CPU tests of librtm3d_b200.so: it loads, exports every declared symbol, and its host-side tables
+and velocity preparation are bit-identical to the oracle (no GPU calls here)."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+import rtmb
+from rtm_cases import bitexact
+
+HEADER = os.path.join(os.path.dirname(__file__), "..", "include", "rtm3d_b200.h")
+
+
+def declared_symbols():
+    src = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char \*|uint64_t)\s*\*?\s*(rtmb_\w+)\s*\(", src, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = rtmb.load()
+    names = declared_symbols()
+    assert len(names) >= 25, names
+    bound = {n for n, _, _ in rtmb.SYMBOLS}
+    for n in names:
+        assert hasattr(lib, n), n
+        assert n in bound, f"{n} missing from the Python binding"
+    assert lib.rtmb_abi_version() == 1
+
+
+@pytest.mark.parametrize("order", [2, 4, 6, 8, 10, 12, 14, 16])
+def test_stencil_coefs(oracle, order):
+    assert bitexact(rtmb.stencil_coefs(order, 10.0, 12.5, 6.25), oracle.stencil_coefs(order, 10.0, 12.5, 6.25))
+
+
+def test_tables(oracle):
+    for blen, f in ((8, 0.2), (32, 0.2), (40, 0.05), (21, 0.7)):
+        assert bitexact(rtmb.taper_vector(blen, f), oracle.taper_vector(blen, f))
+    for nt, dt, fp in ((1000, 0.001, 15.0), (3000, 0.001, 12.0), (2500, 0.00125, 10.0)):
+        assert bitexact(rtmb.ricker(nt, dt, fp), oracle.ricker(nt, dt, fp))
+
+
+@pytest.mark.parametrize("bc", ["abc", "rbc", "hbc"])
+def test_prepare_velocity(oracle, bc):
+    rng = np.random.default_rng(4)
+    v = (1500 + 3000 * rng.random((11, 13, 9))).astype(np.float32)
+    a = rtmb.prepare_velocity(v, 7, bc, seed=77)
+    b = oracle.extend_init_borders(v, 7, bc, seed=77)
+    assert bitexact(a, b)
+    assert bitexact(rtmb.v2dt2(a, 0.001), oracle.v2dt2(b, 0.001))
+
+
+def test_invalid_arguments_are_errors_not_exits():
+    lib = rtmb.load()
+    p = rtmb.Params()
+    p.nx = p.ny = p.nz = 8
+    p.nt, p.ntstep, p.stencil_order = 10, 3, 8   # nt % ntstep != 0
+    import ctypes as C
+    h = C.c_void_p()
+    assert lib.rtmb_create(C.byref(p), C.byref(h)) == rtmb.RTMB_EINVAL
+    p.ntstep = 5
+    p.stencil_order = 7                            # odd order
+    assert lib.rtmb_create(C.byref(p), C.byref(h)) == rtmb.RTMB_EINVAL
+    assert lib.rtmb_stencil_coefs(3, 1.0, 1.0, 1.0, None) == rtmb.RTMB_EINVAL
