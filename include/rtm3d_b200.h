@@ -98,6 +98,19 @@ int rtmb_sync(rtmb_ctx *ctx);
 int rtmb_abi_version(void);
 /* Count of this library's kernel launches since the context was created. */
 uint64_t rtmb_launch_count(const rtmb_ctx *ctx);
+/* Per-kernel timing of the per-shot drivers (no counterpart in the reference, whose report keeps
+ * millisecond wall times per phase, src/kernel/RTMKernel.cpp:11-80).  When enabled, every driver
+ * launch is bracketed by CUDA events on the context's stream; the durations are summed per category
+ * at the end of each driver call.  Enabling clears the totals. */
+#define RTMB_PROF_CATEGORIES 5
+#define RTMB_PROF_MODEL 0             /* modeling step (taper, source, receivers fused) */
+#define RTMB_PROF_FORWARD 1           /* migration forward step */
+#define RTMB_PROF_BACKWARD_SOURCE 2   /* backward source-wavefield reconstruction step */
+#define RTMB_PROF_BACKWARD_RECEIVER 3 /* backward receiver step with receiver injection and imaging */
+#define RTMB_PROF_OTHER 4
+int rtmb_profile(rtmb_ctx *ctx, int enable);
+/* ms[RTMB_PROF_CATEGORIES]: summed kernel time; launches[RTMB_PROF_CATEGORIES]: launch counts. */
+int rtmb_profile_read(const rtmb_ctx *ctx, double *ms, uint64_t *launches);
 
 /* ------------------------------------------------------------------ host-side tables
  * Bit-identical to the reference's host computations; usable without a GPU. */

@@ -4,6 +4,7 @@
 #include <cstring>
 #include <string>
 #include <utility>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -30,6 +31,13 @@ struct rtmb_ctx {
     int chunk = 0;
     uint64_t launches = 0;
     std::string err;
+    // optional per-kernel timing of the drivers (rtmb_profile): an event pair around each launch
+    bool prof = false;
+    std::vector<cudaEvent_t> ev;        // pool, two per recorded launch
+    std::vector<int> ev_cat;            // category of each recorded launch
+    size_t ev_used = 0;
+    double prof_ms[RTMB_PROF_CATEGORIES] = {};
+    uint64_t prof_n[RTMB_PROF_CATEGORIES] = {};
 };
 
 namespace {
@@ -59,6 +67,47 @@ int fail(rtmb_ctx *c, int code, const char *fmt, ...) {
         ++ctx->launches;                                                                          \
         CK(call);                                                                                 \
     } while (0)
+
+// A driver launch of category CAT, bracketed by profiling events when rtmb_profile is on.
+#define LAUNCH_CAT(CAT, call)                                                                     \
+    do {                                                                                          \
+        const size_t slot_ = prof_begin(ctx, CAT);                                                \
+        LAUNCH(call);                                                                             \
+        prof_end(ctx, slot_);                                                                     \
+    } while (0)
+
+size_t prof_begin(rtmb_ctx *c, int cat) {
+    if (!c->prof) return (size_t)-1;
+    if (c->ev_used + 2 > c->ev.size()) {
+        for (int k = 0; k < 256; ++k) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) return (size_t)-1;
+            c->ev.push_back(e);
+        }
+        c->ev_cat.resize(c->ev.size() / 2);
+    }
+    const size_t slot = c->ev_used / 2;
+    c->ev_cat[slot] = cat;
+    cudaEventRecord(c->ev[c->ev_used], c->stream);
+    c->ev_used += 2;
+    return slot;
+}
+
+void prof_end(rtmb_ctx *c, size_t slot) {
+    if (slot != (size_t)-1) cudaEventRecord(c->ev[2 * slot + 1], c->stream);
+}
+
+// After a stream synchronisation: fold the recorded event pairs into the per-category totals.
+void prof_collect(rtmb_ctx *c) {
+    for (size_t s = 0; s < c->ev_used / 2; ++s) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, c->ev[2 * s], c->ev[2 * s + 1]) == cudaSuccess) {
+            c->prof_ms[c->ev_cat[s]] += ms;
+            c->prof_n[c->ev_cat[s]] += 1;
+        }
+    }
+    c->ev_used = 0;
+}
 
 rtmb::Geom geom(const rtmb_ctx *c) { return rtmb::Geom{c->nxe, c->nye, c->nze, (int)c->p.blen, c->h}; }
 
@@ -106,6 +155,7 @@ int check_err_flag(rtmb_ctx *ctx) {
     unsigned h = 0;
     CK(cudaMemcpyAsync(&h, ctx->d_err, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->prof) prof_collect(ctx);
     if (h) {
         CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(unsigned), ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
@@ -151,7 +201,7 @@ void set_receivers(rtmb::StepArgs &a, const rtmb_ctx *c, int mode, float *rec, i
 // Forward time loop shared by modeling and the migration forward pass.  Leaves the last two
 // wavefields in (*P, *PP) raw (untapered): *P = u(nt-1), *PP = u(nt).
 int run_forward(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, int taper_mode, float *rec,
-                float *upb, float **P_out, float **PP_out) {
+                float *upb, float **P_out, float **PP_out, int cat) {
     const rtmb_params &p = ctx->p;
     const size_t nb = ctx->n * sizeof(float);
     float *P = ctx->d_w[0], *PP = ctx->d_w[1];
@@ -178,7 +228,7 @@ int run_forward(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, int taper_
         if (rec) set_receivers(a, ctx, rtmb::kRecSample, rec, (int)it);
         if (upb) { a.upb_mode = rtmb::kUpbSave; a.upb = upb + (size_t)it * upb_step; }
         if (quirk) { a.quirk_in = ctx->d_quirk[(it + 1) % 3]; a.quirk_out = ctx->d_quirk[it % 3]; }
-        LAUNCH(rtmb::launch_step(a, (int)p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
+        LAUNCH_CAT(cat, rtmb::launch_step(a, (int)p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
     }
     *P_out = P;
     *PP_out = PP;
@@ -255,6 +305,7 @@ int rtmb_destroy(rtmb_ctx *ctx) {
     if (!ctx) return RTMB_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (cudaEvent_t e : ctx->ev) cudaEventDestroy(e);
     float *bufs[] = {ctx->d_taper, ctx->d_wavelet, ctx->d_v2dt2, ctx->d_w[0], ctx->d_w[1], ctx->d_w[2],
                      ctx->d_w[3], ctx->d_quirk[0], ctx->d_quirk[1], ctx->d_quirk[2], ctx->d_upb,
                      ctx->d_rec, ctx->d_img};
@@ -269,6 +320,20 @@ int rtmb_destroy(rtmb_ctx *ctx) {
 int rtmb_set_stream(rtmb_ctx *ctx, void *cuda_stream) {
     if (!ctx) return RTMB_EINVAL;
     ctx->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : ctx->own_stream;
+    return RTMB_OK;
+}
+
+int rtmb_profile(rtmb_ctx *ctx, int enable) {
+    if (!ctx) return RTMB_EINVAL;
+    ctx->prof = enable != 0;
+    ctx->ev_used = 0;
+    for (int k = 0; k < RTMB_PROF_CATEGORIES; ++k) { ctx->prof_ms[k] = 0.0; ctx->prof_n[k] = 0; }
+    return RTMB_OK;
+}
+
+int rtmb_profile_read(const rtmb_ctx *ctx, double *ms, uint64_t *launches) {
+    if (!ctx || !ms || !launches) return RTMB_EINVAL;
+    for (int k = 0; k < RTMB_PROF_CATEGORIES; ++k) { ms[k] = ctx->prof_ms[k]; launches[k] = ctx->prof_n[k]; }
     return RTMB_OK;
 }
 
@@ -383,7 +448,7 @@ int rtmb_model_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, float 
     if ((rc = alloc_driver(ctx))) return rc;
     float *P, *PP;
     // RTMFiniteDifferencesKernel.cpp:169-216: taper all faces, step, inject, sample.
-    if ((rc = run_forward(ctx, sx, sy, sz, rtmb::kTaperAll, rec, nullptr, &P, &PP))) return rc;
+    if ((rc = run_forward(ctx, sx, sy, sz, rtmb::kTaperAll, rec, nullptr, &P, &PP, RTMB_PROF_MODEL))) return rc;
     return check_err_flag(ctx);
 }
 
@@ -404,10 +469,10 @@ int rtmb_migrate_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, cons
     // forward pass (HBC.cpp:96-210 / RBC.cpp:54-144)
     float *sP, *sPP;
     if ((rc = run_forward(ctx, sx, sy, sz, hbc ? rtmb::kTaperUpper : rtmb::kTaperNone, nullptr,
-                          hbc ? ctx->d_upb : nullptr, &sP, &sPP)))
+                          hbc ? ctx->d_upb : nullptr, &sP, &sPP, RTMB_PROF_FORWARD)))
         return rc;
     // snap0 is P after its last in-place taper (HBC.cpp:150, 203)
-    if (hbc) LAUNCH(rtmb::launch_taper(sP, ctx->d_taper, geom(ctx), 1, 0, ctx->stream));
+    if (hbc) LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_taper(sP, ctx->d_taper, geom(ctx), 1, 0, ctx->stream));
 
     // backward pass (HBC.cpp:212-364 / RBC.cpp:146-274)
     float *rP = ctx->d_w[2], *rPP = ctx->d_w[3];
@@ -433,13 +498,15 @@ int rtmb_migrate_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, cons
         } else if (it < (int)p.nt - 2) {
             src.P = s_cur; src.PP = s_prev; src.it = it;
             if (hbc) src.upb = ctx->d_upb + (size_t)it * upb_step;
-            LAUNCH(rtmb::launch_step(src, (int)p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
+            LAUNCH_CAT(RTMB_PROF_BACKWARD_SOURCE,
+                       rtmb::launch_step(src, (int)p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
             std::swap(s_cur, s_prev);
         }
         rcv.P = rP; rcv.PP = rPP; rcv.it = it;
         rcv.ps = s_cur;
         set_receivers(rcv, ctx, rmode, const_cast<float *>(rec), it);
-        LAUNCH(rtmb::launch_step(rcv, (int)p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
+        LAUNCH_CAT(RTMB_PROF_BACKWARD_RECEIVER,
+                   rtmb::launch_step(rcv, (int)p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
         std::swap(rP, rPP);
     }
     return check_err_flag(ctx);

@@ -11,10 +11,10 @@
 //     register queue of x taps) until the plane is computed H planes later (y and z taps);
 //   * the core ring (R slots): the PP and v2dt2 tiles (and PS and IMG for the imaging form) of the
 //     plane being computed.
-// One block barrier per plane keeps the warps in step (the plane loop is unrolled by the queue
-// length 2H+1 so the register queue rotates at compile time, and warps in step share the fetched
-// instructions); it also releases the slots of the previous plane, which the producer refills at
-// once, D-H-1 planes (P) and R-1 planes (core) ahead of their use.
+// One block barrier per plane keeps the warps in step and releases the slots of the previous
+// plane, which the producer refills at once, D-H-1 planes (P) and R-1 planes (core) ahead of their
+// use.  Each thread keeps the 2H+1 x taps of its four points in a register queue that shifts by one
+// plane per iteration.
 //
 // Every wait is bounded (about two seconds): a wait that runs out sets error bit 2 and the CTA stops,
 // after waiting, again bounded, for the copies it issued.
@@ -233,23 +233,19 @@ __global__ void __launch_bounds__(kThreads, 2)
 
     float4 q[NQ];
     float nanacc = 0.f;  // stays 0 unless a NaN or an infinity is written
-
-
     // warm-up: P planes 0 .. 2H-1 into the queue; planes 0 .. H-1 are not computed here
     for (int k = 0; k < 2 * H; ++k) {
         wait_p(k);
         if (TAPER != kTaperNone) taper_stage(k);
     }
 #pragma unroll
-    for (int k = 0; k < 2 * H; ++k) q[k] = ld_f4(pring + (k % D) * STRIDE + (ty + H) * SPITCH + col);
+    for (int k = 0; k < 2 * H; ++k) q[k + 1] = ld_f4(pring + (k % D) * STRIDE + (ty + H) * SPITCH + col);
     if (__syncthreads_or(bad_wait)) goto drain;
     if (tid == 0) issue_p(H + D - 1);  // planes 0 .. H-1 were only needed for the queue
 
-    for (int i0 = 0; i0 < n; i0 += NQ) {
-#pragma unroll
-        for (int u = 0; u < NQ; ++u) {
-            const int i = i0 + u;
-            if (i >= n) break;  // uniform
+#pragma unroll 1
+    for (int i = 0; i < n; ++i) {
+        {
             const int x = xc0 + i;
             if (i > 0) {
                 // every warp is done with plane i-1: its P and core slots are free
@@ -267,7 +263,9 @@ __global__ void __launch_bounds__(kThreads, 2)
             } else if (bad_wait) {
                 goto drain;  // a timed-out wait leaves the data undefined; stop without computing
             }
-            q[(u + 2 * H) % NQ] = ld_f4(pring + (kin % D) * STRIDE + (ty + H) * SPITCH + col);
+#pragma unroll
+            for (int k = 0; k < NQ - 1; ++k) q[k] = q[k + 1];  // advance the x queue
+            q[NQ - 1] = ld_f4(pring + (kin % D) * STRIDE + (ty + H) * SPITCH + col);
             const float *s = pring + ((i + H) % D) * STRIDE;
 
             float lap[kVZ] = {0.f, 0.f, 0.f, 0.f};
@@ -276,7 +274,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 #pragma unroll
                 for (int k = 0; k < (kVZ + 2 * ZH) / 4; ++k) {
                     const float4 t4 =
-                        (k == ZH / 4) ? q[(u + H) % NQ] : ld_f4(s + (ty + H) * SPITCH + col - ZH + 4 * k);
+                        (k == ZH / 4) ? q[H] : ld_f4(s + (ty + H) * SPITCH + col - ZH + 4 * k);
                     zr[4 * k + 0] = t4.x; zr[4 * k + 1] = t4.y; zr[4 * k + 2] = t4.z; zr[4 * k + 3] = t4.w;
                 }
                 if (EXACT) {
@@ -285,8 +283,8 @@ __global__ void __launch_bounds__(kThreads, 2)
                     for (int e = 0; e < kVZ; ++e) { ax[e] = 0.f; ay[e] = 0.f; az[e] = 0.f; }
 #pragma unroll
                     for (int io = 0; io < NQ; ++io) {
-                        const float4 qx = q[(u + io) % NQ];
-                        const float4 ry = (io == H) ? q[(u + H) % NQ] : ld_f4(s + (ty + io) * SPITCH + col);
+                        const float4 qx = q[io];
+                        const float4 ry = (io == H) ? q[H] : ld_f4(s + (ty + io) * SPITCH + col);
 #pragma unroll
                         for (int e = 0; e < kVZ; ++e) {
                             ax[e] = ax[e] + get(qx, e) * a.cx[io];
@@ -298,13 +296,13 @@ __global__ void __launch_bounds__(kThreads, 2)
                     for (int e = 0; e < kVZ; ++e) lap[e] = ax[e] + ay[e] + az[e];
                 } else {
                     const float cc = a.cx[H] + a.cy[H] + a.cz[H];
-                    const float4 qc = q[(u + H) % NQ];
+                    const float4 qc = q[H];
 #pragma unroll
                     for (int e = 0; e < kVZ; ++e) lap[e] = get(qc, e) * cc;
 #pragma unroll
                     for (int io = 0; io < NQ; ++io) {
                         if (io == H) continue;
-                        const float4 qx = q[(u + io) % NQ];
+                        const float4 qx = q[io];
                         const float4 ry = ld_f4(s + (ty + io) * SPITCH + col);
 #pragma unroll
                         for (int e = 0; e < kVZ; ++e) {
@@ -327,7 +325,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             if (IMG) { ps4 = ld_f4(ct + 2 * CORE); im4 = ld_f4(ct + 3 * CORE); }
             if (!row_ok) continue;
 
-            const float4 qc = q[(u + H) % NQ];
+            const float4 qc = q[H];
             float ppv[kVZ] = {pp_raw.x, pp_raw.y, pp_raw.z, pp_raw.w};
             if (TAPER != kTaperNone) {
                 const bool pp_taper = pp_taper_yz || (TAPER == kTaperAll && (x < a.blen || x >= a.nxe - a.blen));

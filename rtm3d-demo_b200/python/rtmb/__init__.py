@@ -68,6 +68,8 @@ SYMBOLS = [
     ("rtmb_set_stream", [_vp, _vp], C.c_int),
     ("rtmb_sync", [_vp], C.c_int),
     ("rtmb_launch_count", [_vp], C.c_uint64),
+    ("rtmb_profile", [_vp, C.c_int], C.c_int),
+    ("rtmb_profile_read", [_vp, C.POINTER(C.c_double), C.POINTER(C.c_uint64)], C.c_int),
     ("rtmb_stencil_coefs", [_u32, C.c_float, C.c_float, C.c_float, _fp], C.c_int),
     ("rtmb_taper_vector", [_u32, C.c_float, _fp], C.c_int),
     ("rtmb_ricker", [_u32, C.c_float, C.c_float, _fp], C.c_int),
@@ -164,6 +166,18 @@ class Context:
     @property
     def launches(self) -> int:
         return int(self.L.rtmb_launch_count(self.h))
+
+    PROF_NAMES = ("model", "forward", "backward_source", "backward_receiver", "other")
+
+    def profile(self, enable: bool = True) -> None:
+        """Time every driver launch with CUDA events (per category); enabling clears the totals."""
+        self._check(self.L.rtmb_profile(self.h, int(enable)))
+
+    def profile_read(self) -> dict:
+        ms = (C.c_double * 5)()
+        n = (C.c_uint64 * 5)()
+        self._check(self.L.rtmb_profile_read(self.h, ms, n))
+        return {name: {"ms": ms[k], "launches": int(n[k])} for k, name in enumerate(self.PROF_NAMES)}
 
     def set_stream(self, stream) -> None:
         self._check(self.L.rtmb_set_stream(self.h, stream))
