@@ -91,6 +91,8 @@ typedef struct rtmb_ctx rtmb_ctx;
 int rtmb_create(const rtmb_params *params, rtmb_ctx **out);
 /* Replaces RTMGPUPlatform::destroyRTMPlatform (:16-21); frees every context-owned buffer. */
 int rtmb_destroy(rtmb_ctx *ctx);
+/* Description of the last failure of this context; with NULL, of the calling thread's last failed
+ * call that takes no context (rtmb_model_shot_noalloc). */
 const char *rtmb_last_error(const rtmb_ctx *ctx);
 /* Run subsequent work on this cudaStream_t (NULL = the context's own stream). */
 int rtmb_set_stream(rtmb_ctx *ctx, void *cuda_stream);
@@ -172,6 +174,25 @@ int rtmb_model_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, float 
  * overwritten (the reference's shotImage). */
 int rtmb_migrate_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const float *rec,
                       float *img);
+/* Modeling without any device allocation.  This entry point has no counterpart in the reference.
+ * It is for callers that cannot call cudaMalloc, for example a host framework whose allocator has
+ * reserved the GPU's memory up front and must account for every byte, or a latency-sensitive loop
+ * that cannot afford cudaMalloc's implicit device synchronisation.  It runs the same shot as
+ * rtmb_model_shot, with the same kernels and results, but creates no context: the caller passes
+ * v2dt2 (padded, device) and rec (device, file layout) and the stream (NULL: the legacy default
+ * stream), and every other buffer lives in one 64 MiB device array inside the library that each GPU
+ * loading the library holds until the process exits.  Grids up to about 8.3 million padded points
+ * fit (two wavefields plus small tables); larger ones are rejected with RTMB_EINVAL.
+ *   - The first call on a device looks up that array's address (once per device, with the device
+ *     current); make that first call before any stream capture on the device.
+ *   - All calls on a device share the array and it keeps the previous call's contents; the entry
+ *     point clears what must start at zero.  Calls that overlap on the GPU (several host threads or
+ *     streams) race on it and must be serialised by the caller.
+ *   - It allocates no device memory and calls no allocating library routine.  On failure,
+ *     rtmb_last_error(NULL) describes the error (per host thread). */
+int rtmb_model_shot_noalloc(const rtmb_params *params, const float *v2dt2, uint32_t sx, uint32_t sy,
+                            uint32_t sz, float *rec, void *cuda_stream);
+
 /* Host-buffer forms: copy in, run, copy out, return when the result is on the host. */
 int rtmb_model_shot_host(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, float *rec_host);
 int rtmb_migrate_shot_host(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz,

@@ -8,37 +8,8 @@
 
 #include <cuda_runtime.h>
 
+#include "ctx.hpp"
 #include "ops.cuh"
-#include "rtm3d_b200.h"
-#include "stencil.cuh"
-
-struct rtmb_ctx {
-    rtmb_params p{};
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    cudaStream_t own_stream = nullptr;
-    int nxe = 0, nye = 0, nze = 0, h = 0;
-    size_t n = 0;
-    float coefs[3 * (rtmb::kMaxOrder + 1)] = {};
-    float *d_taper = nullptr, *d_wavelet = nullptr;
-    unsigned *d_err = nullptr;
-    // driver state
-    float *d_v2dt2 = nullptr;
-    float *d_w[4] = {};          // source pair, receiver pair
-    float *d_quirk[3] = {};      // front-right taper side buffers (modeling)
-    float *d_upb = nullptr;      // [nt][nxe][nye][h] (HBC)
-    float *d_rec = nullptr, *d_img = nullptr;  // staging for the host-buffer forms
-    int chunk = 0;
-    uint64_t launches = 0;
-    std::string err;
-    // optional per-kernel timing of the drivers (rtmb_profile): an event pair around each launch
-    bool prof = false;
-    std::vector<cudaEvent_t> ev;        // pool, two per recorded launch
-    std::vector<int> ev_cat;            // category of each recorded launch
-    size_t ev_used = 0;
-    double prof_ms[RTMB_PROF_CATEGORIES] = {};
-    uint64_t prof_n[RTMB_PROF_CATEGORIES] = {};
-};
 
 namespace {
 
@@ -151,7 +122,9 @@ rtmb::StepArgs base_args(const rtmb_ctx *c) {
 bool exact(const rtmb_ctx *c) { return !(c->p.flags & RTMB_FLAG_FAST_FMA); }
 bool tma_ok(const rtmb_ctx *c) { return !(c->p.flags & RTMB_FLAG_NO_TMA); }
 
-int check_err_flag(rtmb_ctx *ctx) {
+}  // namespace
+
+int rtmb::driver::check_err_flag(rtmb_ctx *ctx) {
     unsigned h = 0;
     CK(cudaMemcpyAsync(&h, ctx->d_err, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -164,6 +137,9 @@ int check_err_flag(rtmb_ctx *ctx) {
     }
     return RTMB_OK;
 }
+
+namespace {
+using rtmb::driver::check_err_flag;
 
 int ensure(rtmb_ctx *ctx, float **buf, size_t count, bool zero) {
     if (!*buf) {
@@ -198,9 +174,12 @@ void set_receivers(rtmb::StepArgs &a, const rtmb_ctx *c, int mode, float *rec, i
     a.rec_base = (long long)(it / ntstep) * r.rcx * r.rcy * ntstep + (it % ntstep);
 }
 
+}  // namespace
+
 // Forward time loop shared by modeling and the migration forward pass.  Leaves the last two
-// wavefields in (*P, *PP) raw (untapered): *P = u(nt-1), *PP = u(nt).
-int run_forward(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, int taper_mode, float *rec,
+// wavefields in (*P, *PP) raw (untapered): *P = u(nt-1), *PP = u(nt).  Every buffer it uses must
+// already be set in the context except the taper side buffers, which it allocates when missing.
+int rtmb::driver::run_forward(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, int taper_mode, float *rec,
                 float *upb, float **P_out, float **PP_out, int cat) {
     const rtmb_params &p = ctx->p;
     const size_t nb = ctx->n * sizeof(float);
@@ -235,6 +214,9 @@ int run_forward(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, int taper_
     return RTMB_OK;
 }
 
+namespace {
+using rtmb::driver::run_forward;
+
 int alloc_driver(rtmb_ctx *ctx) {
     for (int k = 0; k < 4; ++k) {
         int rc = ensure(ctx, &ctx->d_w[k], ctx->n, false);
@@ -245,11 +227,41 @@ int alloc_driver(rtmb_ctx *ctx) {
 
 }  // namespace
 
+namespace {
+thread_local std::string g_noctx_error = "null context";
+}  // namespace
+
+void rtmb::driver::init_geometry(rtmb_ctx *ctx) {
+    const rtmb_params &p = ctx->p;
+    ctx->h = (int)p.stencil_order / 2;
+    ctx->nxe = (int)(p.nx + 2 * p.blen);
+    ctx->nye = (int)(p.ny + 2 * p.blen);
+    ctx->nze = (int)(p.nz + 2 * p.blen);
+    ctx->n = (size_t)ctx->nxe * ctx->nye * ctx->nze;
+    const int nxi = ctx->nxe - 2 * ctx->h, nyi = ctx->nye - 2 * ctx->h;
+    const int tiles = ((ctx->nze + rtmb::kTZ - 1) / rtmb::kTZ) * ((nyi + rtmb::kTY - 1) / rtmb::kTY);
+    ctx->chunk = pick_chunk(nxi > 0 ? nxi : 1, tiles > 0 ? tiles : 1);
+    rtmb_stencil_coefs(p.stencil_order, p.dx, p.dy, p.dz, ctx->coefs);
+}
+
+int rtmb::driver::check_model_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz) {
+    int rc = check_shot(ctx, sx, sy, sz);
+    if (rc) return rc;
+    if (ctx->p.receiver_depth_z + ctx->p.blen >= (uint32_t)ctx->nze - ctx->h)
+        return fail(ctx, RTMB_EINVAL, "receiver depth outside the computed region");
+    return RTMB_OK;
+}
+
+int rtmb::driver::fail_noctx(int code, const char *msg) {
+    g_noctx_error = msg;
+    return code;
+}
+
 extern "C" {
 
 int rtmb_abi_version(void) { return RTMB_ABI_VERSION; }
 
-const char *rtmb_last_error(const rtmb_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+const char *rtmb_last_error(const rtmb_ctx *ctx) { return ctx ? ctx->err.c_str() : g_noctx_error.c_str(); }
 
 uint64_t rtmb_launch_count(const rtmb_ctx *ctx) { return ctx ? ctx->launches : 0; }
 
@@ -262,14 +274,7 @@ int rtmb_create(const rtmb_params *params, rtmb_ctx **out) {
     if (!p.ntstep || p.nt % p.ntstep) return RTMB_EINVAL;  // RTMParam.cpp:241-245 rejects nt < ntstep
     rtmb_ctx *ctx = new rtmb_ctx;
     ctx->p = p;
-    ctx->h = (int)p.stencil_order / 2;
-    ctx->nxe = (int)(p.nx + 2 * p.blen);
-    ctx->nye = (int)(p.ny + 2 * p.blen);
-    ctx->nze = (int)(p.nz + 2 * p.blen);
-    ctx->n = (size_t)ctx->nxe * ctx->nye * ctx->nze;
-    const int nxi = ctx->nxe - 2 * ctx->h, nyi = ctx->nye - 2 * ctx->h;
-    const int tiles = ((ctx->nze + rtmb::kTZ - 1) / rtmb::kTZ) * ((nyi + rtmb::kTY - 1) / rtmb::kTY);
-    ctx->chunk = pick_chunk(nxi > 0 ? nxi : 1, tiles > 0 ? tiles : 1);
+    rtmb::driver::init_geometry(ctx);
     auto bail = [&](int code) {
         rtmb_destroy(ctx);
         return code;
@@ -283,7 +288,6 @@ int rtmb_create(const rtmb_params *params, rtmb_ctx **out) {
     ctx->device = dev;
     if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) return bail(RTMB_ECUDA);
     ctx->stream = ctx->own_stream;
-    rtmb_stencil_coefs(p.stencil_order, p.dx, p.dy, p.dz, ctx->coefs);
     float *tap = new float[p.blen > 0 ? p.blen : 1];
     float *wav = new float[p.nt];
     rtmb_taper_vector(p.blen, p.taper_factor, tap);
@@ -441,10 +445,8 @@ int rtmb_load_v2dt2(rtmb_ctx *ctx, const float *v2dt2, int from_host) {
 
 int rtmb_model_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, float *rec) {
     if (!ctx || !rec) return fail(ctx, RTMB_EINVAL, "rtmb_model_shot: null pointer");
-    int rc = check_shot(ctx, sx, sy, sz);
+    int rc = rtmb::driver::check_model_shot(ctx, sx, sy, sz);
     if (rc) return rc;
-    if (ctx->p.receiver_depth_z + ctx->p.blen >= (uint32_t)ctx->nze - ctx->h)
-        return fail(ctx, RTMB_EINVAL, "receiver depth outside the computed region");
     if ((rc = alloc_driver(ctx))) return rc;
     float *P, *PP;
     // RTMFiniteDifferencesKernel.cpp:169-216: taper all faces, step, inject, sample.

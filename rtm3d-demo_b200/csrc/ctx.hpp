@@ -1,0 +1,56 @@
+// ctx.hpp -- the library's context object and the driver helpers shared by api.cu and noalloc.cu.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "rtm3d_b200.h"
+#include "stencil.cuh"
+
+struct rtmb_ctx {
+    rtmb_params p{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    int nxe = 0, nye = 0, nze = 0, h = 0;
+    size_t n = 0;
+    float coefs[3 * (rtmb::kMaxOrder + 1)] = {};
+    float *d_taper = nullptr, *d_wavelet = nullptr;
+    unsigned *d_err = nullptr;
+    // driver state
+    float *d_v2dt2 = nullptr;
+    float *d_w[4] = {};          // source pair, receiver pair
+    float *d_quirk[3] = {};      // front-right taper side buffers (modeling)
+    float *d_upb = nullptr;      // [nt][nxe][nye][h] (HBC)
+    float *d_rec = nullptr, *d_img = nullptr;  // staging for the host-buffer forms
+    int chunk = 0;
+    uint64_t launches = 0;
+    std::string err;
+    // optional per-kernel timing of the drivers (rtmb_profile): an event pair around each launch
+    bool prof = false;
+    std::vector<cudaEvent_t> ev;        // pool, two per recorded launch
+    std::vector<int> ev_cat;            // category of each recorded launch
+    size_t ev_used = 0;
+    double prof_ms[RTMB_PROF_CATEGORIES] = {};
+    uint64_t prof_n[RTMB_PROF_CATEGORIES] = {};
+};
+
+namespace rtmb {
+namespace driver {
+
+// Forward time loop shared by modeling and the migration forward pass (see api.cu).
+int run_forward(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, int taper_mode, float *rec,
+                float *upb, float **P_out, float **PP_out, int cat);
+// Reads and clears the device error flag after synchronising the context's stream.
+int check_err_flag(rtmb_ctx *ctx);
+// Fills the derived sizes and the host copy of the stencil coefficients of a context.
+void init_geometry(rtmb_ctx *ctx);
+// Argument checks of a modeling shot (source inside the model, receivers inside the computed region).
+int check_model_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz);
+// Records a message for a call that has no context (rtmb_last_error(NULL) returns it).
+int fail_noctx(int code, const char *msg);
+
+}  // namespace driver
+}  // namespace rtmb

@@ -6,6 +6,7 @@
 #include <cstring>
 #include <vector>
 
+#include "host_math.hpp"
 #include "rtm3d_b200.h"
 
 namespace {
@@ -149,6 +150,13 @@ void borders_rbc(float *ve, int nx, int ny, int nz, int b) {
 
 }  // namespace
 
+float rtmb::ricker_sample(uint32_t it, float dt, float fpeak) {
+    const float t = static_cast<float>(static_cast<double>(static_cast<float>(it) * dt) - 1.0 / fpeak);
+    const float x = static_cast<float>(M_PI * fpeak * t);
+    const float xx = x * x;
+    return static_cast<float>(static_cast<double>(std::exp(-xx)) * (1.0 - 2.0 * xx));
+}
+
 extern "C" {
 
 int rtmb_stencil_coefs(uint32_t order, float dx, float dy, float dz, float *out) {
@@ -175,12 +183,7 @@ int rtmb_taper_vector(uint32_t blen, float taper_factor, float *out) {
 
 int rtmb_ricker(uint32_t nt, float dt, float fpeak, float *out) {
     if (!out && nt) return RTMB_EINVAL;
-    for (uint32_t it = 0; it < nt; ++it) {
-        const float t = static_cast<float>(static_cast<double>(static_cast<float>(it) * dt) - 1.0 / fpeak);
-        const float x = static_cast<float>(M_PI * fpeak * t);
-        const float xx = x * x;
-        out[it] = static_cast<float>(static_cast<double>(std::exp(-xx)) * (1.0 - 2.0 * xx));
-    }
+    for (uint32_t it = 0; it < nt; ++it) out[it] = rtmb::ricker_sample(it, dt, fpeak);
     return RTMB_OK;
 }
 

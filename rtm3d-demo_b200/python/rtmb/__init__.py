@@ -91,6 +91,7 @@ SYMBOLS = [
     ("rtmb_migrate_shot", [_vp, _u32, _u32, _u32, _vp, _vp], C.c_int),
     ("rtmb_model_shot_host", [_vp, _u32, _u32, _u32, _vp], C.c_int),
     ("rtmb_migrate_shot_host", [_vp, _u32, _u32, _u32, _vp, _vp], C.c_int),
+    ("rtmb_model_shot_noalloc", [C.POINTER(Params), _vp, _u32, _u32, _u32, _vp, _vp], C.c_int),
 ]
 
 _LIB = None
@@ -234,6 +235,15 @@ class Context:
 
     def migrate_shot_host(self, sx, sy, sz, rec_host, img_host):
         self._check(self.L.rtmb_migrate_shot_host(self.h, sx, sy, sz, _ptr(rec_host), _ptr(img_host)))
+
+
+def model_shot_noalloc(params: Params, v2dt2, sx: int, sy: int, sz: int, rec, stream=None) -> None:
+    """Modeling through rtmb_model_shot_noalloc: no context and no device allocation (v2dt2 and rec
+    are device buffers the caller owns; the library's fixed 64 MiB scratch holds everything else)."""
+    L = load()
+    rc = L.rtmb_model_shot_noalloc(C.byref(params), _ptr(v2dt2), sx, sy, sz, _ptr(rec), stream)
+    if rc != RTMB_OK:
+        raise RtmbError(rc, L.rtmb_last_error(None).decode())
 
 
 # host-side tables (no GPU needed) ----------------------------------------------
