@@ -11,13 +11,15 @@
 //     register queue of x taps) until the plane is computed H planes later (y and z taps);
 //   * the core ring (R slots): the PP and v2dt2 tiles (and PS and IMG for the imaging form) of the
 //     plane being computed.
-// One block barrier per plane keeps the warps in step and releases the slots of the previous
-// plane, which the producer refills at once, D-H-1 planes (P) and R-1 planes (core) ahead of their
-// use.  Each thread keeps the 2H+1 x taps of its four points in a register queue that shifts by one
-// plane per iteration.
+// The CTA has eight consumer warps and one producer warp.  Lane 0 of the producer warp issues the
+// loads in order; each slot is refilled once its "empty" mbarrier shows that all eight consumer warps
+// have released it, so loads run up to D-H-1 planes (P) and R-1 planes (core) ahead and no consumer
+// ever waits at a block barrier (the taper forms add a consumer-only named barrier per tapered
+// plane).  Each thread keeps the 2H+1 x taps of its four points in a register queue that shifts by
+// one plane per iteration.
 //
-// Every wait is bounded (about two seconds): a wait that runs out sets error bit 2 and the CTA stops,
-// after waiting, again bounded, for the copies it issued.
+// Every wait is bounded (about two seconds): a wait that runs out sets error bit 2 and the warp
+// stops; the producer waits, again bounded, for the copies it issued before it exits.
 #pragma once
 #include <cuda.h>
 
@@ -72,6 +74,19 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
 
 __device__ __forceinline__ float4 ld_f4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 
+// Barrier 1 over the kThreads consumer threads only (the producer warp never joins it).
+__device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kThreads) : "memory"); }
+__device__ __forceinline__ bool consumer_sync_or(bool v) {
+    uint32_t out;
+    asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, 1, %2, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+                 : "=r"(out)
+                 : "r"((uint32_t)v), "n"(kThreads)
+                 : "memory");
+    return out != 0;
+}
+
+constexpr int kTmaThreads = kThreads + 32;  // eight consumer warps and one producer warp
+
 // Tensor maps of one launch.  p: box {TZ + 2ZH, TY + 2H, 1}; the others: box {TZ, TY, 1}.
 struct TmaMaps {
     CUtensorMap p, pp, v, ps, img;
@@ -90,12 +105,12 @@ struct TmaShape {
     static constexpr int R = IMG ? 3 : 4;                    // core slots
     static_assert(2 * H <= D && D >= H + 2, "warm-up planes and the lookahead must fit in the P ring");
     static constexpr size_t SMEM =
-        ((size_t)D * STRIDE + (size_t)R * NCORE * CORE) * sizeof(float) + (D + R) * sizeof(uint64_t);
+        ((size_t)D * STRIDE + (size_t)R * NCORE * CORE) * sizeof(float) + 2 * (D + R) * sizeof(uint64_t);
 };
 
 // TAPER: kTaperNone / kTaperUpper / kTaperAll.  IMG: the epilogue accumulates the image.
 template <int H, bool EXACT, int TAPER, bool IMG>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kTmaThreads, 2)
     tma_step_kernel(const __grid_constant__ TmaMaps maps, const __grid_constant__ StepArgs a) {
     using S = TmaShape<H, IMG>;
     constexpr int ZH = S::ZH, SPITCH = S::SPITCH, STAGE = S::STAGE, STRIDE = S::STRIDE, D = S::D, R = S::R;
@@ -107,6 +122,9 @@ __global__ void __launch_bounds__(kThreads, 2)
     float *cring = smem + D * STRIDE;
     uint64_t *pfull = reinterpret_cast<uint64_t *>(cring + R * NCORE * CORE);
     uint64_t *cfull = pfull + D;
+    uint64_t *pempty = cfull + R;
+    uint64_t *cempty = pempty + D;
+    constexpr int NCW = kThreads / 32;  // consumer warps
 
     const int tid = threadIdx.x;
     const int tz = tid % ZQ, ty = tid / ZQ;
@@ -122,40 +140,47 @@ __global__ void __launch_bounds__(kThreads, 2)
     const size_t plane = (size_t)a.nye * a.nze;
 
     if (tid == 0) {
-        for (int s = 0; s < D; ++s) mbar_init(&pfull[s], 1);
-        for (int s = 0; s < R; ++s) mbar_init(&cfull[s], 1);
+        for (int s = 0; s < D; ++s) { mbar_init(&pfull[s], 1); mbar_init(&pempty[s], NCW); }
+        for (int s = 0; s < R; ++s) { mbar_init(&cfull[s], 1); mbar_init(&cempty[s], NCW); }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    __syncthreads();
+    __syncthreads();  // the last block-wide barrier: the producer warp leaves below
 
-    // ---- producer (thread 0): loads are issued in order, each after a block barrier has released
-    // its slot
-    int p_issued = 0, c_issued = 0;  // next P plane / next core plane to issue
-    auto issue_p = [&](int upto) {
-        for (; p_issued <= upto && p_issued < nplanes; ++p_issued) {
-            const int k = p_issued, s = k % D;
+    if (tid >= kThreads) {
+        // ---- producer: P plane k into slot k % D once plane k - D has been released; the core
+        // tiles of output plane i = k - 2H right after, once core plane i - R has been released
+        if (tid != kThreads) return;
+        bool ok = true;
+        int p_issued = 0, c_issued = 0;
+        for (int k = 0; k < nplanes && ok; ++k) {
+            const int s = k % D;
+            if (k >= D && !(ok = mbar_wait(&pempty[s], ((k / D) + 1) & 1))) break;
             mbar_expect_tx(&pfull[s], STAGE * sizeof(float));
             tma_load_3d(pring + s * STRIDE, &maps.p, &pfull[s], zt0 - ZH, yt0 - H, xc0 - H + k);
-        }
-    };
-    auto issue_c = [&](int upto) {
-        for (; c_issued <= upto && c_issued < n; ++c_issued) {
-            const int i = c_issued, s = i % R;
-            float *dst = cring + s * NCORE * CORE;
-            mbar_expect_tx(&cfull[s], NCORE * CORE * sizeof(float));
-            tma_load_3d(dst, &maps.pp, &cfull[s], zt0, yt0, xc0 + i);
-            tma_load_3d(dst + CORE, &maps.v, &cfull[s], zt0, yt0, xc0 + i);
-            if (IMG) {
-                tma_load_3d(dst + 2 * CORE, &maps.ps, &cfull[s], zt0, yt0, xc0 + i);
-                tma_load_3d(dst + 3 * CORE, &maps.img, &cfull[s], zt0, yt0, xc0 + i);
+            p_issued = k + 1;
+            if (k >= 2 * H) {
+                const int i = k - 2 * H, cs = i % R;
+                if (i >= R && !(ok = mbar_wait(&cempty[cs], ((i / R) + 1) & 1))) break;
+                float *dst = cring + cs * NCORE * CORE;
+                mbar_expect_tx(&cfull[cs], NCORE * CORE * sizeof(float));
+                tma_load_3d(dst, &maps.pp, &cfull[cs], zt0, yt0, xc0 + i);
+                tma_load_3d(dst + CORE, &maps.v, &cfull[cs], zt0, yt0, xc0 + i);
+                if (IMG) {
+                    tma_load_3d(dst + 2 * CORE, &maps.ps, &cfull[cs], zt0, yt0, xc0 + i);
+                    tma_load_3d(dst + 3 * CORE, &maps.img, &cfull[cs], zt0, yt0, xc0 + i);
+                }
+                c_issued = i + 1;
             }
         }
-    };
-    if (tid == 0) {
-        issue_p(D - 1);
-        issue_c(R - 1);
+        if (!ok && a.err) atomicOr(a.err, 2u);
+        // stay until every copy this CTA issued has landed (bounded), so none outlives the CTA
+        for (int k = p_issued > D ? p_issued - D : 0; k < p_issued; ++k)
+            if (!mbar_wait(&pfull[k % D], (k / D) & 1)) break;
+        for (int i = c_issued > R ? c_issued - R : 0; i < c_issued; ++i)
+            if (!mbar_wait(&cfull[i % R], (i / R) & 1)) break;
+        return;
     }
-    // (planes D .. D+H-1 follow once the warm-up planes 0 .. H-1 are in the queue)
+    const int lane = tid & 31;
 
     // ---- per-thread constants, hoisted out of the plane loop
     const bool row_ok = y < a.nye && z0 < a.nze;
@@ -197,14 +222,15 @@ __global__ void __launch_bounds__(kThreads, 2)
     const int ccol = ty * kTZ + tz * kVZ;  // this thread's offset in a core tile
 
     bool bad_wait = false;
-    int kdone = 0;  // P planes whose wait succeeded, in order
     auto wait_p = [&](int k) {  // warp-uniform outcome, so a warp never splits at a timeout
-        const bool ok = __all_sync(0xffffffffu, mbar_wait(&pfull[k % D], (k / D) & 1));
-        if (ok && !bad_wait) kdone = k + 1;
-        bad_wait |= !ok;
+        bad_wait |= !__all_sync(0xffffffffu, mbar_wait(&pfull[k % D], (k / D) & 1));
     };
-    // taper of the tile of P plane k, in place (TAPER forms).  The pass is collective: every thread
-    // tapers a share of the tile, so it ends with a block barrier.
+    auto release_p = [&](int k) {  // this warp no longer reads P plane k
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&pempty[k % D]);
+    };
+    // taper of the tile of P plane k, in place (TAPER forms).  The pass is collective: every consumer
+    // thread tapers a share of the tile, so it ends with the consumer barrier.
     auto taper_stage = [&](int k) {
         const int x = xc0 - H + k;
         bool need;
@@ -228,7 +254,9 @@ __global__ void __launch_bounds__(kThreads, 2)
             }
             st[c] = v;
         }
-        __syncthreads();
+        // the slot is refilled by TMA later: order these generic-proxy writes before that
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        consumer_sync();
     };
 
     float4 q[NQ];
@@ -238,27 +266,20 @@ __global__ void __launch_bounds__(kThreads, 2)
         wait_p(k);
         if (TAPER != kTaperNone) taper_stage(k);
     }
+    if (bad_wait) goto drain;
 #pragma unroll
     for (int k = 0; k < 2 * H; ++k) q[k + 1] = ld_f4(pring + (k % D) * STRIDE + (ty + H) * SPITCH + col);
-    if (__syncthreads_or(bad_wait)) goto drain;
-    if (tid == 0) issue_p(H + D - 1);  // planes 0 .. H-1 were only needed for the queue
+#pragma unroll
+    for (int k = 0; k < H; ++k) release_p(k);  // planes 0 .. H-1 were only needed for the queue
 
 #pragma unroll 1
     for (int i = 0; i < n; ++i) {
         {
             const int x = xc0 + i;
-            if (i > 0) {
-                // every warp is done with plane i-1: its P and core slots are free
-                if (__syncthreads_or(bad_wait)) goto drain;
-                if (tid == 0) {
-                    issue_p(i - 1 + H + D);
-                    issue_c(i - 1 + R);
-                }
-            }
             const int kin = i + 2 * H;
             wait_p(kin);
             if (TAPER != kTaperNone) {
-                if (__syncthreads_or(bad_wait)) goto drain;  // the taper pass is collective
+                if (consumer_sync_or(bad_wait)) goto drain;  // the taper pass is collective
                 taper_stage(kin);
             } else if (bad_wait) {
                 goto drain;  // a timed-out wait leaves the data undefined; stop without computing
@@ -313,6 +334,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                     }
                 }
             }
+            release_p(i + H);  // the tile of plane x is no longer read
             // core tiles of plane x
             const int cs = i % R;
             if (!__all_sync(0xffffffffu, mbar_wait(&cfull[cs], (i / R) & 1))) {
@@ -323,6 +345,8 @@ __global__ void __launch_bounds__(kThreads, 2)
             const float4 pp_raw = ld_f4(ct), vv = ld_f4(ct + CORE);
             float4 ps4 = pp_raw, im4 = pp_raw;
             if (IMG) { ps4 = ld_f4(ct + 2 * CORE); im4 = ld_f4(ct + 3 * CORE); }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&cempty[cs]);
             if (!row_ok) continue;
 
             const float4 qc = q[H];
@@ -407,14 +431,8 @@ __global__ void __launch_bounds__(kThreads, 2)
     return;
 
 drain:
-    // A wait ran out: record it, then wait (bounded) for the copies thread 0 issued.
+    // A wait ran out: record it and stop this warp (the producer outlives the copies it issued).
     if (a.err) atomicOr(a.err, 2u);
-    if (tid == 0) {
-        for (int k = kdone; k < p_issued; ++k)
-            if (!mbar_wait(&pfull[k % D], (k / D) & 1)) break;
-        for (int i = (c_issued > R ? c_issued - R : 0); i < c_issued; ++i)
-            if (!mbar_wait(&cfull[i % R], (i / R) & 1)) break;
-    }
 }
 
 template <int H>
@@ -432,7 +450,7 @@ cudaError_t launch_tma_h(const TmaMaps &maps, const StepArgs &a, bool exact, int
             if (e != cudaSuccess) return e;
             attr_done[variant] |= bit;
         }
-        kern<<<grid, kThreads, smem, s>>>(maps, a);
+        kern<<<grid, kTmaThreads, smem, s>>>(maps, a);
         return cudaGetLastError();
     };
 #define RTMB_TMA_CASE(EX, TP, IM) \
