@@ -65,6 +65,18 @@ typedef enum rtmb_boundary { RTMB_BC_ABC = 1, RTMB_BC_HBC = 2, RTMB_BC_RBC = 3 }
 #define RTMB_FLAG_USE_GRAPH     0x10u /* capture each time loop in a CUDA graph */
 #define RTMB_FLAG_NO_TMA        0x20u /* use the plain-load step kernel even when rows are 16-byte
                                          aligned (the TMA-pipelined kernel is the default then) */
+/* Storage forms of the per-shot drivers (no reference counterpart; the reference stores FP32).
+ * The wavefields the drivers own (source and receiver pairs) are stored as FP16 or BF16 holding
+ * value * 2^-e, with one power-of-two exponent per stored time level chosen from the previous
+ * levels' max |value| so that no level overflows; all stencil arithmetic stays FP32.  The record,
+ * v2dt2 and the caller's image stay FP32.  Needs stencil_order 8 and nz + 2*blen a multiple of 8,
+ * boundary RBC for migration (modeling tapers every face as usual); the per-operator entry
+ * points ignore these flags. */
+#define RTMB_FLAG_STORE_F16     0x40u
+#define RTMB_FLAG_STORE_BF16    0x80u
+/* With a storage flag: accumulate the image over the time steps in FP64 (the caller's FP32 image
+ * is written from it at the end of the shot). */
+#define RTMB_FLAG_IMG_F64       0x100u
 
 /* The input.json parameters on the path (include/RTMParam.hpp:188-249). */
 typedef struct rtmb_params {
@@ -192,6 +204,23 @@ int rtmb_migrate_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, cons
  *     rtmb_last_error(NULL) describes the error (per host thread). */
 int rtmb_model_shot_noalloc(const rtmb_params *params, const float *v2dt2, uint32_t sx, uint32_t sy,
                             uint32_t sz, float *rec, void *cuda_stream);
+
+/* rtmb_migrate_shot that ADDS the shot's image to a caller-owned FP64 stack (padded, device)
+ * instead of writing an FP32 image: the shot stacking of RTMAcousticController.cpp:223-242 with an
+ * FP64 accumulator.  With a storage flag the time accumulation runs in FP64 directly into the
+ * stack; with FP32 storage the FP32 shot image is added to it.  No reference counterpart. */
+int rtmb_migrate_shot_acc64(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const float *rec,
+                            double *stack);
+
+/* FP64 GPU oracle (no reference counterpart): the reference's operator sequence of
+ * RTMFiniteDifferencesKernel::rtmModel and RTMHBCKernel/RTMRBCKernel::rtmMigrate, one launch per
+ * operator, in double precision on the same discrete scheme (the FP32 stencil coefficients, taper
+ * factors, Ricker samples and v2dt2, widened).  It is the yardstick for the error of the FP32 and
+ * 16-bit forms, not a fast path.  rec (model): double record in file layout; img (migrate): padded
+ * double image, overwritten; both device pointers.  Ignores the storage and FMA flags. */
+int rtmb_model_shot_f64(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, double *rec);
+int rtmb_migrate_shot_f64(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const float *rec,
+                          double *img);
 
 /* Host-buffer forms: copy in, run, copy out, return when the result is on the host. */
 int rtmb_model_shot_host(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, float *rec_host);

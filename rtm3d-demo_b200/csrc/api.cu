@@ -1,4 +1,5 @@
 // api.cu -- context, C ABI entry points and the per-shot time-loop drivers of librtm3d_b200.
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -141,12 +142,38 @@ int rtmb::driver::check_err_flag(rtmb_ctx *ctx) {
 namespace {
 using rtmb::driver::check_err_flag;
 
-int ensure(rtmb_ctx *ctx, float **buf, size_t count, bool zero) {
+int ensure_bytes(rtmb_ctx *ctx, void **buf, size_t bytes, bool zero) {
     if (!*buf) {
-        CK(cudaMalloc(buf, count * sizeof(float)));
-        if (zero) CK(cudaMemsetAsync(*buf, 0, count * sizeof(float), ctx->stream));
+        CK(cudaMalloc(buf, bytes));
+        if (zero) CK(cudaMemsetAsync(*buf, 0, bytes, ctx->stream));
     }
     return RTMB_OK;
+}
+
+int ensure(rtmb_ctx *ctx, float **buf, size_t count, bool zero) {
+    return ensure_bytes(ctx, reinterpret_cast<void **>(buf), count * sizeof(float), zero);
+}
+
+size_t wave_bytes(const rtmb_ctx *c) { return c->n * (c->store == rtmb::kStoreF32 ? sizeof(float) : 2); }
+
+// Scale records of the storage forms: a pool of 3 nt + 8 records per shot (forward levels, rebuilt
+// source levels, receiver levels), cleared at the start of each shot.
+int reset_scales(rtmb_ctx *ctx) {
+    const int need = 3 * (int)ctx->p.nt + 8;
+    if (ctx->sc_cap < need) {
+        if (ctx->d_scale) CK(cudaFree(ctx->d_scale));
+        ctx->d_scale = nullptr;
+        ctx->sc_cap = 0;
+        CK(cudaMalloc(&ctx->d_scale, need * sizeof(rtmb::ScaleRec)));
+        ctx->sc_cap = need;
+    }
+    CK(cudaMemsetAsync(ctx->d_scale, 0, ctx->sc_cap * sizeof(rtmb::ScaleRec), ctx->stream));
+    ctx->sc_next = 0;
+    return RTMB_OK;
+}
+
+rtmb::ScaleRec *new_scale(rtmb_ctx *ctx) {
+    return ctx->sc_next < ctx->sc_cap ? ctx->d_scale + ctx->sc_next++ : nullptr;
 }
 
 int check_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz) {
@@ -180,9 +207,10 @@ void set_receivers(rtmb::StepArgs &a, const rtmb_ctx *c, int mode, float *rec, i
 // wavefields in (*P, *PP) raw (untapered): *P = u(nt-1), *PP = u(nt).  Every buffer it uses must
 // already be set in the context except the taper side buffers, which it allocates when missing.
 int rtmb::driver::run_forward(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, int taper_mode, float *rec,
-                float *upb, float **P_out, float **PP_out, int cat) {
+                float *upb, float **P_out, float **PP_out, int cat, rtmb::ScaleRec **sc_out) {
     const rtmb_params &p = ctx->p;
-    const size_t nb = ctx->n * sizeof(float);
+    const size_t nb = wave_bytes(ctx);
+    const bool st = ctx->store != rtmb::kStoreF32;
     float *P = ctx->d_w[0], *PP = ctx->d_w[1];
     CK(cudaMemsetAsync(P, 0, nb, ctx->stream));
     CK(cudaMemsetAsync(PP, 0, nb, ctx->stream));
@@ -200,17 +228,30 @@ int rtmb::driver::run_forward(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t 
     a.taper_mode = taper_mode;
     a.quirk = quirk;
     a.sxe = (int)(sx + p.blen); a.sye = (int)(sy + p.blen); a.sze = (int)(sz + p.blen);
+    a.store = ctx->store;
+    a.inj = ctx->wmax;
+    rtmb::ScaleRec *scP = nullptr, *scPP = nullptr;  // records of the levels in P and PP
+    if (st && (!(scP = new_scale(ctx)) || !(scPP = new_scale(ctx))))
+        return fail(ctx, RTMB_EINVAL, "scale record pool exhausted");
     const size_t upb_step = (size_t)ctx->nxe * ctx->nye * ctx->h;
     for (uint32_t it = 0; it < p.nt; ++it) {
         std::swap(P, PP);
+        std::swap(scP, scPP);
         a.P = P; a.PP = PP; a.it = (int)it;
+        rtmb::ScaleRec *lvl = nullptr;
+        if (st) {
+            if (!(lvl = new_scale(ctx))) return fail(ctx, RTMB_EINVAL, "scale record pool exhausted");
+            a.sc_p = scP; a.sc_pp = scPP; a.sc_out = lvl;
+        }
         if (rec) set_receivers(a, ctx, rtmb::kRecSample, rec, (int)it);
         if (upb) { a.upb_mode = rtmb::kUpbSave; a.upb = upb + (size_t)it * upb_step; }
         if (quirk) { a.quirk_in = ctx->d_quirk[(it + 1) % 3]; a.quirk_out = ctx->d_quirk[it % 3]; }
         LAUNCH_CAT(cat, rtmb::launch_step(a, (int)p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
+        if (st) scPP = lvl;
     }
     *P_out = P;
     *PP_out = PP;
+    if (sc_out) { sc_out[0] = scP; sc_out[1] = scPP; }
     return RTMB_OK;
 }
 
@@ -219,7 +260,11 @@ using rtmb::driver::run_forward;
 
 int alloc_driver(rtmb_ctx *ctx) {
     for (int k = 0; k < 4; ++k) {
-        int rc = ensure(ctx, &ctx->d_w[k], ctx->n, false);
+        int rc = ensure_bytes(ctx, reinterpret_cast<void **>(&ctx->d_w[k]), wave_bytes(ctx), false);
+        if (rc) return rc;
+    }
+    if (ctx->store != rtmb::kStoreF32) {
+        int rc = ensure(ctx, &ctx->d_inj, 2, true);
         if (rc) return rc;
     }
     return RTMB_OK;
@@ -272,8 +317,19 @@ int rtmb_create(const rtmb_params *params, rtmb_ctx **out) {
     if (!p.nx || !p.ny || !p.nz || p.stencil_order < 2 || p.stencil_order > 16 || (p.stencil_order & 1u))
         return RTMB_EINVAL;
     if (!p.ntstep || p.nt % p.ntstep) return RTMB_EINVAL;  // RTMParam.cpp:241-245 rejects nt < ntstep
+    const uint32_t sf = p.flags & (RTMB_FLAG_STORE_F16 | RTMB_FLAG_STORE_BF16);
+    if (sf == (RTMB_FLAG_STORE_F16 | RTMB_FLAG_STORE_BF16))
+        return rtmb::driver::fail_noctx(RTMB_EINVAL, "rtmb_create: choose one of RTMB_FLAG_STORE_F16 and _BF16");
+    if ((p.flags & RTMB_FLAG_IMG_F64) && !sf)
+        return rtmb::driver::fail_noctx(RTMB_EINVAL, "rtmb_create: RTMB_FLAG_IMG_F64 needs a 16-bit storage flag");
+    if (sf && !rtmb::storage_form_supported((int)p.stencil_order, (int)(p.nz + 2 * p.blen)))
+        return rtmb::driver::fail_noctx(RTMB_EINVAL,
+                                        "rtmb_create: the 16-bit storage forms need stencil_order 8 and nz + 2*blen "
+                                        "a multiple of 8");
     rtmb_ctx *ctx = new rtmb_ctx;
     ctx->p = p;
+    ctx->store = sf == RTMB_FLAG_STORE_F16 ? rtmb::kStoreF16 : (sf ? rtmb::kStoreBF16 : rtmb::kStoreF32);
+    ctx->img64 = (p.flags & RTMB_FLAG_IMG_F64) != 0;
     rtmb::driver::init_geometry(ctx);
     auto bail = [&](int code) {
         rtmb_destroy(ctx);
@@ -292,6 +348,7 @@ int rtmb_create(const rtmb_params *params, rtmb_ctx **out) {
     float *wav = new float[p.nt];
     rtmb_taper_vector(p.blen, p.taper_factor, tap);
     rtmb_ricker(p.nt, p.dt, p.fpeak, wav);
+    for (uint32_t i = 0; i < p.nt; ++i) ctx->wmax = std::fmax(ctx->wmax, std::fabs(wav[i]));
     bool ok = cudaMalloc(&ctx->d_taper, sizeof(float) * (p.blen > 0 ? p.blen : 1)) == cudaSuccess &&
               cudaMalloc(&ctx->d_wavelet, sizeof(float) * p.nt) == cudaSuccess &&
               cudaMalloc(&ctx->d_err, sizeof(unsigned)) == cudaSuccess &&
@@ -316,6 +373,12 @@ int rtmb_destroy(rtmb_ctx *ctx) {
     for (float *b : bufs)
         if (b) cudaFree(b);
     if (ctx->d_err) cudaFree(ctx->d_err);
+    if (ctx->d_scale) cudaFree(ctx->d_scale);
+    if (ctx->d_inj) cudaFree(ctx->d_inj);
+    if (ctx->d_img64) cudaFree(ctx->d_img64);
+    for (double *b : ctx->d_f64)
+        if (b) cudaFree(b);
+    if (ctx->d_upb64) cudaFree(ctx->d_upb64);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return RTMB_OK;
@@ -448,14 +511,21 @@ int rtmb_model_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, float 
     int rc = rtmb::driver::check_model_shot(ctx, sx, sy, sz);
     if (rc) return rc;
     if ((rc = alloc_driver(ctx))) return rc;
+    if (ctx->store != rtmb::kStoreF32 && (rc = reset_scales(ctx))) return rc;
     float *P, *PP;
     // RTMFiniteDifferencesKernel.cpp:169-216: taper all faces, step, inject, sample.
     if ((rc = run_forward(ctx, sx, sy, sz, rtmb::kTaperAll, rec, nullptr, &P, &PP, RTMB_PROF_MODEL))) return rc;
     return check_err_flag(ctx);
 }
 
-int rtmb_migrate_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const float *rec, float *img) {
-    if (!ctx || !rec || !img) return fail(ctx, RTMB_EINVAL, "rtmb_migrate_shot: null pointer");
+}  // extern "C"
+
+namespace {
+
+// The migration of one shot.  img_out: the caller's FP32 image (overwritten) or, with acc64, the
+// caller's FP64 stack (added to).
+int migrate_impl(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const float *rec, void *img_out,
+                 bool acc64) {
     int rc = check_shot(ctx, sx, sy, sz);
     if (rc) return rc;
     const rtmb_params &p = ctx->p;
@@ -463,55 +533,125 @@ int rtmb_migrate_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, cons
         return fail(ctx, RTMB_EINVAL, "migration boundary must be HBC or RBC");
     if (p.receiver_depth_z + p.blen >= (uint32_t)ctx->nze - ctx->h)
         return fail(ctx, RTMB_EINVAL, "receiver depth outside the computed region");
-    if ((rc = alloc_driver(ctx))) return rc;
+    const bool st = ctx->store != rtmb::kStoreF32;
+    if (!st && acc64) {
+        // FP32 storage: the FP32 shot image, then added to the FP64 stack
+        if ((rc = ensure(ctx, &ctx->d_img, ctx->n, false))) return rc;
+        if ((rc = migrate_impl(ctx, sx, sy, sz, rec, ctx->d_img, false))) return rc;
+        LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_stack64(static_cast<double *>(img_out), ctx->d_img, ctx->n, ctx->stream));
+        return check_err_flag(ctx);
+    }
     const bool hbc = p.boundary == RTMB_BC_HBC;
+    if (st && hbc) return fail(ctx, RTMB_EINVAL, "the 16-bit storage forms migrate with boundary RBC");
+    if ((rc = alloc_driver(ctx))) return rc;
+    if (st && (rc = reset_scales(ctx))) return rc;
     const size_t upb_step = (size_t)ctx->nxe * ctx->nye * ctx->h;
     if (hbc && (rc = ensure(ctx, &ctx->d_upb, upb_step * p.nt, true))) return rc;
 
     // forward pass (HBC.cpp:96-210 / RBC.cpp:54-144)
     float *sP, *sPP;
+    rtmb::ScaleRec *scs[2] = {nullptr, nullptr};
     if ((rc = run_forward(ctx, sx, sy, sz, hbc ? rtmb::kTaperUpper : rtmb::kTaperNone, nullptr,
-                          hbc ? ctx->d_upb : nullptr, &sP, &sPP, RTMB_PROF_FORWARD)))
+                          hbc ? ctx->d_upb : nullptr, &sP, &sPP, RTMB_PROF_FORWARD, scs)))
         return rc;
     // snap0 is P after its last in-place taper (HBC.cpp:150, 203)
     if (hbc) LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_taper(sP, ctx->d_taper, geom(ctx), 1, 0, ctx->stream));
 
+    // image target: the caller's FP32 image, the caller's FP64 stack, or the FP64 image that is
+    // rounded into the caller's FP32 image at the end
+    void *img = img_out;
+    bool img64 = false;
+    if (st && acc64) {
+        img64 = true;
+    } else if (st && ctx->img64) {
+        if ((rc = ensure_bytes(ctx, reinterpret_cast<void **>(&ctx->d_img64), ctx->n * sizeof(double), false)))
+            return rc;
+        img = ctx->d_img64;
+        img64 = true;
+    }
+    if (!acc64) CK(cudaMemsetAsync(img, 0, ctx->n * (img64 ? sizeof(double) : sizeof(float)), ctx->stream));
+
     // backward pass (HBC.cpp:212-364 / RBC.cpp:146-274)
     float *rP = ctx->d_w[2], *rPP = ctx->d_w[3];
-    CK(cudaMemsetAsync(rP, 0, ctx->n * sizeof(float), ctx->stream));
-    CK(cudaMemsetAsync(rPP, 0, ctx->n * sizeof(float), ctx->stream));
-    CK(cudaMemsetAsync(img, 0, ctx->n * sizeof(float), ctx->stream));
+    CK(cudaMemsetAsync(rP, 0, wave_bytes(ctx), ctx->stream));
+    CK(cudaMemsetAsync(rPP, 0, wave_bytes(ctx), ctx->stream));
+    rtmb::ScaleRec *sc_rP = nullptr, *sc_rPP = nullptr;
+    if (st) {
+        if (!(sc_rP = new_scale(ctx)) || !(sc_rPP = new_scale(ctx)))
+            return fail(ctx, RTMB_EINVAL, "scale record pool exhausted");
+        // the receiver levels' exponent bound includes max |record| (the injected values)
+        const size_t nrec = (size_t)p.nt * p.receiver_count_x * p.receiver_count_y;
+        LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_absmax(rec, nrec, ctx->d_inj, ctx->stream));
+    }
     const bool full = p.flags & RTMB_FLAG_IMG_FULL_Z;
     float *s_cur = sPP, *s_prev = sP;  // it = nt-1 images snap1
+    rtmb::ScaleRec *sc_cur = scs[1], *sc_prev = scs[0];
     rtmb::StepArgs src = base_args(ctx);
     src.V = ctx->d_v2dt2;
+    src.store = ctx->store;
     if (hbc) src.upb_mode = rtmb::kUpbRestore;
     rtmb::StepArgs rcv = base_args(ctx);
     rcv.V = ctx->d_v2dt2;
     rcv.taper_mode = hbc ? rtmb::kTaperUpper : rtmb::kTaperNone;
-    rcv.img = img;
+    rcv.img = static_cast<float *>(img);
+    rcv.img64 = img64;
     rcv.img_z0 = full ? 0 : (int)p.blen;
     rcv.img_z1 = full ? ctx->nze : ctx->nze - (int)p.blen;
+    rcv.store = ctx->store;
+    rcv.inj_dev = st ? ctx->d_inj : nullptr;
     const int rmode = (p.flags & RTMB_FLAG_RCV_ADD) ? rtmb::kRecAdd : rtmb::kRecOverwrite;
     for (int it = (int)p.nt - 1; it >= 0; --it) {
         if (it == (int)p.nt - 2) {
             s_cur = sP;
             s_prev = sPP;
+            std::swap(sc_cur, sc_prev);
         } else if (it < (int)p.nt - 2) {
             src.P = s_cur; src.PP = s_prev; src.it = it;
             if (hbc) src.upb = ctx->d_upb + (size_t)it * upb_step;
+            rtmb::ScaleRec *lvl = nullptr;
+            if (st) {
+                if (!(lvl = new_scale(ctx))) return fail(ctx, RTMB_EINVAL, "scale record pool exhausted");
+                src.sc_p = sc_cur; src.sc_pp = sc_prev; src.sc_out = lvl;
+            }
             LAUNCH_CAT(RTMB_PROF_BACKWARD_SOURCE,
                        rtmb::launch_step(src, (int)p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
             std::swap(s_cur, s_prev);
+            sc_prev = sc_cur;
+            sc_cur = lvl;
         }
         rcv.P = rP; rcv.PP = rPP; rcv.it = it;
         rcv.ps = s_cur;
+        rtmb::ScaleRec *lvl = nullptr;
+        if (st) {
+            if (!(lvl = new_scale(ctx))) return fail(ctx, RTMB_EINVAL, "scale record pool exhausted");
+            rcv.sc_p = sc_rP; rcv.sc_pp = sc_rPP; rcv.sc_out = lvl; rcv.sc_ps = sc_cur;
+        }
         set_receivers(rcv, ctx, rmode, const_cast<float *>(rec), it);
         LAUNCH_CAT(RTMB_PROF_BACKWARD_RECEIVER,
                    rtmb::launch_step(rcv, (int)p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
         std::swap(rP, rPP);
+        sc_rPP = sc_rP;
+        sc_rP = lvl;
     }
+    if (img != img_out)
+        LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_to_float(ctx->d_img64, static_cast<float *>(img_out), ctx->n,
+                                                          ctx->stream));
     return check_err_flag(ctx);
+}
+
+}  // namespace
+
+extern "C" {
+
+int rtmb_migrate_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const float *rec, float *img) {
+    if (!ctx || !rec || !img) return fail(ctx, RTMB_EINVAL, "rtmb_migrate_shot: null pointer");
+    return migrate_impl(ctx, sx, sy, sz, rec, img, false);
+}
+
+int rtmb_migrate_shot_acc64(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const float *rec,
+                            double *stack) {
+    if (!ctx || !rec || !stack) return fail(ctx, RTMB_EINVAL, "rtmb_migrate_shot_acc64: null pointer");
+    return migrate_impl(ctx, sx, sy, sz, rec, stack, true);
 }
 
 int rtmb_model_shot_host(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, float *rec_host) {

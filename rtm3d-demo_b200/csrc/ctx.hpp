@@ -27,6 +27,17 @@ struct rtmb_ctx {
     float *d_rec = nullptr, *d_img = nullptr;  // staging for the host-buffer forms
     int chunk = 0;
     uint64_t launches = 0;
+    // storage forms (RTMB_FLAG_STORE_*): element type of d_w, one scale record per stored level
+    int store = rtmb::kStoreF32;
+    bool img64 = false;              // RTMB_FLAG_IMG_F64
+    float wmax = 0.f;                // max |Ricker sample|
+    rtmb::ScaleRec *d_scale = nullptr;
+    int sc_cap = 0, sc_next = 0;
+    float *d_inj = nullptr;          // device scalars: [0] max |record|, [1] max forward level
+    double *d_img64 = nullptr;       // FP64 image of the FP32-output migration with RTMB_FLAG_IMG_F64
+    // FP64 GPU oracle (f64.cu)
+    double *d_f64[4] = {};
+    double *d_upb64 = nullptr;
     std::string err;
     // optional per-kernel timing of the drivers (rtmb_profile): an event pair around each launch
     bool prof = false;
@@ -41,8 +52,9 @@ namespace rtmb {
 namespace driver {
 
 // Forward time loop shared by modeling and the migration forward pass (see api.cu).
+// With a storage form, sc_out (if not null) receives the scale records of *P_out and *PP_out.
 int run_forward(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, int taper_mode, float *rec,
-                float *upb, float **P_out, float **PP_out, int cat);
+                float *upb, float **P_out, float **PP_out, int cat, rtmb::ScaleRec **sc_out = nullptr);
 // Reads and clears the device error flag after synchronising the context's stream.
 int check_err_flag(rtmb_ctx *ctx);
 // Fills the derived sizes and the host copy of the stencil coefficients of a context.

@@ -55,6 +55,8 @@ extern "C" int rtmb_model_shot_noalloc(const rtmb_params *params, const float *v
     if (!p.nx || !p.ny || !p.nz || p.stencil_order < 2 || p.stencil_order > 16 || (p.stencil_order & 1u) ||
         !p.ntstep || p.nt % p.ntstep)
         return fail_noctx(RTMB_EINVAL, "rtmb_model_shot_noalloc: invalid parameters");
+    if (p.flags & (RTMB_FLAG_STORE_F16 | RTMB_FLAG_STORE_BF16 | RTMB_FLAG_IMG_F64))
+        return fail_noctx(RTMB_EINVAL, "rtmb_model_shot_noalloc: the 16-bit storage forms need a context");
 
     // a context on the stack: it owns nothing, every device pointer below points into g_scratch or
     // at the caller's buffers

@@ -1,5 +1,6 @@
 // ops.cu -- per-operator kernels.  Each reproduces one reference CPU operator exactly (same
-// multiply order, no contraction: the library is built with --fmad=false).
+// multiply order, no contraction: the library is built with --fmad=false).  The kernels are
+// templates on the wavefield type: float for the operator API, double for the FP64 GPU oracle.
 #include "ops.cuh"
 
 namespace rtmb {
@@ -12,7 +13,8 @@ __device__ __forceinline__ float fac(const float *t, int b, int n, int i) {
 // One thread owns a (y, z) column and walks x, so the front-right quirk of taper3D (a cell that
 // takes its value from x = blen, RTMCPUPlatform.cpp:900-904) reads the raw value of its own column
 // before anything in the column is written.
-__global__ void taper_kernel(float *P, const float *__restrict__ t, Geom g, int upper, int quirk) {
+template <typename R>
+__global__ void taper_kernel(R *P, const float *__restrict__ t, Geom g, int upper, int quirk) {
     const int z = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     if (z >= g.nze) return;
@@ -21,21 +23,21 @@ __global__ void taper_kernel(float *P, const float *__restrict__ t, Geom g, int 
     const bool zb = upper ? (z < b) : (z < b || z >= g.nze - b);
     if (upper && !zb) return;
     const size_t plane = (size_t)g.nye * g.nze;
-    float *col = P + (size_t)y * g.nze + z;
-    const float ty = yb ? fac(t, b, g.nye, y) : 1.f;
-    const float tz = zb ? fac(t, b, g.nze, z) : 1.f;
+    R *col = P + (size_t)y * g.nze + z;
+    const R ty = yb ? (R)fac(t, b, g.nye, y) : (R)1;
+    const R tz = zb ? (R)fac(t, b, g.nze, z) : (R)1;
     // the x range that changes: the whole column if y or z is in a border, else the two x slabs
     const bool whole = yb || zb;
     const bool qcol = !upper && quirk && y >= g.nye - b && !zb;  // right y border, z interior
-    float face = 0.f;
+    R face = 0;
     if (qcol) face = col[(size_t)b * plane] * ty;  // (blen, y, z) after the right-face taper
     for (int x = 0; x < g.nxe; ++x) {
         const bool xb = x < b || x >= g.nxe - b;
         if (!whole && !xb) { x = g.nxe - b - 1; continue; }
-        float v = col[(size_t)x * plane];
+        R v = col[(size_t)x * plane];
         if (xb && zb) {
             if (yb) v = v * ty;
-            v = v * fac(t, b, g.nxe, x);
+            v = v * (R)fac(t, b, g.nxe, x);
             v = v * tz;
         } else if (yb && zb) {
             v = v * ty;
@@ -44,24 +46,28 @@ __global__ void taper_kernel(float *P, const float *__restrict__ t, Geom g, int 
             v = v * tz;
         } else if (xb && yb) {
             if (qcol && x < b) {
-                v = face * fac(t, b, g.nxe, x);
+                v = face * (R)fac(t, b, g.nxe, x);
                 v = v * ty;
             } else {
-                v = v * fac(t, b, g.nxe, x);
+                v = v * (R)fac(t, b, g.nxe, x);
                 v = v * ty;
             }
         } else if (yb) {
             v = v * ty;
         } else {
-            v = v * fac(t, b, g.nxe, x);
+            v = v * (R)fac(t, b, g.nxe, x);
         }
         col[(size_t)x * plane] = v;
     }
 }
 
-__global__ void source_kernel(float *PP, const float *w, int it, size_t off) { PP[off] = PP[off] + w[it]; }
+template <typename R>
+__global__ void source_kernel(R *PP, const float *w, int it, size_t off) { PP[off] = PP[off] + (R)w[it]; }
 
-__global__ void receivers_kernel(float *PP, float *rec, int lt, int mode, RcvGeom r, Geom g) {
+// R: wavefield type; RC: record type (the FP64 oracle samples into a double record and injects
+// the FP32 record).
+template <typename R, typename RC>
+__global__ void receivers_kernel(R *PP, RC *rec, int lt, int mode, RcvGeom r, Geom g) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y;
     if (j >= r.rcy || i >= r.rcx) return;
@@ -69,12 +75,13 @@ __global__ void receivers_kernel(float *PP, float *rec, int lt, int mode, RcvGeo
     if (x < 0 || x >= g.nxe || y < 0 || y >= g.nye) return;
     const size_t o = ((size_t)x * g.nye + y) * g.nze + r.rz;
     const size_t ro = ((size_t)i * r.rcy + j) * r.ntstep + lt;
-    if (mode == 1) rec[ro] = PP[o];
-    else if (mode == 2) PP[o] = rec[ro];
-    else PP[o] = PP[o] + rec[ro];
+    if (mode == 1) rec[ro] = (RC)PP[o];
+    else if (mode == 2) PP[o] = (R)rec[ro];
+    else PP[o] = PP[o] + (R)rec[ro];
 }
 
-__global__ void upb_kernel(float *P, float *upb, int lt, int rw, Geom g) {
+template <typename R>
+__global__ void upb_kernel(R *P, R *upb, int lt, int rw, Geom g) {
     const int y = blockIdx.x * blockDim.x + threadIdx.x;
     const int x = blockIdx.y;
     if (y >= g.nye) return;
@@ -86,8 +93,8 @@ __global__ void upb_kernel(float *P, float *upb, int lt, int rw, Geom g) {
     }
 }
 
-__global__ void image_kernel(float *img, const float *__restrict__ ps, const float *__restrict__ pr,
-                             int z0, int z1, Geom g) {
+template <typename R>
+__global__ void image_kernel(R *img, const R *__restrict__ ps, const R *__restrict__ pr, int z0, int z1, Geom g) {
     const size_t n = (size_t)g.nxe * g.nye * g.nze;
     for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
         const int z = (int)(o % g.nze);
@@ -115,45 +122,116 @@ __global__ void stack_kernel(float *acc, const float *__restrict__ img, size_t n
         acc[o] = acc[o] + img[o];
 }
 
+// max |x| over n floats into *out (zero beforehand), as the bits of a non-negative float
+__global__ void absmax_kernel(const float *__restrict__ x, size_t n, unsigned *out) {
+    float m = 0.f;
+    for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x)
+        m = fmaxf(m, fabsf(x[o]));
+    const unsigned b = __reduce_max_sync(0xffffffffu, __float_as_uint(m));
+    if ((threadIdx.x & 31) == 0 && b) atomicMax(out, b);
+}
+
+// max amax over n scale records into *out (zero beforehand)
+__global__ void scale_max_kernel(const ScaleRec *__restrict__ r, int n, unsigned *out) {
+    unsigned m = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) m = max(m, r[i].amax);
+    m = __reduce_max_sync(0xffffffffu, m);
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
+__global__ void to_float_kernel(const double *__restrict__ a, float *out, size_t n) {
+    for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x)
+        out[o] = (float)a[o];
+}
+
+__global__ void stack64_kernel(double *acc, const float *__restrict__ img, size_t n) {
+    for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x)
+        acc[o] = acc[o] + (double)img[o];
+}
+
 unsigned grid1d(size_t n) {
     size_t b = (n + 255) / 256;
     return (unsigned)(b > 148u * 64u ? 148u * 64u : (b == 0 ? 1 : b));
 }
 
+template <typename R>
+cudaError_t taper_t(R *P, const float *taper, const Geom &g, int upper, int quirk, cudaStream_t s) {
+    if (g.blen <= 0) return cudaSuccess;
+    dim3 grid((g.nze + 127) / 128, g.nye);
+    taper_kernel<R><<<grid, 128, 0, s>>>(P, taper, g, upper, quirk);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t source_t(R *PP, const float *wavelet, int it, int x, int y, int z, const Geom &g, cudaStream_t s) {
+    source_kernel<R><<<1, 1, 0, s>>>(PP, wavelet, it, ((size_t)x * g.nye + y) * g.nze + z);
+    return cudaGetLastError();
+}
+
+template <typename R, typename RC>
+cudaError_t receivers_t(R *PP, RC *rec, int lt, int mode, const RcvGeom &r, const Geom &g, cudaStream_t s) {
+    if (r.rcx <= 0 || r.rcy <= 0) return cudaSuccess;
+    dim3 grid((r.rcy + 127) / 128, r.rcx);
+    receivers_kernel<R, RC><<<grid, 128, 0, s>>>(PP, rec, lt, mode, r, g);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t upb_t(R *P, R *upb, int lt, int rw, const Geom &g, cudaStream_t s) {
+    dim3 grid((g.nye + 127) / 128, g.nxe);
+    upb_kernel<R><<<grid, 128, 0, s>>>(P, upb, lt, rw, g);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t image_t(R *img, const R *ps, const R *pr, int z0, int z1, const Geom &g, cudaStream_t s) {
+    image_kernel<R><<<grid1d((size_t)g.nxe * g.nye * g.nze), 256, 0, s>>>(img, ps, pr, z0, z1, g);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 cudaError_t launch_taper(float *P, const float *taper, const Geom &g, int upper, int quirk, cudaStream_t s) {
-    if (g.blen <= 0) return cudaSuccess;
-    dim3 grid((g.nze + 127) / 128, g.nye);
-    taper_kernel<<<grid, 128, 0, s>>>(P, taper, g, upper, quirk);
-    return cudaGetLastError();
+    return taper_t(P, taper, g, upper, quirk, s);
 }
-
+cudaError_t launch_taper(double *P, const float *taper, const Geom &g, int upper, int quirk, cudaStream_t s) {
+    return taper_t(P, taper, g, upper, quirk, s);
+}
 cudaError_t launch_source(float *PP, const float *wavelet, int it, int x, int y, int z, const Geom &g,
                           cudaStream_t s) {
-    source_kernel<<<1, 1, 0, s>>>(PP, wavelet, it, ((size_t)x * g.nye + y) * g.nze + z);
-    return cudaGetLastError();
+    return source_t(PP, wavelet, it, x, y, z, g, s);
 }
-
+cudaError_t launch_source(double *PP, const float *wavelet, int it, int x, int y, int z, const Geom &g,
+                          cudaStream_t s) {
+    return source_t(PP, wavelet, it, x, y, z, g, s);
+}
 cudaError_t launch_receivers(float *PP, float *rec, int lt, int mode, const RcvGeom &r, const Geom &g,
                              cudaStream_t s) {
-    if (r.rcx <= 0 || r.rcy <= 0) return cudaSuccess;
-    dim3 grid((r.rcy + 127) / 128, r.rcx);
-    receivers_kernel<<<grid, 128, 0, s>>>(PP, rec, lt, mode, r, g);
-    return cudaGetLastError();
+    return receivers_t(PP, rec, lt, mode, r, g, s);
 }
-
+cudaError_t launch_receivers(double *PP, float *rec, int lt, int mode, const RcvGeom &r, const Geom &g,
+                             cudaStream_t s) {
+    return receivers_t(PP, rec, lt, mode, r, g, s);
+}
+cudaError_t launch_receivers(double *PP, double *rec, int lt, int mode, const RcvGeom &r, const Geom &g,
+                             cudaStream_t s) {
+    return receivers_t(PP, rec, lt, mode, r, g, s);
+}
 cudaError_t launch_upb(float *P, float *upb, int lt, int rw, const Geom &g, cudaStream_t s) {
-    dim3 grid((g.nye + 127) / 128, g.nxe);
-    upb_kernel<<<grid, 128, 0, s>>>(P, upb, lt, rw, g);
-    return cudaGetLastError();
+    return upb_t(P, upb, lt, rw, g, s);
 }
-
+cudaError_t launch_upb(double *P, double *upb, int lt, int rw, const Geom &g, cudaStream_t s) {
+    return upb_t(P, upb, lt, rw, g, s);
+}
 cudaError_t launch_image(float *img, const float *ps, const float *pr, int z0, int z1, const Geom &g,
                          cudaStream_t s) {
-    image_kernel<<<grid1d((size_t)g.nxe * g.nye * g.nze), 256, 0, s>>>(img, ps, pr, z0, z1, g);
-    return cudaGetLastError();
+    return image_t(img, ps, pr, z0, z1, g, s);
 }
+cudaError_t launch_image(double *img, const double *ps, const double *pr, int z0, int z1, const Geom &g,
+                         cudaStream_t s) {
+    return image_t(img, ps, pr, z0, z1, g, s);
+}
+
 
 cudaError_t launch_filter_remove(const float *img, float *out, const float *c3, const Geom &g, cudaStream_t s) {
     const int nx = g.nxe - 2 * g.blen, ny = g.nye - 2 * g.blen, nz = g.nze - 2 * g.blen;
@@ -166,6 +244,30 @@ cudaError_t launch_filter_remove(const float *img, float *out, const float *c3, 
 
 cudaError_t launch_stack(float *acc, const float *img, size_t n, cudaStream_t s) {
     stack_kernel<<<grid1d(n), 256, 0, s>>>(acc, img, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_absmax(const float *x, size_t n, float *out, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(float), s);
+    if (e != cudaSuccess || n == 0) return e;
+    absmax_kernel<<<grid1d(n), 256, 0, s>>>(x, n, reinterpret_cast<unsigned *>(out));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scale_max(const ScaleRec *r, int n, float *out, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(out, 0, sizeof(float), s);
+    if (e != cudaSuccess || n <= 0) return e;
+    scale_max_kernel<<<1, 256, 0, s>>>(r, n, reinterpret_cast<unsigned *>(out));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_to_float(const double *a, float *out, size_t n, cudaStream_t s) {
+    to_float_kernel<<<grid1d(n), 256, 0, s>>>(a, out, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stack64(double *acc, const float *img, size_t n, cudaStream_t s) {
+    stack64_kernel<<<grid1d(n), 256, 0, s>>>(acc, img, n);
     return cudaGetLastError();
 }
 

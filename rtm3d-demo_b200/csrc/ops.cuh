@@ -3,6 +3,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "stencil.cuh"
+
 namespace rtmb {
 
 struct Geom {
@@ -32,5 +34,27 @@ cudaError_t launch_image(float *img, const float *ps, const float *pr, int z0, i
 cudaError_t launch_filter_remove(const float *img, float *out, const float *c3, const Geom &g, cudaStream_t s);
 // acc += img over n floats.
 cudaError_t launch_stack(float *acc, const float *img, size_t n, cudaStream_t s);
+
+// FP64 overloads of the operators above, for the FP64 GPU oracle (same operator sequence and
+// multiply order, double arithmetic).
+cudaError_t launch_taper(double *P, const float *taper, const Geom &g, int upper, int quirk, cudaStream_t s);
+cudaError_t launch_source(double *PP, const float *wavelet, int it, int x, int y, int z, const Geom &g,
+                          cudaStream_t s);
+cudaError_t launch_receivers(double *PP, float *rec, int lt, int mode, const RcvGeom &r, const Geom &g,
+                             cudaStream_t s);
+cudaError_t launch_receivers(double *PP, double *rec, int lt, int mode, const RcvGeom &r, const Geom &g,
+                             cudaStream_t s);
+cudaError_t launch_upb(double *P, double *upb, int lt, int rw, const Geom &g, cudaStream_t s);
+cudaError_t launch_image(double *img, const double *ps, const double *pr, int z0, int z1, const Geom &g,
+                         cudaStream_t s);
+
+// *out = max |x| over n floats.
+cudaError_t launch_absmax(const float *x, size_t n, float *out, cudaStream_t s);
+// *out = max amax over n scale records.
+cudaError_t launch_scale_max(const ScaleRec *r, int n, float *out, cudaStream_t s);
+// out = (float) a over n values.
+cudaError_t launch_to_float(const double *a, float *out, size_t n, cudaStream_t s);
+// acc += (double) img over n values.
+cudaError_t launch_stack64(double *acc, const float *img, size_t n, cudaStream_t s);
 
 }  // namespace rtmb

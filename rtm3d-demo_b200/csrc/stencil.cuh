@@ -16,6 +16,7 @@
 // the y/z taps come from a double-buffered shared-memory copy of the current plane plus halo.
 // Loads for plane x+1 are issued before the arithmetic of plane x.
 #pragma once
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -28,6 +29,17 @@ constexpr int kThreads = (kTZ / kVZ) * kTY;  // 256
 constexpr int kMaxOrder = 16;
 
 enum TaperMode : int { kTaperNone = 0, kTaperUpper = 1, kTaperAll = 2 };
+// How P, PP and ps are stored in HBM.  The 16-bit forms hold value * 2^-e in the 16-bit type, with
+// one power-of-two exponent e per stored time level (ScaleRec); all arithmetic stays FP32.
+enum StoreType : int { kStoreF32 = 0, kStoreF16 = 1, kStoreBF16 = 2 };
+
+// Scale record of one stored time level of a 16-bit wavefield.  e: the level's exponent, written by
+// the launch that produces the level; amax: bits of max |value| over the level (a non-negative float,
+// so its bits order like the values), accumulated by that launch with atomicMax; zero beforehand.
+struct ScaleRec {
+    int e;
+    unsigned amax;
+};
 enum RecMode : int { kRecNone = 0, kRecSample = 1, kRecOverwrite = 2, kRecAdd = 3 };
 enum UpbMode : int { kUpbNone = 0, kUpbSave = 1, kUpbRestore = 2 };
 
@@ -66,10 +78,34 @@ struct StepArgs {
     int img_z0, img_z1;
     // error flags (bit 0: NaN)
     unsigned int *err;
+    // storage form.  store != kStoreF32: P, PP and ps point at 16-bit values (StoreType), with the
+    // scale records below; img64: img points at doubles.
+    int store;
+    int img64;
+    const ScaleRec *sc_p, *sc_pp, *sc_ps;
+    ScaleRec *sc_out;           // record of the level this launch writes into PP
+    float inj;                  // bound on |values| written by injection (source, receivers, border)
+    const float *inj_dev;       // optional device scalar added to inj
 };
+
+// Exponent of a produced level: the smallest e with bound * 2^-e < 2^15.  bound is
+// 8 * max(amax(P), amax(PP)) + injection: a stable step (v^2 dt^2 * sum|coef| <= 4 over the three
+// axes) keeps |2p - pp + v^2 dt^2 lap p| <= 7 max(amax(P), amax(PP)), so a 16-bit level never
+// overflows (FP16 max 65504 > 2^15) and keeps at least 12 bits of headroom below it.
+__host__ __device__ inline int storage_exponent(float bound) {
+    if (!(bound > 0.f)) return 0;
+    int k = 0;
+    (void)frexpf(bound, &k);  // bound = m 2^k, 0.5 <= m < 1
+    int e = k - 15;
+    return e < -100 ? -100 : (e > 100 ? 100 : e);
+}
 
 // Launch one step.  Selects the instantiation for order/2 and the alignment of the arrays.
 // allow_tma = false forces the plain-load form (used by tests to check both forms).
 cudaError_t launch_step(const StepArgs &a, int order, bool exact, cudaStream_t s, bool allow_tma = true);
+
+// Whether the 16-bit storage forms (and the FP64 image) can run on this geometry: order 8 and
+// z rows whose 16-bit pitch is a multiple of 16 bytes (nze % 8 == 0).
+bool storage_form_supported(int order, int nze);
 
 }  // namespace rtmb

@@ -22,6 +22,8 @@
 // stops; the producer waits, again bounded, for the copies it issued before it exits.
 #pragma once
 #include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include "stencil_common.cuh"
 
@@ -92,35 +94,104 @@ struct TmaMaps {
     CUtensorMap p, pp, v, ps, img;
 };
 
-template <int H, bool IMG>
+// Element access for the storage types.  ld4 reads four consecutive values from shared memory and
+// widens them to FP32; st4 narrows four FP32 values and stores them to global memory.
+template <typename T>
+struct Stor;
+template <>
+struct Stor<float> {
+    static constexpr bool kScaled = false;
+    __device__ static float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+    __device__ static float to_f(float v) { return v; }
+    __device__ static float from_f(float v) { return v; }
+    __device__ static void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
+};
+template <>
+struct Stor<__half> {
+    static constexpr bool kScaled = true;
+    __device__ static float4 ld4(const __half *p) {
+        const uint2 u = *reinterpret_cast<const uint2 *>(p);
+        const float2 a = __half22float2(*reinterpret_cast<const __half2 *>(&u.x));
+        const float2 b = __half22float2(*reinterpret_cast<const __half2 *>(&u.y));
+        return make_float4(a.x, a.y, b.x, b.y);
+    }
+    __device__ static float to_f(__half v) { return __half2float(v); }
+    __device__ static __half from_f(float v) { return __float2half_rn(v); }
+    __device__ static void st4(__half *p, float4 v) {
+        const __half2 a = __floats2half2_rn(v.x, v.y), b = __floats2half2_rn(v.z, v.w);
+        uint2 u;
+        u.x = *reinterpret_cast<const uint32_t *>(&a);
+        u.y = *reinterpret_cast<const uint32_t *>(&b);
+        *reinterpret_cast<uint2 *>(p) = u;
+    }
+};
+template <>
+struct Stor<__nv_bfloat16> {
+    static constexpr bool kScaled = true;
+    __device__ static float4 ld4(const __nv_bfloat16 *p) {
+        const uint2 u = *reinterpret_cast<const uint2 *>(p);
+        const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&u.x));
+        const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&u.y));
+        return make_float4(a.x, a.y, b.x, b.y);
+    }
+    __device__ static float to_f(__nv_bfloat16 v) { return __bfloat162float(v); }
+    __device__ static __nv_bfloat16 from_f(float v) { return __float2bfloat16_rn(v); }
+    __device__ static void st4(__nv_bfloat16 *p, float4 v) {
+        const __nv_bfloat162 a = __floats2bfloat162_rn(v.x, v.y), b = __floats2bfloat162_rn(v.z, v.w);
+        uint2 u;
+        u.x = *reinterpret_cast<const uint32_t *>(&a);
+        u.y = *reinterpret_cast<const uint32_t *>(&b);
+        *reinterpret_cast<uint2 *>(p) = u;
+    }
+};
+
+// 2^e as a float for -126 <= e <= 127 (exact).
+__device__ __forceinline__ float exp2i(int e) { return __int_as_float((e + 127) << 23); }
+
+// Shared-memory plan of one variant.  T: storage type of P/PP/ps; IT: image type.
+template <int H, bool IMG, typename T = float, typename IT = float>
 struct TmaShape {
-    static constexpr int ZH = ((H + 3) / 4) * 4;
+    static constexpr int EALIGN = 16 / (int)sizeof(T) > 4 ? 16 / (int)sizeof(T) : 4;
+    static constexpr int ZH = ((H + EALIGN - 1) / EALIGN) * EALIGN;  // z halo: whole 16-byte units
     static constexpr int SROWS = kTY + 2 * H;
     static constexpr int SPITCH = kTZ + 2 * ZH;
-    static constexpr int STAGE = SROWS * SPITCH;             // floats written by one P tile load
-    static constexpr int STRIDE = ((STAGE + 31) / 32) * 32;  // P slot pitch: 128-byte aligned
-    static constexpr int CORE = kTZ * kTY;                   // floats of one core tile
-    static constexpr int NCORE = IMG ? 4 : 2;                // PP, V (, PS, IMG)
-    static constexpr int D = IMG ? H + 5 : H + 6;            // P slots
-    static constexpr int R = IMG ? 3 : 4;                    // core slots
+    static constexpr int STAGE = SROWS * SPITCH;  // elements written by one P tile load
+    static constexpr int SALIGN = 128 / (int)sizeof(T);
+    static constexpr int STRIDE = ((STAGE + SALIGN - 1) / SALIGN) * SALIGN;  // P slot pitch: 128 B
+    static constexpr int CORE = kTZ * kTY;  // elements of one core tile
+    // core slot, in bytes: PP (T), V (float) [, PS (T), IMG (IT)]
+    static constexpr int OFF_V = CORE * (int)sizeof(T);
+    static constexpr int OFF_PS = OFF_V + CORE * 4;
+    static constexpr int OFF_IMG = OFF_PS + CORE * (int)sizeof(T);
+    static constexpr int CSLOT = IMG ? OFF_IMG + CORE * (int)sizeof(IT) : OFF_PS;
+    static constexpr int D = IMG ? H + 5 : H + 6;  // P slots
+    static constexpr int R = IMG ? 3 : 4;          // core slots
     static_assert(2 * H <= D && D >= H + 2, "warm-up planes and the lookahead must fit in the P ring");
-    static constexpr size_t SMEM =
-        ((size_t)D * STRIDE + (size_t)R * NCORE * CORE) * sizeof(float) + 2 * (D + R) * sizeof(uint64_t);
+    static constexpr size_t PRING_BYTES = (size_t)D * STRIDE * sizeof(T);
+    static constexpr size_t SMEM = PRING_BYTES + (size_t)R * CSLOT + 2 * (D + R) * sizeof(uint64_t);
 };
 
 // TAPER: kTaperNone / kTaperUpper / kTaperAll.  IMG: the epilogue accumulates the image.
-template <int H, bool EXACT, int TAPER, bool IMG>
+// T: storage type of P, PP and ps (float: the FP32 form, bit-identical to the plain-load kernel;
+// __half / __nv_bfloat16: scaled 16-bit storage).  IT: image type (float or double).
+template <int H, bool EXACT, int TAPER, bool IMG, typename T = float, typename IT = float>
 __global__ void __launch_bounds__(kTmaThreads, 2)
     tma_step_kernel(const __grid_constant__ TmaMaps maps, const __grid_constant__ StepArgs a) {
-    using S = TmaShape<H, IMG>;
+    using S = TmaShape<H, IMG, T, IT>;
+    using ST = Stor<T>;
+    constexpr bool SC = ST::kScaled;
+    // CB: the consumers meet at named barriers (taper passes), so a timed-out wait must be seen by
+    // all of them at the next barrier instead of one warp leaving alone
+    constexpr bool CB = TAPER != kTaperNone;
+    static_assert(!(SC && EXACT), "the 16-bit storage forms use the FMA arithmetic");
     constexpr int ZH = S::ZH, SPITCH = S::SPITCH, STAGE = S::STAGE, STRIDE = S::STRIDE, D = S::D, R = S::R;
-    constexpr int CORE = S::CORE, NCORE = S::NCORE;
+    constexpr int CSLOT = S::CSLOT;
     constexpr int NQ = 2 * H + 1;
     constexpr int ZQ = kTZ / kVZ;
-    extern __shared__ __align__(128) float smem[];
-    float *pring = smem;
-    float *cring = smem + D * STRIDE;
-    uint64_t *pfull = reinterpret_cast<uint64_t *>(cring + R * NCORE * CORE);
+    extern __shared__ __align__(128) unsigned char smem[];
+    T *pring = reinterpret_cast<T *>(smem);
+    unsigned char *cring = smem + S::PRING_BYTES;
+    uint64_t *pfull = reinterpret_cast<uint64_t *>(cring + R * CSLOT);
     uint64_t *cfull = pfull + D;
     uint64_t *pempty = cfull + R;
     uint64_t *cempty = pempty + D;
@@ -155,19 +226,19 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
         for (int k = 0; k < nplanes && ok; ++k) {
             const int s = k % D;
             if (k >= D && !(ok = mbar_wait(&pempty[s], ((k / D) + 1) & 1))) break;
-            mbar_expect_tx(&pfull[s], STAGE * sizeof(float));
+            mbar_expect_tx(&pfull[s], STAGE * sizeof(T));
             tma_load_3d(pring + s * STRIDE, &maps.p, &pfull[s], zt0 - ZH, yt0 - H, xc0 - H + k);
             p_issued = k + 1;
             if (k >= 2 * H) {
                 const int i = k - 2 * H, cs = i % R;
                 if (i >= R && !(ok = mbar_wait(&cempty[cs], ((i / R) + 1) & 1))) break;
-                float *dst = cring + cs * NCORE * CORE;
-                mbar_expect_tx(&cfull[cs], NCORE * CORE * sizeof(float));
+                unsigned char *dst = cring + cs * CSLOT;
+                mbar_expect_tx(&cfull[cs], CSLOT);
                 tma_load_3d(dst, &maps.pp, &cfull[cs], zt0, yt0, xc0 + i);
-                tma_load_3d(dst + CORE, &maps.v, &cfull[cs], zt0, yt0, xc0 + i);
+                tma_load_3d(dst + S::OFF_V, &maps.v, &cfull[cs], zt0, yt0, xc0 + i);
                 if (IMG) {
-                    tma_load_3d(dst + 2 * CORE, &maps.ps, &cfull[cs], zt0, yt0, xc0 + i);
-                    tma_load_3d(dst + 3 * CORE, &maps.img, &cfull[cs], zt0, yt0, xc0 + i);
+                    tma_load_3d(dst + S::OFF_PS, &maps.ps, &cfull[cs], zt0, yt0, xc0 + i);
+                    tma_load_3d(dst + S::OFF_IMG, &maps.img, &cfull[cs], zt0, yt0, xc0 + i);
                 }
                 c_issued = i + 1;
             }
@@ -181,6 +252,23 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
         return;
     }
     const int lane = tid & 31;
+    const T *Pg = reinterpret_cast<const T *>(a.P);
+
+    // ---- scales of the 16-bit forms: the stored levels hold value * 2^-e
+    float sP = 1.f, sPP = 1.f, sPS = 1.f, sOutInv = 1.f, sPPinv = 1.f, sKeep = 1.f;
+    if constexpr (SC) {
+        const ScaleRec rp = *a.sc_p, rpp = *a.sc_pp;
+        sP = exp2i(rp.e);
+        sPP = exp2i(rpp.e);
+        sPPinv = exp2i(-rpp.e);
+        if (IMG) sPS = exp2i(a.sc_ps->e);
+        const float bound = 8.f * fmaxf(__uint_as_float(rp.amax), __uint_as_float(rpp.amax)) + a.inj +
+                            (a.inj_dev ? *a.inj_dev : 0.f);
+        const int eN = storage_exponent(bound);
+        sOutInv = exp2i(-eN);
+        sKeep = exp2i(max(-126, min(127, rpp.e - eN)));  // re-stores cells outside the computed region
+        if (tid == 0 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0) a.sc_out->e = eN;
+    }
 
     // ---- per-thread constants, hoisted out of the plane loop
     const bool row_ok = y < a.nye && z0 < a.nze;
@@ -217,7 +305,7 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
     if (TAPER == kTaperUpper) pp_taper_yz = z0 < a.blen;
 
     const size_t row_off = (size_t)y * a.nze + z0;
-    float *PPp = a.PP + row_off;
+    T *PPp = reinterpret_cast<T *>(a.PP) + row_off;
     const int col = ZH + tz * kVZ;
     const int ccol = ty * kTZ + tz * kVZ;  // this thread's offset in a core tile
 
@@ -229,30 +317,31 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
         __syncwarp();
         if (lane == 0) mbar_arrive(&pempty[k % D]);
     };
-    // taper of the tile of P plane k, in place (TAPER forms).  The pass is collective: every consumer
-    // thread tapers a share of the tile, so it ends with the consumer barrier.
+    // taper of the tile of P plane k, in place and in stored units (TAPER forms).  The pass is
+    // collective: every consumer thread tapers a share of the tile, so it ends with the consumer
+    // barrier.
     auto taper_stage = [&](int k) {
         const int x = xc0 - H + k;
         bool need;
         if (TAPER == kTaperAll) need = tile_taper_yz || x < a.blen || x >= a.nxe - a.blen;
         else need = tile_taper_yz;
         if (!need) return;  // uniform across the CTA
-        float *st = pring + (k % D) * STRIDE;
+        T *st = pring + (k % D) * STRIDE;
         for (int c = tid; c < STAGE; c += kThreads) {
             const int r = c / SPITCH, cc = c % SPITCH;
             const int yy = yt0 - H + r, zz = zt0 - ZH + cc;
             if (yy >= a.nye || zz < 0 || zz >= a.nze) continue;
-            float v = st[c];
+            float v = ST::to_f(st[c]);
             if (TAPER == kTaperAll && quirk_cell(x, yy, zz, a)) {
                 const float tyy = face_factor(a.taper, a.blen, a.nye, yy);
-                v = __ldg(a.P + (size_t)a.blen * plane + (size_t)yy * a.nze + zz);
+                v = ST::to_f(Pg[(size_t)a.blen * plane + (size_t)yy * a.nze + zz]);
                 v = v * tyy;
                 v = v * face_factor(a.taper, a.blen, a.nxe, x);
                 v = v * tyy;
             } else {
                 v = taper_once(v, x, yy, zz, a);
             }
-            st[c] = v;
+            st[c] = ST::from_f(v);
         }
         // the slot is refilled by TMA later: order these generic-proxy writes before that
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -261,14 +350,15 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
 
     float4 q[NQ];
     float nanacc = 0.f;  // stays 0 unless a NaN or an infinity is written
+    float amax = 0.f;    // max |value| written (16-bit forms)
     // warm-up: P planes 0 .. 2H-1 into the queue; planes 0 .. H-1 are not computed here
     for (int k = 0; k < 2 * H; ++k) {
         wait_p(k);
         if (TAPER != kTaperNone) taper_stage(k);
     }
-    if (bad_wait) goto drain;
+    if (CB ? consumer_sync_or(bad_wait) : bad_wait) goto drain;
 #pragma unroll
-    for (int k = 0; k < 2 * H; ++k) q[k + 1] = ld_f4(pring + (k % D) * STRIDE + (ty + H) * SPITCH + col);
+    for (int k = 0; k < 2 * H; ++k) q[k + 1] = ST::ld4(pring + (k % D) * STRIDE + (ty + H) * SPITCH + col);
 #pragma unroll
     for (int k = 0; k < H; ++k) release_p(k);  // planes 0 .. H-1 were only needed for the queue
 
@@ -278,7 +368,8 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
             const int x = xc0 + i;
             const int kin = i + 2 * H;
             wait_p(kin);
-            if (TAPER != kTaperNone) {
+            const T *s = pring + ((i + H) % D) * STRIDE;  // the centre plane's tile
+            if constexpr (CB) {
                 if (consumer_sync_or(bad_wait)) goto drain;  // the taper pass is collective
                 taper_stage(kin);
             } else if (bad_wait) {
@@ -286,8 +377,7 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
             }
 #pragma unroll
             for (int k = 0; k < NQ - 1; ++k) q[k] = q[k + 1];  // advance the x queue
-            q[NQ - 1] = ld_f4(pring + (kin % D) * STRIDE + (ty + H) * SPITCH + col);
-            const float *s = pring + ((i + H) % D) * STRIDE;
+            q[NQ - 1] = ST::ld4(pring + (kin % D) * STRIDE + (ty + H) * SPITCH + col);
 
             float lap[kVZ] = {0.f, 0.f, 0.f, 0.f};
             if (row_ok) {
@@ -295,7 +385,7 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
 #pragma unroll
                 for (int k = 0; k < (kVZ + 2 * ZH) / 4; ++k) {
                     const float4 t4 =
-                        (k == ZH / 4) ? q[H] : ld_f4(s + (ty + H) * SPITCH + col - ZH + 4 * k);
+                        (k == ZH / 4) ? q[H] : ST::ld4(s + (ty + H) * SPITCH + col - ZH + 4 * k);
                     zr[4 * k + 0] = t4.x; zr[4 * k + 1] = t4.y; zr[4 * k + 2] = t4.z; zr[4 * k + 3] = t4.w;
                 }
                 if (EXACT) {
@@ -305,7 +395,7 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
 #pragma unroll
                     for (int io = 0; io < NQ; ++io) {
                         const float4 qx = q[io];
-                        const float4 ry = (io == H) ? q[H] : ld_f4(s + (ty + io) * SPITCH + col);
+                        const float4 ry = (io == H) ? q[H] : ST::ld4(s + (ty + io) * SPITCH + col);
 #pragma unroll
                         for (int e = 0; e < kVZ; ++e) {
                             ax[e] = ax[e] + get(qx, e) * a.cx[io];
@@ -324,7 +414,7 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
                     for (int io = 0; io < NQ; ++io) {
                         if (io == H) continue;
                         const float4 qx = q[io];
-                        const float4 ry = ld_f4(s + (ty + io) * SPITCH + col);
+                        const float4 ry = ST::ld4(s + (ty + io) * SPITCH + col);
 #pragma unroll
                         for (int e = 0; e < kVZ; ++e) {
                             lap[e] = fmaf(get(qx, e), a.cx[io], lap[e]);
@@ -339,18 +429,32 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
             const int cs = i % R;
             if (!__all_sync(0xffffffffu, mbar_wait(&cfull[cs], (i / R) & 1))) {
                 bad_wait = true;
+                if (CB) continue;  // the other warps learn of it at the next barrier
                 goto drain;
             }
-            const float *ct = cring + cs * NCORE * CORE + ccol;
-            const float4 pp_raw = ld_f4(ct), vv = ld_f4(ct + CORE);
-            float4 ps4 = pp_raw, im4 = pp_raw;
-            if (IMG) { ps4 = ld_f4(ct + 2 * CORE); im4 = ld_f4(ct + 3 * CORE); }
+            const unsigned char *ct = cring + cs * CSLOT;
+            const float4 pp_raw = ST::ld4(reinterpret_cast<const T *>(ct) + ccol);
+            const float4 vv = ld_f4(reinterpret_cast<const float *>(ct + S::OFF_V) + ccol);
+            float4 ps4 = pp_raw;
+            IT im[kVZ];
+            if (IMG) {
+                ps4 = ST::ld4(reinterpret_cast<const T *>(ct + S::OFF_PS) + ccol);
+                const IT *imt = reinterpret_cast<const IT *>(ct + S::OFF_IMG) + ccol;
+                if constexpr (sizeof(IT) == 4) {
+                    const float4 t4 = ld_f4(reinterpret_cast<const float *>(imt));
+                    im[0] = t4.x; im[1] = t4.y; im[2] = t4.z; im[3] = t4.w;
+                } else {
+                    const double2 d0 = reinterpret_cast<const double2 *>(imt)[0];
+                    const double2 d1 = reinterpret_cast<const double2 *>(imt)[1];
+                    im[0] = d0.x; im[1] = d0.y; im[2] = d1.x; im[3] = d1.y;
+                }
+            }
             __syncwarp();
             if (lane == 0) mbar_arrive(&cempty[cs]);
             if (!row_ok) continue;
 
             const float4 qc = q[H];
-            float ppv[kVZ] = {pp_raw.x, pp_raw.y, pp_raw.z, pp_raw.w};
+            float ppv[kVZ] = {pp_raw.x, pp_raw.y, pp_raw.z, pp_raw.w};  // stored units
             if (TAPER != kTaperNone) {
                 const bool pp_taper = pp_taper_yz || (TAPER == kTaperAll && (x < a.blen || x >= a.nxe - a.blen));
                 if (pp_taper) {
@@ -362,6 +466,7 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
                         if (TAPER == kTaperAll && quirk_cell(x, y, z, a)) {
                             const float ty_ = face_factor(a.taper, a.blen, a.nye, y);
                             pp = a.quirk_in[(size_t)(y - (a.nye - a.blen)) * (a.nze - 2 * a.blen) + (z - a.blen)];
+                            if (SC) pp = pp * sPPinv;  // the side buffer holds values, not stored units
                             pp = pp * ty_;
                             pp = pp * ty_;
                             pp = pp * face_factor(a.taper, a.blen, a.nxe, x);
@@ -381,6 +486,8 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
                     const float d = two_p - ppv[e];
                     const float vl = get(vv, e) * lap[e];
                     npp[e] = d + vl;
+                } else if (SC) {  // exact power-of-two rescaling of the stored units
+                    npp[e] = fmaf(get(vv, e), lap[e] * sP, (2.f * sP) * get(qc, e) - ppv[e] * sPP);
                 } else {
                     npp[e] = fmaf(get(vv, e), lap[e], 2.f * get(qc, e) - ppv[e]);
                 }
@@ -411,23 +518,45 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
             float4 out;
 #pragma unroll
             for (int e = 0; e < kVZ; ++e) {
-                const float o = ((vmask >> e) & 1u) ? npp[e] : get(pp_raw, e);
+                const bool v = (vmask >> e) & 1u;
+                float o;
+                if (SC) {
+                    o = v ? npp[e] * sOutInv : get(pp_raw, e) * sKeep;
+                    if (v) amax = fmaxf(amax, fabsf(npp[e]));
+                    nanacc = fmaf(0.f, npp[e], nanacc);
+                } else {
+                    o = v ? npp[e] : get(pp_raw, e);
+                    nanacc = fmaf(0.f, o, nanacc);  // stays 0 unless a NaN or an infinity appears
+                }
                 put(out, e, o);
-                nanacc = fmaf(0.f, o, nanacc);  // stays 0 unless a NaN or an infinity appears
             }
-            *reinterpret_cast<float4 *>(PPp + (size_t)x * plane) = out;
+            ST::st4(PPp + (size_t)x * plane, out);
             if (IMG && imask) {
-                float4 im;
+                IT *ig = reinterpret_cast<IT *>(a.img) + row_off + (size_t)x * plane;
+                IT res[kVZ];
 #pragma unroll
                 for (int e = 0; e < kVZ; ++e) {
-                    const float acc = get(im4, e) + get(ps4, e) * get(out, e);
-                    put(im, e, ((imask >> e) & 1u) ? acc : get(im4, e));
+                    IT acc;
+                    if (SC) acc = im[e] + (IT)(get(ps4, e) * sPS) * (IT)npp[e];
+                    else acc = im[e] + (IT)get(ps4, e) * (IT)get(out, e);
+                    res[e] = ((imask >> e) & 1u) ? acc : im[e];
                 }
-                *reinterpret_cast<float4 *>(a.img + row_off + (size_t)x * plane) = im;
+                if constexpr (sizeof(IT) == 4) {
+                    *reinterpret_cast<float4 *>(ig) = make_float4((float)res[0], (float)res[1], (float)res[2],
+                                                                  (float)res[3]);
+                } else {
+                    reinterpret_cast<double2 *>(ig)[0] = make_double2((double)res[0], (double)res[1]);
+                    reinterpret_cast<double2 *>(ig)[1] = make_double2((double)res[2], (double)res[3]);
+                }
             }
         }
     }
     if (nanacc != nanacc && a.err) atomicOr(a.err, 1u);
+    if (bad_wait && a.err) atomicOr(a.err, 2u);  // a core-tile wait ran out in the last plane
+    if constexpr (SC) {
+        const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(amax));
+        if (lane == 0 && m) atomicMax(&a.sc_out->amax, m);
+    }
     return;
 
 drain:
@@ -466,6 +595,39 @@ cudaError_t launch_tma_h(const TmaMaps &maps, const StepArgs &a, bool exact, int
     RTMB_TMA_CASE(false, kTaperNone, true)
     RTMB_TMA_CASE(false, kTaperUpper, true)
 #undef RTMB_TMA_CASE
+    return cudaErrorInvalidValue;
+}
+
+// The 16-bit storage forms (order 8, FMA arithmetic): T = __half or __nv_bfloat16; img64 selects a
+// double image.
+template <typename T>
+cudaError_t launch_tma_store(const TmaMaps &maps, const StepArgs &a, int taper, bool img, bool img64, dim3 grid,
+                             cudaStream_t s) {
+    static unsigned long long attr_done[8] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int variant = (img ? (img64 ? 6 : 3) : 0) + taper;
+    auto run = [&](void (*kern)(TmaMaps, StepArgs), size_t smem) -> cudaError_t {
+        const unsigned long long bit = 1ull << (dev & 63);
+        if (!(attr_done[variant] & bit)) {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            attr_done[variant] |= bit;
+        }
+        kern<<<grid, kTmaThreads, smem, s>>>(maps, a);
+        return cudaGetLastError();
+    };
+#define RTMB_TMA_STORE_CASE(TP, IM, IT)                                                          \
+    if (taper == TP && img == IM && (!IM || img64 == (sizeof(IT) == 8)))                         \
+        return run(tma_step_kernel<4, false, TP, IM, T, IT>, TmaShape<4, IM, T, IT>::SMEM);
+    RTMB_TMA_STORE_CASE(kTaperNone, false, float)
+    RTMB_TMA_STORE_CASE(kTaperUpper, false, float)
+    RTMB_TMA_STORE_CASE(kTaperAll, false, float)
+    RTMB_TMA_STORE_CASE(kTaperNone, true, float)
+    RTMB_TMA_STORE_CASE(kTaperUpper, true, float)
+    RTMB_TMA_STORE_CASE(kTaperNone, true, double)
+    RTMB_TMA_STORE_CASE(kTaperUpper, true, double)
+#undef RTMB_TMA_STORE_CASE
     return cudaErrorInvalidValue;
 }
 

@@ -23,6 +23,9 @@ FLAG_IMG_FULL_Z = 0x4
 FLAG_NO_TAPER_QUIRK = 0x8
 FLAG_USE_GRAPH = 0x10
 FLAG_NO_TMA = 0x20
+FLAG_STORE_F16 = 0x40
+FLAG_STORE_BF16 = 0x80
+FLAG_IMG_F64 = 0x100
 
 # every symbol include/rtm3d_b200.h declares: (name, argtypes, restype)
 _vp, _fp, _u32, _i32 = C.c_void_p, C.POINTER(C.c_float), C.c_uint32, C.c_int32
@@ -92,6 +95,9 @@ SYMBOLS = [
     ("rtmb_model_shot_host", [_vp, _u32, _u32, _u32, _vp], C.c_int),
     ("rtmb_migrate_shot_host", [_vp, _u32, _u32, _u32, _vp, _vp], C.c_int),
     ("rtmb_model_shot_noalloc", [C.POINTER(Params), _vp, _u32, _u32, _u32, _vp, _vp], C.c_int),
+    ("rtmb_migrate_shot_acc64", [_vp, _u32, _u32, _u32, _vp, _vp], C.c_int),
+    ("rtmb_model_shot_f64", [_vp, _u32, _u32, _u32, _vp], C.c_int),
+    ("rtmb_migrate_shot_f64", [_vp, _u32, _u32, _u32, _vp, _vp], C.c_int),
 ]
 
 _LIB = None
@@ -138,7 +144,7 @@ class Context:
         h = _vp()
         rc = self.L.rtmb_create(C.byref(params), C.byref(h))
         if rc != RTMB_OK:
-            raise RtmbError(rc, "rtmb_create failed")
+            raise RtmbError(rc, "rtmb_create failed: " + self.L.rtmb_last_error(None).decode())
         self.h = h
         if stream is not None:
             self._check(self.L.rtmb_set_stream(self.h, _ptr(stream) if not isinstance(stream, int) else stream))
@@ -229,6 +235,18 @@ class Context:
 
     def migrate_shot(self, sx, sy, sz, rec, img):
         self._check(self.L.rtmb_migrate_shot(self.h, sx, sy, sz, _ptr(rec), _ptr(img)))
+
+    def migrate_shot_acc64(self, sx, sy, sz, rec, stack):
+        """Adds this shot's image to an FP64 stack (padded, device, float64)."""
+        self._check(self.L.rtmb_migrate_shot_acc64(self.h, sx, sy, sz, _ptr(rec), _ptr(stack)))
+
+    def model_shot_f64(self, sx, sy, sz, rec64):
+        """FP64 GPU oracle modeling: rec64 is a float64 device record in file layout."""
+        self._check(self.L.rtmb_model_shot_f64(self.h, sx, sy, sz, _ptr(rec64)))
+
+    def migrate_shot_f64(self, sx, sy, sz, rec, img64):
+        """FP64 GPU oracle migration: rec float32, img64 float64 padded image (overwritten)."""
+        self._check(self.L.rtmb_migrate_shot_f64(self.h, sx, sy, sz, _ptr(rec), _ptr(img64)))
 
     def model_shot_host(self, sx, sy, sz, rec_host):
         self._check(self.L.rtmb_model_shot_host(self.h, sx, sy, sz, _ptr(rec_host)))

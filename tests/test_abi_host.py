@@ -62,3 +62,24 @@ def test_invalid_arguments_are_errors_not_exits():
     p.stencil_order = 7                            # odd order
     assert lib.rtmb_create(C.byref(p), C.byref(h)) == rtmb.RTMB_EINVAL
     assert lib.rtmb_stencil_coefs(3, 1.0, 1.0, 1.0, None) == rtmb.RTMB_EINVAL
+
+
+def test_storage_flag_combinations_are_checked_before_any_device_work():
+    """rtmb_create rejects storage-form flags the library cannot honour (no CUDA call is made)."""
+    import ctypes as C
+    lib = rtmb.load()
+    h = C.c_void_p()
+
+    def create(order, nz, blen, flags):
+        p = rtmb.Params()
+        p.nx = p.ny = 16
+        p.nz, p.blen, p.nt, p.ntstep, p.stencil_order, p.flags = nz, blen, 10, 5, order, flags
+        return lib.rtmb_create(C.byref(p), C.byref(h))
+
+    both = rtmb.FLAG_STORE_F16 | rtmb.FLAG_STORE_BF16
+    assert create(8, 16, 8, both) == rtmb.RTMB_EINVAL
+    assert b"choose one" in lib.rtmb_last_error(None)
+    assert create(8, 16, 8, rtmb.FLAG_IMG_F64) == rtmb.RTMB_EINVAL      # FP64 image needs 16-bit storage
+    assert create(4, 16, 8, rtmb.FLAG_STORE_F16) == rtmb.RTMB_EINVAL    # order 8 only
+    assert create(8, 17, 8, rtmb.FLAG_STORE_BF16) == rtmb.RTMB_EINVAL   # nz + 2 blen = 33: not a multiple of 8
+    assert b"multiple of 8" in lib.rtmb_last_error(None)
