@@ -50,7 +50,12 @@ typedef enum rtmb_status {
 } rtmb_status;
 
 /* Boundary handling of a migration (getRTMBoundaryCondition, include/RTMGrid.hpp:27-57). */
-typedef enum rtmb_boundary { RTMB_BC_ABC = 1, RTMB_BC_HBC = 2, RTMB_BC_RBC = 3 } rtmb_boundary;
+typedef enum rtmb_boundary {
+    RTMB_BC_ABC = 1,
+    RTMB_BC_HBC = 2,
+    RTMB_BC_RBC = 3,
+    RTMB_BC_LEARNED = 4 /* modeling with the learned 8-cell closure (rtmb_closure_*); no reference value */
+} rtmb_boundary;
 
 /* Flags for rtmb_params.flags. */
 #define RTMB_FLAG_FAST_FMA      0x1u  /* contract stencil arithmetic into FMA; not bit-exact with the
@@ -62,7 +67,11 @@ typedef enum rtmb_boundary { RTMB_BC_ABC = 1, RTMB_BC_HBC = 2, RTMB_BC_RBC = 3 }
                                          instead of z in [blen, nze-blen) (CPU, RTMCPUPlatform.cpp:532) */
 #define RTMB_FLAG_NO_TAPER_QUIRK 0x8u /* taper the front-right x-y edge from its own cells instead of
                                          from x = blen (RTMCPUPlatform.cpp:901) */
-#define RTMB_FLAG_USE_GRAPH     0x10u /* capture each time loop in a CUDA graph */
+#define RTMB_FLAG_USE_GRAPH     0x10u /* per-shot drivers: capture the shot's launches in a CUDA
+                                         graph on the context's stream and replay it with one launch;
+                                         the executable graph is updated in place for the next shot.
+                                         Not on the legacy or per-thread default streams, nor while
+                                         rtmb_profile is on (launches then run one by one). */
 #define RTMB_FLAG_NO_TMA        0x20u /* use the plain-load step kernel even when rows are 16-byte
                                          aligned (the TMA-pipelined kernel is the default then) */
 /* Storage forms of the per-shot drivers (no reference counterpart; the reference stores FP32).
@@ -221,6 +230,48 @@ int rtmb_migrate_shot_acc64(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz
 int rtmb_model_shot_f64(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, double *rec);
 int rtmb_migrate_shot_f64(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const float *rec,
                           double *img);
+
+/* ------------------------------------------------------------------ learned boundary closure
+ * No reference counterpart (the reference absorbs with the taper of taper3D, RTMCPUPlatform.cpp:710-920).
+ * A per-cell MLP (55 -> 32 -> 32 -> 1, tanh; BF16 tensor-core GEMMs with FP32 accumulation) closes
+ * an 8-cell strip on every face, so modeling runs on nx+16 x ny+16 x nz+16 instead of nx+2*blen ...:
+ * the network advances the strip's outer 4 cells, the stencil the inner 4.  Inputs per strip cell: the 3x3x3 neighbourhood of p(t) and p(t-1) in the frame of
+ * its nearest face (inward normal first), divided by their max |value| s, and the Courant number
+ * sqrt(v2dt2)/dx; 64 BF16 features per row (the last 9 zero).  Output r: the correction to the
+ * first-order one-way (upwind) update of an outgoing wave, p(t+1) = p + C (p_in - p) + s*clamp(r, +-0.5),
+ * p_in the inward neighbour, C the Courant number.
+ * params: RTMB_CLOSURE_NPARAM floats, W1[32][64], b1[32], W2[32][32], b2[32], w3[32], b3.
+ * Device pointers unless stated; on failure of the context-free calls rtmb_last_error(NULL) describes
+ * the error. */
+#define RTMB_CLOSURE_NPARAM 3169
+#define RTMB_CLOSURE_NIN 64
+int rtmb_closure_param_count(void);
+/* Seeded Glorot-uniform initialisation of host params (biases zero). */
+int rtmb_closure_init(float *params_host, uint64_t seed);
+/* y[i] = network(X[i]) for n rows of BF16 features (X: n*64 bf16). */
+int rtmb_closure_forward(const float *params, const void *X, uint64_t n, float *y, void *cuda_stream);
+/* Gradient of loss = mean_i (network(X[i]) - R[i])^2 with respect to params, and the loss. */
+int rtmb_closure_grad(const float *params, const void *X, const float *R, uint32_t n, float *grad, float *loss,
+                      void *cuda_stream);
+/* Adam training: steps mini-batches of batch rows drawn at random (seeded) from (X, R); params is
+ * updated in place; loss_host (optional, host) receives each step's batch loss.  noise: standard
+ * deviation of Gaussian noise added to the 54 normalised wavefield features of each drawn row. */
+int rtmb_closure_train(float *params, const void *X, const float *R, uint64_t n, uint32_t steps, uint32_t batch,
+                       float lr, float noise, uint64_t seed, float *loss_host, void *cuda_stream);
+/* Training pairs from a modeling shot of the plain method on a wide context (blen >= 16, loaded
+ * v2dt2): the strip of the 8-cell domain nx+16 x ny+16 x nz+16 centred in it, sampled at
+ * per_step random strip cells on steps t0, t0+tstride, ... (cells whose neighbourhood max |p| is
+ * below min_scale are skipped); X (capacity*64 bf16) and R (capacity floats) receive the rows,
+ * *count (host) how many were written. */
+int rtmb_closure_collect(rtmb_ctx *wide, uint32_t sx, uint32_t sy, uint32_t sz, uint32_t t0, uint32_t tstride,
+                         uint32_t per_step, uint64_t seed, float min_scale, void *X, float *R, uint64_t capacity,
+                         uint64_t *count);
+/* Installs params (device or host) in a context with boundary RTMB_BC_LEARNED and blen 8; its
+ * rtmb_model_shot then advances the strip with the network (the stencil runs inside it).  Strip
+ * cells whose neighbourhood max |p| is below min_scale stay zero (the stencil's numerical tail ahead
+ * of the wavefront, where the network is not trained); the others are multiplied by
+ * 1 - damp * ((4 - depth) / 4)^2 each step, depth 0 at the outer face (0 <= damp < 1). */
+int rtmb_closure_set(rtmb_ctx *ctx, const float *params, float min_scale, float damp);
 
 /* Host-buffer forms: copy in, run, copy out, return when the result is on the host. */
 int rtmb_model_shot_host(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, float *rec_host);

@@ -49,7 +49,7 @@ int fail(rtmb_ctx *c, int code, const char *fmt, ...) {
     } while (0)
 
 size_t prof_begin(rtmb_ctx *c, int cat) {
-    if (!c->prof) return (size_t)-1;
+    if (!c->prof || c->capturing) return (size_t)-1;
     if (c->ev_used + 2 > c->ev.size()) {
         for (int k = 0; k < 256; ++k) {
             cudaEvent_t e;
@@ -176,6 +176,67 @@ rtmb::ScaleRec *new_scale(rtmb_ctx *ctx) {
     return ctx->sc_next < ctx->sc_cap ? ctx->d_scale + ctx->sc_next++ : nullptr;
 }
 
+// RTMB_FLAG_USE_GRAPH: a driver's launches between begin() and end() are captured into a CUDA graph
+// on the context's stream and replayed with one cudaGraphLaunch.  The executable graph of each
+// driver kind is kept and updated in place (cudaGraphExecUpdate) when the next shot's graph has
+// the same shape, so a new shot re-captures (host work only) but does not re-instantiate.  Not
+// used on the legacy or per-thread default streams (which cannot be captured), while profiling,
+// or when the caller is already capturing the stream (the launches then go into its graph).
+struct GraphScope {
+    rtmb_ctx *ctx;
+    int kind;
+    bool active = false;
+    GraphScope(rtmb_ctx *c, int k) : ctx(c), kind(k) {}
+    int begin() {
+        if (!(ctx->p.flags & RTMB_FLAG_USE_GRAPH) || ctx->prof || ctx->stream == cudaStreamLegacy ||
+            ctx->stream == cudaStreamPerThread || ctx->stream == nullptr)
+            return RTMB_OK;
+        cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+        CK(cudaStreamIsCapturing(ctx->stream, &st));
+        if (st != cudaStreamCaptureStatusNone) return RTMB_OK;
+        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
+        active = true;
+        ctx->capturing = true;
+        return RTMB_OK;
+    }
+    int end() {
+        if (!active) return RTMB_OK;
+        active = false;
+        ctx->capturing = false;
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamEndCapture(ctx->stream, &g));
+        cudaGraphExec_t &exec = ctx->gexec[kind];
+        if (exec) {
+            cudaGraphExecUpdateResultInfo info;
+            if (cudaGraphExecUpdate(exec, g, &info) != cudaSuccess) {
+                (void)cudaGetLastError();
+                cudaGraphExecDestroy(exec);
+                exec = nullptr;
+            }
+        }
+        if (!exec) {
+            const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+            if (e != cudaSuccess) {
+                exec = nullptr;
+                cudaGraphDestroy(g);
+                return fail(ctx, RTMB_ECUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+            }
+        }
+        cudaGraphDestroy(g);
+        CK(cudaGraphLaunch(exec, ctx->stream));
+        return RTMB_OK;
+    }
+    ~GraphScope() {
+        if (active) {  // an error ended the driver early: end and drop the capture
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(ctx->stream, &g);
+            if (g) cudaGraphDestroy(g);
+            (void)cudaGetLastError();
+            ctx->capturing = false;
+        }
+    }
+};
+
 int check_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz) {
     const rtmb_params &p = ctx->p;
     // RTMController.cpp:149-155 rejects sources outside the model
@@ -207,7 +268,8 @@ void set_receivers(rtmb::StepArgs &a, const rtmb_ctx *c, int mode, float *rec, i
 // wavefields in (*P, *PP) raw (untapered): *P = u(nt-1), *PP = u(nt).  Every buffer it uses must
 // already be set in the context except the taper side buffers, which it allocates when missing.
 int rtmb::driver::run_forward(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, int taper_mode, float *rec,
-                float *upb, float **P_out, float **PP_out, int cat, rtmb::ScaleRec **sc_out) {
+                float *upb, float **P_out, float **PP_out, int cat, rtmb::ScaleRec **sc_out,
+                StepHook *hook) {
     const rtmb_params &p = ctx->p;
     const size_t nb = wave_bytes(ctx);
     const bool st = ctx->store != rtmb::kStoreF32;
@@ -246,7 +308,10 @@ int rtmb::driver::run_forward(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t 
         if (rec) set_receivers(a, ctx, rtmb::kRecSample, rec, (int)it);
         if (upb) { a.upb_mode = rtmb::kUpbSave; a.upb = upb + (size_t)it * upb_step; }
         if (quirk) { a.quirk_in = ctx->d_quirk[(it + 1) % 3]; a.quirk_out = ctx->d_quirk[it % 3]; }
+        int rc;
+        if (hook && (rc = hook->before((int)it, P, PP))) return rc;
         LAUNCH_CAT(cat, rtmb::launch_step(a, (int)p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
+        if (hook && (rc = hook->after((int)it, P, PP))) return rc;
         if (st) scPP = lvl;
     }
     *P_out = P;
@@ -379,6 +444,12 @@ int rtmb_destroy(rtmb_ctx *ctx) {
     for (double *b : ctx->d_f64)
         if (b) cudaFree(b);
     if (ctx->d_upb64) cudaFree(ctx->d_upb64);
+    for (cudaGraphExec_t g : ctx->gexec)
+        if (g) cudaGraphExecDestroy(g);
+    if (ctx->d_cells) cudaFree(ctx->d_cells);
+    if (ctx->d_faces) cudaFree(ctx->d_faces);
+    if (ctx->d_side) cudaFree(ctx->d_side);
+    if (ctx->d_cparams) cudaFree(ctx->d_cparams);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return RTMB_OK;
@@ -513,8 +584,30 @@ int rtmb_model_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, float 
     if ((rc = alloc_driver(ctx))) return rc;
     if (ctx->store != rtmb::kStoreF32 && (rc = reset_scales(ctx))) return rc;
     float *P, *PP;
+    const bool learned = ctx->p.boundary == RTMB_BC_LEARNED;
+    if (learned && !ctx->d_cparams) return fail(ctx, RTMB_EINVAL, "boundary RTMB_BC_LEARNED needs rtmb_closure_set");
+    if (learned && ctx->store != rtmb::kStoreF32)
+        return fail(ctx, RTMB_EINVAL, "the learned closure runs with FP32 storage");
+    // the learned closure: the strip's next level before each step, scattered after it
+    struct Closure : rtmb::driver::StepHook {
+        rtmb_ctx *c;
+        int before(int, const float *P, float *PP) override {
+            ++c->launches;
+            return rtmb::driver::closure_hook_before(c, P, PP);
+        }
+        int after(int, const float *, float *PP) override {
+            ++c->launches;
+            return rtmb::driver::closure_hook_after(c, PP);
+        }
+    } closure;
+    closure.c = ctx;
+    GraphScope graph(ctx, 0);
+    if ((rc = graph.begin())) return rc;
     // RTMFiniteDifferencesKernel.cpp:169-216: taper all faces, step, inject, sample.
-    if ((rc = run_forward(ctx, sx, sy, sz, rtmb::kTaperAll, rec, nullptr, &P, &PP, RTMB_PROF_MODEL))) return rc;
+    if ((rc = run_forward(ctx, sx, sy, sz, learned ? rtmb::kTaperNone : rtmb::kTaperAll, rec, nullptr, &P, &PP,
+                          RTMB_PROF_MODEL, nullptr, learned ? &closure : nullptr)))
+        return rc;
+    if ((rc = graph.end())) return rc;
     return check_err_flag(ctx);
 }
 
@@ -547,6 +640,11 @@ int migrate_impl(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const flo
     if (st && (rc = reset_scales(ctx))) return rc;
     const size_t upb_step = (size_t)ctx->nxe * ctx->nye * ctx->h;
     if (hbc && (rc = ensure(ctx, &ctx->d_upb, upb_step * p.nt, true))) return rc;
+    if (st && ctx->img64 && !acc64 &&
+        (rc = ensure_bytes(ctx, reinterpret_cast<void **>(&ctx->d_img64), ctx->n * sizeof(double), false)))
+        return rc;
+    GraphScope graph(ctx, 1);
+    if ((rc = graph.begin())) return rc;
 
     // forward pass (HBC.cpp:96-210 / RBC.cpp:54-144)
     float *sP, *sPP;
@@ -564,8 +662,6 @@ int migrate_impl(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const flo
     if (st && acc64) {
         img64 = true;
     } else if (st && ctx->img64) {
-        if ((rc = ensure_bytes(ctx, reinterpret_cast<void **>(&ctx->d_img64), ctx->n * sizeof(double), false)))
-            return rc;
         img = ctx->d_img64;
         img64 = true;
     }
@@ -636,6 +732,7 @@ int migrate_impl(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const flo
     if (img != img_out)
         LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_to_float(ctx->d_img64, static_cast<float *>(img_out), ctx->n,
                                                           ctx->stream));
+    if ((rc = graph.end())) return rc;
     return check_err_flag(ctx);
 }
 

@@ -1,0 +1,808 @@
+// closure.cu -- kernels and entry points of the learned absorbing-boundary closure (closure.cuh):
+// strip-cell lists, feature gathering, the tcgen05 MLP forward (training and inference), the
+// backward pass, Adam, training-pair collection on a wide domain, and the per-step inference that
+// the modeling driver runs for boundary RTMB_BC_LEARNED.  No reference counterpart: the reference's
+// absorbing layers are the taper of taper3D / taperUpper3D (RTMCPUPlatform.cpp:566-920).
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include <cuda_bf16.h>
+
+#include "closure.cuh"
+#include "ctx.hpp"
+#include "umma.cuh"
+
+namespace rtmb {
+namespace closure {
+namespace {
+
+// ------------------------------------------------------------------ geometry and features
+
+// Face code (axis * 2 + side) of the box face nearest to box cell (cx, cy, cz) (box-relative), or
+// -1 if the cell is kNet or more cells from every face.  Ties go to the first face in x-low,
+// x-high, y-low, ...
+__host__ __device__ inline int face_of(int cx, int cy, int cz, int nx, int ny, int nz) {
+    const int d[6] = {cx, nx - 1 - cx, cy, ny - 1 - cy, cz, nz - 1 - cz};
+    int best = 0;
+    for (int f = 1; f < 6; ++f)
+        if (d[f] < d[best]) best = f;
+    return d[best] < kNet ? best : -1;
+}
+
+// The 55 features of the cell at array offset off (box-relative coordinates c[3], face f), in
+// FP32, normalised by s (returned; 0 when the neighbourhood is all zero).  base: the first-order
+// one-way (upwind) update of an outgoing wave, p + C (p_in - p) with p_in the inward neighbour at
+// t and C the Courant number; the network predicts the correction to it.
+__device__ inline float gather(const float *__restrict__ P, const float *__restrict__ PP,
+                               const float *__restrict__ V, const Box &b, int cx, int cy, int cz, int f,
+                               float inv_dx, float (&feat)[kUsed], float *base) {
+    const int axis = f >> 1, side = f & 1;
+    const int t1 = axis == 0 ? 1 : 0, t2 = axis == 2 ? 1 : 2;
+    const int c[3] = {cx, cy, cz};
+    const int n[3] = {b.nx, b.ny, b.nz};
+    const size_t plane = (size_t)b.ay * b.az;
+    float s = 0.f;
+#pragma unroll
+    for (int u = -1; u <= 1; ++u)
+#pragma unroll
+        for (int v = -1; v <= 1; ++v)
+#pragma unroll
+            for (int w = -1; w <= 1; ++w) {
+                int q[3] = {c[0], c[1], c[2]};
+                q[axis] += side ? -u : u;
+                q[t1] += v;
+                q[t2] += w;
+                float a = 0.f, bb = 0.f;
+                if (q[0] >= 0 && q[0] < n[0] && q[1] >= 0 && q[1] < n[1] && q[2] >= 0 && q[2] < n[2]) {
+                    const size_t o = (size_t)(q[0] + b.ox) * plane + (size_t)(q[1] + b.oy) * b.az + (q[2] + b.oz);
+                    a = __ldg(P + o);
+                    bb = __ldg(PP + o);
+                }
+                const int j = (u + 1) * 9 + (v + 1) * 3 + (w + 1);
+                feat[j] = a;
+                feat[27 + j] = bb;
+                s = fmaxf(s, fmaxf(fabsf(a), fabsf(bb)));
+            }
+    const size_t o = (size_t)(cx + b.ox) * plane + (size_t)(cy + b.oy) * b.az + (cz + b.oz);
+    const float courant = sqrtf(__ldg(V + o)) * inv_dx;
+    *base = fmaf(courant, feat[22] - feat[13], feat[13]);  // feat[22]: (u, v, w) = (+1, 0, 0)
+    const float inv = s > 0.f ? 1.f / s : 0.f;
+#pragma unroll
+    for (int j = 0; j < 54; ++j) feat[j] *= inv;
+    feat[54] = courant;
+    return s;
+}
+
+// ------------------------------------------------------------------ tcgen05 MLP tile
+
+constexpr int kTile = 128;  // cells per tile = MMA M
+constexpr int kLboA = (kTile / 8) * 128;      // A tiles: 16 row groups of 128 bytes per K chunk
+constexpr int kLboB = (kHid / 8) * 128;       // B tiles: 4 row groups per K chunk
+constexpr uint32_t kIdesc = umma::idesc_bf16_f32(kTile, kHid);
+constexpr uint32_t kTmemCols = 64;            // [0, 32): layer 1, [32, 64): layer 2
+constexpr float kMaxCorr = 0.5f;              // bound on the network's correction, in units of s
+
+struct __align__(128) MlpSmem {
+    unsigned char a1[kTile * kIn * 2];   // features, BF16, K-major
+    unsigned char a2[kTile * kHid * 2];  // hidden layer 1, BF16, K-major
+    unsigned char w1[kHid * kIn * 2];    // W1 (N = 32 rows, K = 64)
+    unsigned char w2[kHid * kHid * 2];   // W2
+    float b1[kHid], b2[kHid], w3[kHid], b3;
+    uint64_t bar;
+    uint32_t tmem;
+    // keeps every descriptor-addressed read of the MMAs inside this CTA's shared memory even if
+    // the operand strides were read the other way round (A would then span 44 KB from a1)
+    unsigned char pad[16384];
+};
+
+__device__ __forceinline__ bool bar_wait(uint64_t *bar, uint32_t parity) {
+    auto try_wait = [&]() {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(umma::smem_addr(bar)), "r"(parity)
+            : "memory");
+        return ok != 0;
+    };
+    if (try_wait()) return true;
+    const long long t0 = clock64();
+    while (!try_wait())
+        if (clock64() - t0 > (1ll << 32)) return false;
+    return true;
+}
+
+// Weights into shared memory (BF16, canonical K-major), biases and w3 in FP32; TMEM allocation and
+// the MMA barrier.  Every thread of the 128-thread CTA calls it.
+__device__ void mlp_setup(MlpSmem &sm, const float *__restrict__ prm) {
+    const int tid = threadIdx.x;
+    if (tid < 32) umma::tmem_alloc(&sm.tmem, kTmemCols);
+    for (int i = tid; i < kHid * kIn; i += kTile) {
+        const int r = i / kIn, k = i % kIn;
+        *reinterpret_cast<__nv_bfloat16 *>(sm.w1 + umma::kmajor_offset(r, k, kLboB)) =
+            __float2bfloat16_rn(prm[kOffW1 + i]);
+    }
+    for (int i = tid; i < kHid * kHid; i += kTile) {
+        const int r = i / kHid, k = i % kHid;
+        *reinterpret_cast<__nv_bfloat16 *>(sm.w2 + umma::kmajor_offset(r, k, kLboB)) =
+            __float2bfloat16_rn(prm[kOffW2 + i]);
+    }
+    if (tid < kHid) {
+        sm.b1[tid] = prm[kOffB1 + tid];
+        sm.b2[tid] = prm[kOffB2 + tid];
+        sm.w3[tid] = prm[kOffW3 + tid];
+    }
+    if (tid == 0) {
+        sm.b3 = prm[kOffB3];
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(umma::smem_addr(&sm.bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+}
+
+// Writes row m of the feature tile from 64 FP32 values (BF16-rounded), 16 bytes at a time.
+__device__ __forceinline__ void put_row(unsigned char *tile, int m, const float *f, int nk, int lbo) {
+    for (int c = 0; c < nk / 8; ++c) {
+        __nv_bfloat162 h[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) h[j] = __floats2bfloat162_rn(f[8 * c + 2 * j], f[8 * c + 2 * j + 1]);
+        *reinterpret_cast<uint4 *>(tile + umma::kmajor_offset(m, 8 * c, lbo)) = *reinterpret_cast<uint4 *>(h);
+    }
+}
+
+// One tile: the caller has written every row of a1.  Returns, for this thread's row, y (the network
+// output) and optionally the hidden activations (h1 rounded to BF16, as layer 2 sees it; h2 FP32).
+// phase: the MMA barrier's next parity, advanced by two.  false: a wait ran out (uniform).
+__device__ bool mlp_tile(MlpSmem &sm, uint32_t &phase, float *y, float *h1_out, float *h2_out) {
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t lane_base = sm.tmem + ((uint32_t)(warp * 32) << 16);
+    umma::fence_smem_to_async();
+    umma::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+        umma::fence_after_sync();
+#pragma unroll
+        for (int s = 0; s < kIn / 16; ++s)
+            umma::mma_bf16(sm.tmem, umma::smem_desc(sm.a1 + s * 2 * kLboA, kLboA, 128),
+                           umma::smem_desc(sm.w1 + s * 2 * kLboB, kLboB, 128), kIdesc, s > 0);
+        umma::commit(&sm.bar);
+    }
+    bool ok = __syncthreads_and(bar_wait(&sm.bar, phase & 1));
+    phase ^= 1;
+    if (!ok) return false;
+    umma::fence_after_sync();
+    float h[32];
+    umma::tmem_ld32(lane_base, h);
+    float hb[32];
+#pragma unroll
+    for (int j = 0; j < kHid; ++j) {
+        const float t = tanhf(h[j] + sm.b1[j]);
+        hb[j] = __bfloat162float(__float2bfloat16_rn(t));
+        if (h1_out) h1_out[j] = hb[j];
+    }
+    put_row(sm.a2, tid, hb, kHid, kLboA);
+    umma::fence_smem_to_async();
+    umma::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+        umma::fence_after_sync();
+#pragma unroll
+        for (int s = 0; s < kHid / 16; ++s)
+            umma::mma_bf16(sm.tmem + kHid, umma::smem_desc(sm.a2 + s * 2 * kLboA, kLboA, 128),
+                           umma::smem_desc(sm.w2 + s * 2 * kLboB, kLboB, 128), kIdesc, s > 0);
+        umma::commit(&sm.bar);
+    }
+    ok = __syncthreads_and(bar_wait(&sm.bar, phase & 1));
+    phase ^= 1;
+    if (!ok) return false;
+    umma::fence_after_sync();
+    umma::tmem_ld32(lane_base + kHid, h);
+    float acc = sm.b3;
+#pragma unroll
+    for (int j = 0; j < kHid; ++j) {
+        const float t = tanhf(h[j] + sm.b2[j]);
+        if (h2_out) h2_out[j] = t;
+        acc = fmaf(sm.w3[j], t, acc);
+    }
+    *y = acc;
+    umma::fence_before_sync();  // the next tile's MMAs overwrite TMEM after the next barrier
+    return true;
+}
+
+__device__ void mlp_teardown(MlpSmem &sm) {
+    umma::fence_before_sync();
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        umma::fence_after_sync();
+        umma::tmem_dealloc(sm.tmem, kTmemCols);
+    }
+}
+
+// ------------------------------------------------------------------ kernels
+
+// y[i] = MLP(X[i]) for n rows of BF16 features; optionally the hidden activations (training).
+__global__ void __launch_bounds__(kTile) mlp_forward_kernel(const float *__restrict__ prm,
+                                                            const __nv_bfloat16 *__restrict__ X, long long n,
+                                                            float *y, float *H1, float *H2, unsigned *err) {
+    __shared__ MlpSmem sm;
+    mlp_setup(sm, prm);
+    uint32_t phase = 0;
+    const long long ntiles = (n + kTile - 1) / kTile;
+    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const long long row = t * kTile + threadIdx.x;
+        float f[kIn];
+        if (row < n) {
+            const uint4 *src = reinterpret_cast<const uint4 *>(X + row * kIn);
+#pragma unroll
+            for (int c = 0; c < kIn / 8; ++c) {
+                const uint4 u = __ldg(src + c);
+                const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&u);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const float2 v = __bfloat1622float2(h[j]);
+                    f[8 * c + 2 * j] = v.x;
+                    f[8 * c + 2 * j + 1] = v.y;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kIn; ++k) f[k] = 0.f;
+        }
+        put_row(sm.a1, threadIdx.x, f, kIn, kLboA);
+        float out, h1[kHid], h2[kHid];
+        const bool train = H1 != nullptr;
+        if (!mlp_tile(sm, phase, &out, train ? h1 : nullptr, train ? h2 : nullptr)) {
+            if (threadIdx.x == 0 && err) atomicOr(err, 2u);
+            break;
+        }
+        if (row < n) {
+            y[row] = out;
+            if (train) {
+#pragma unroll
+                for (int j = 0; j < kHid; ++j) {
+                    H1[row * kHid + j] = h1[j];
+                    H2[row * kHid + j] = h2[j];
+                }
+            }
+        }
+    }
+    mlp_teardown(sm);
+}
+
+// Per-step inference on the strip: side[i] = p(t+1) of strip cell i.
+__global__ void __launch_bounds__(kTile) strip_step_kernel(const float *__restrict__ prm,
+                                                           const float *__restrict__ P,
+                                                           const float *__restrict__ PP,
+                                                           const float *__restrict__ V, Box b,
+                                                           const uint32_t *__restrict__ cells,
+                                                           const uint8_t *__restrict__ faces, long long ncells,
+                                                           float inv_dx, float min_scale, float damp, float *side,
+                                                           unsigned *err) {
+    __shared__ MlpSmem sm;
+    mlp_setup(sm, prm);
+    uint32_t phase = 0;
+    const long long ntiles = (ncells + kTile - 1) / kTile;
+    const size_t plane = (size_t)b.ay * b.az;
+    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const long long i = t * kTile + threadIdx.x;
+        float f[kIn];
+        float s = 0.f, base = 0.f, keep = 1.f;
+        if (i < ncells) {
+            const uint32_t off = cells[i];
+            const int cx = (int)(off / plane) - b.ox, cy = (int)((off % plane) / b.az) - b.oy,
+                      cz = (int)(off % b.az) - b.oz;
+            const int fc = faces[i], ax = fc >> 1;
+            const int c[3] = {cx, cy, cz}, n[3] = {b.nx, b.ny, b.nz};
+            const int depth = (fc & 1) ? n[ax] - 1 - c[ax] : c[ax];  // 0 at the outer face
+            const float u = (float)(kNet - depth) / kNet;
+            keep = 1.f - damp * u * u;
+            float feat[kUsed];
+            s = gather(P, PP, V, b, cx, cy, cz, fc, inv_dx, feat, &base);
+#pragma unroll
+            for (int k = 0; k < kUsed; ++k) f[k] = feat[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < kUsed; ++k) f[k] = 0.f;
+        }
+#pragma unroll
+        for (int k = kUsed; k < kIn; ++k) f[k] = 0.f;
+        put_row(sm.a1, threadIdx.x, f, kIn, kLboA);
+        float r;
+        if (!mlp_tile(sm, phase, &r, nullptr, nullptr)) {
+            if (threadIdx.x == 0 && err) atomicOr(err, 2u);
+            break;
+        }
+        if (i < ncells) {
+            // below min_scale the neighbourhood holds only the stencil's numerical tail ahead of
+            // the wavefront (the network was not trained there): the strip cell stays at zero.
+            // The new value is kept within the neighbourhood's range [-s, s], so the network can
+            // never amplify what reaches the strip from one step to the next.
+            const float rc = fminf(kMaxCorr, fmaxf(-kMaxCorr, r));
+            const float o = s < min_scale ? 0.f : fminf(s, fmaxf(-s, keep * fmaf(s, rc, base)));
+            side[i] = o;
+            if (o != o && err) atomicOr(err, 1u);
+        }
+    }
+    mlp_teardown(sm);
+}
+
+__global__ void strip_scatter_kernel(float *PP, const uint32_t *__restrict__ cells, const float *__restrict__ side,
+                                     long long ncells) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ncells; i += (long long)gridDim.x * blockDim.x)
+        PP[cells[i]] = side[i];
+}
+
+__host__ __device__ inline uint64_t mix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+// Training-pair collection, before the step: features of cells_per_step strip cells drawn at
+// random (seeded) from p(t) = P and p(t-1) = PP.  Cells whose neighbourhood max |p| is below
+// min_scale are skipped: far ahead of the wavefront the stencil's numerical tail is orders of
+// magnitude below the waves the closure must absorb.
+__global__ void sample_features_kernel(const float *__restrict__ P, const float *__restrict__ PP,
+                                       const float *__restrict__ V, Box b, const uint32_t *__restrict__ cells,
+                                       const uint8_t *__restrict__ faces, long long ncells, int per_step,
+                                       uint64_t key, float inv_dx, float min_scale, __nv_bfloat16 *X,
+                                       unsigned long long cap,
+                                       unsigned long long *count, long long *slot_of, float *stash) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= per_step) return;
+    const long long i = (long long)(mix64(key + (uint64_t)j) % (uint64_t)ncells);
+    const uint32_t off = cells[i];
+    const size_t plane = (size_t)b.ay * b.az;
+    const int cx = (int)(off / plane) - b.ox, cy = (int)((off % plane) / b.az) - b.oy, cz = (int)(off % b.az) - b.oz;
+    float feat[kUsed], base;
+    const float s = gather(P, PP, V, b, cx, cy, cz, faces[i], inv_dx, feat, &base);
+    slot_of[j] = -1;
+    if (!(s > 0.f) || s < min_scale) return;
+    const unsigned long long slot = atomicAdd(count, 1ull);
+    if (slot >= cap) return;
+    slot_of[j] = (long long)slot;
+    stash[3 * j] = __uint_as_float(off);
+    stash[3 * j + 1] = base;
+    stash[3 * j + 2] = s;
+    __nv_bfloat16 *row = X + slot * kIn;
+    for (int k = 0; k < kIn; ++k) row[k] = __float2bfloat16_rn(k < kUsed ? feat[k] : 0.f);
+}
+
+// ... after the step: the target r = (p(t+1) - base) / s.
+__global__ void sample_target_kernel(const float *__restrict__ PPnew, int per_step, const long long *slot_of,
+                                     const float *stash, float *R) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= per_step || slot_of[j] < 0) return;
+    const uint32_t off = __float_as_uint(stash[3 * j]);
+    R[slot_of[j]] = (PPnew[off] - stash[3 * j + 1]) / stash[3 * j + 2];
+}
+
+// Random mini-batch (with replacement, seeded): rows of (X, R) into (Xb, Rb).
+// With noise > 0 the 54 wavefield features get Gaussian noise of that standard deviation (the
+// features are normalised to max 1), so that the network is trained on inputs a little off the
+// data, as it meets them when its own outputs feed back step after step.
+__global__ void gather_batch_kernel(const __nv_bfloat16 *__restrict__ X, const float *__restrict__ R, long long n,
+                                    int B, uint64_t key, float noise, __nv_bfloat16 *Xb, float *Rb) {
+    const int i = blockIdx.x;
+    const long long src = (long long)(mix64(key + (uint64_t)i) % (uint64_t)n);
+    const int k0 = 2 * threadIdx.x;  // 32 threads x 2 features
+    __nv_bfloat162 v = reinterpret_cast<const __nv_bfloat162 *>(X + src * kIn)[threadIdx.x];
+    if (noise > 0.f && k0 < 54) {
+        const uint64_t h = mix64(key ^ (0xD1B54A32D192ED03ull * (uint64_t)(i * 32 + threadIdx.x + 1)));
+        const float u1 = ((h >> 40) + 1) * (1.0f / 16777217.0f), u2 = ((h >> 16) & 0xFFFFFF) * (1.0f / 16777216.0f);
+        const float r = sqrtf(-2.f * logf(u1));
+        float2 f = __bfloat1622float2(v);
+        f.x += noise * r * cosf(6.2831853f * u2);
+        f.y += noise * r * sinf(6.2831853f * u2);
+        v = __floats2bfloat162_rn(f.x, f.y);
+    }
+    reinterpret_cast<__nv_bfloat162 *>(Xb + (long long)i * kIn)[threadIdx.x] = v;
+    if (threadIdx.x == 0) Rb[i] = R[src];
+}
+
+// Backward, per row: loss contribution and the pre-activation gradients of both hidden layers.
+// The network as trained: z1 = W1b x + b1, h1 = bf16(tanh z1), z2 = W2b h1 + b2, h2 = tanh z2,
+// y = w3 . h2 + b3 with W1b, W2b the BF16 weights; loss = mean (y - r)^2.  Gradients treat the BF16
+// roundings as identity (straight-through).
+__global__ void backward_rows_kernel(const float *__restrict__ prm, const float *__restrict__ y,
+                                     const float *__restrict__ R, const float *__restrict__ H1,
+                                     const float *__restrict__ H2, int B, float *dZ1, float *dZ2, float *dY,
+                                     float *loss) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.f;
+    if (i < B) {
+        const float e = y[i] - R[i];
+        l = e * e / B;
+        const float dy = 2.f * e / B;
+        dY[i] = dy;
+        float d2[kHid];
+#pragma unroll
+        for (int j = 0; j < kHid; ++j) {
+            const float h = H2[(long long)i * kHid + j];
+            d2[j] = dy * prm[kOffW3 + j] * (1.f - h * h);
+            dZ2[(long long)i * kHid + j] = d2[j];
+        }
+#pragma unroll 4
+        for (int k = 0; k < kHid; ++k) {
+            float a = 0.f;
+#pragma unroll
+            for (int j = 0; j < kHid; ++j)
+                a = fmaf(__bfloat162float(__float2bfloat16_rn(prm[kOffW2 + j * kHid + k])), d2[j], a);
+            const float h = H1[(long long)i * kHid + k];
+            dZ1[(long long)i * kHid + k] = a * (1.f - h * h);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, l);
+}
+
+// Parameter gradients: one thread per parameter, summing over the B rows of the batch.
+__global__ void grad_reduce_kernel(const __nv_bfloat16 *__restrict__ Xb, const float *__restrict__ H1,
+                                   const float *__restrict__ H2, const float *__restrict__ dZ1,
+                                   const float *__restrict__ dZ2, const float *__restrict__ dY, int B, float *g) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= kNParam) return;
+    float a = 0.f;
+    if (p < kOffB1) {
+        const int j = p / kIn, k = p % kIn;
+        for (int i = 0; i < B; ++i) a = fmaf(dZ1[(long long)i * kHid + j], __bfloat162float(Xb[(long long)i * kIn + k]), a);
+    } else if (p < kOffW2) {
+        const int j = p - kOffB1;
+        for (int i = 0; i < B; ++i) a += dZ1[(long long)i * kHid + j];
+    } else if (p < kOffB2) {
+        const int j = (p - kOffW2) / kHid, k = (p - kOffW2) % kHid;
+        for (int i = 0; i < B; ++i) a = fmaf(dZ2[(long long)i * kHid + j], H1[(long long)i * kHid + k], a);
+    } else if (p < kOffW3) {
+        const int j = p - kOffB2;
+        for (int i = 0; i < B; ++i) a += dZ2[(long long)i * kHid + j];
+    } else if (p < kOffB3) {
+        const int j = p - kOffW3;
+        for (int i = 0; i < B; ++i) a = fmaf(dY[i], H2[(long long)i * kHid + j], a);
+    } else {
+        for (int i = 0; i < B; ++i) a += dY[i];
+    }
+    g[p] = a;
+}
+
+// Adam (beta1 0.9, beta2 0.999, eps 1e-8) with bias correction; step counts from 1.
+__global__ void adam_kernel(float *prm, const float *__restrict__ g, float *m, float *v, int step, float lr) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= kNParam) return;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float mm = b1 * m[p] + (1.f - b1) * g[p];
+    const float vv = b2 * v[p] + (1.f - b2) * g[p] * g[p];
+    m[p] = mm;
+    v[p] = vv;
+    const float mh = mm / (1.f - powf(b1, (float)step)), vh = vv / (1.f - powf(b2, (float)step));
+    prm[p] -= lr * mh / (sqrtf(vh) + 1e-8f);
+}
+
+int grid_for(long long tiles) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long g = (long long)sms * 6;
+    return (int)(tiles < g ? (tiles > 0 ? tiles : 1) : g);
+}
+
+}  // namespace
+
+// The network's cells of box b (the outer kNet cells of its strip), ordered by array offset, with
+// their face codes.
+void strip_cells(const Box &b, std::vector<uint32_t> &cells, std::vector<uint8_t> &faces) {
+    cells.clear();
+    faces.clear();
+    for (int x = 0; x < b.nx; ++x)
+        for (int y = 0; y < b.ny; ++y) {
+            const bool full = x < kNet || x >= b.nx - kNet || y < kNet || y >= b.ny - kNet;
+            for (int z = 0; z < b.nz; ++z) {
+                if (!full && z == kNet && b.nz - kNet > kNet) z = b.nz - kNet;
+                const int f = face_of(x, y, z, b.nx, b.ny, b.nz);
+                if (f < 0) continue;
+                cells.push_back((uint32_t)(((size_t)(x + b.ox) * b.ay + (y + b.oy)) * b.az + (z + b.oz)));
+                faces.push_back((uint8_t)f);
+            }
+        }
+}
+
+cudaError_t launch_strip_step(const float *prm, const float *P, const float *PP, const float *V, const Box &b,
+                              const uint32_t *cells, const uint8_t *faces, long long ncells, float inv_dx,
+                              float min_scale, float damp, float *side, unsigned *err, cudaStream_t s) {
+    const long long tiles = (ncells + kTile - 1) / kTile;
+    strip_step_kernel<<<grid_for(tiles), kTile, 0, s>>>(prm, P, PP, V, b, cells, faces, ncells, inv_dx, min_scale,
+                                                        damp, side, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_strip_scatter(float *PP, const uint32_t *cells, const float *side, long long ncells,
+                                 cudaStream_t s) {
+    const long long blocks = (ncells + 255) / 256;
+    strip_scatter_kernel<<<(unsigned)(blocks < 148 * 32 ? (blocks > 0 ? blocks : 1) : 148 * 32), 256, 0, s>>>(
+        PP, cells, side, ncells);
+    return cudaGetLastError();
+}
+
+}  // namespace closure
+}  // namespace rtmb
+
+// ------------------------------------------------------------------ entry points
+
+using namespace rtmb::closure;
+
+namespace {
+
+thread_local std::string g_closure_err;
+
+int cfail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    return rtmb::driver::fail_noctx(code, buf);
+}
+
+#define CKC(call)                                                                                 \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return cfail(e_ == cudaErrorMemoryAllocation ? RTMB_ENOMEM : RTMB_ECUDA, "%s: %s", #call, \
+                         cudaGetErrorString(e_));                                                 \
+    } while (0)
+
+// Reads and clears an error word; maps bit 1 to ETIMEOUT and bit 0 to ENAN.
+int read_err(unsigned *d_err, cudaStream_t s) {
+    unsigned h = 0;
+    CKC(cudaMemcpyAsync(&h, d_err, sizeof h, cudaMemcpyDeviceToHost, s));
+    CKC(cudaStreamSynchronize(s));
+    if (h & 2u) return cfail(RTMB_ETIMEOUT, "closure: a bounded wait for a tensor-core MMA ran out");
+    if (h & 1u) return cfail(RTMB_ENAN, "closure: a NaN appeared");
+    return RTMB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rtmb_closure_param_count(void) { return kNParam; }
+
+int rtmb_closure_init(float *params, uint64_t seed) {
+    if (!params) return cfail(RTMB_EINVAL, "rtmb_closure_init: null pointer");
+    std::memset(params, 0, sizeof(float) * kNParam);
+    uint64_t st = seed ? seed : 1;
+    auto uni = [&]() {  // xorshift64*, uniform in [-1, 1)
+        st ^= st >> 12; st ^= st << 25; st ^= st >> 27;
+        return (double)((st * 2685821657736338717ull) >> 11) / 4503599627370496.0 - 1.0;
+    };
+    const double a1 = std::sqrt(6.0 / (kUsed + kHid)), a2 = std::sqrt(6.0 / (2 * kHid)), a3 = std::sqrt(6.0 / (kHid + 1));
+    for (int j = 0; j < kHid; ++j)
+        for (int k = 0; k < kUsed; ++k) params[kOffW1 + j * kIn + k] = (float)(a1 * uni());
+    for (int i = 0; i < kHid * kHid; ++i) params[kOffW2 + i] = (float)(a2 * uni());
+    for (int j = 0; j < kHid; ++j) params[kOffW3 + j] = (float)(a3 * uni());
+    return RTMB_OK;
+}
+
+int rtmb_closure_forward(const float *params, const void *X, uint64_t n, float *y, void *stream) {
+    if (!params || (!X && n) || (!y && n)) return cfail(RTMB_EINVAL, "rtmb_closure_forward: null pointer");
+    if (!n) return RTMB_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    unsigned *err = nullptr;
+    CKC(cudaMallocAsync(&err, sizeof(unsigned), s));
+    CKC(cudaMemsetAsync(err, 0, sizeof(unsigned), s));
+    const long long tiles = ((long long)n + kTile - 1) / kTile;
+    mlp_forward_kernel<<<grid_for(tiles), kTile, 0, s>>>(params, static_cast<const __nv_bfloat16 *>(X), (long long)n,
+                                                         y, nullptr, nullptr, err);
+    CKC(cudaGetLastError());
+    const int rc = read_err(err, s);
+    cudaFreeAsync(err, s);
+    return rc;
+}
+
+int rtmb_closure_grad(const float *params, const void *X, const float *R, uint32_t n, float *grad, float *loss,
+                      void *stream) {
+    if (!params || !X || !R || !grad || !loss || !n) return cfail(RTMB_EINVAL, "rtmb_closure_grad: bad argument");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    float *buf = nullptr;
+    const size_t nb = (size_t)n * (1 + 4 * kHid + 1);
+    CKC(cudaMallocAsync(&buf, nb * sizeof(float) + 16, s));
+    float *y = buf, *H1 = y + n, *H2 = H1 + (size_t)n * kHid, *dZ1 = H2 + (size_t)n * kHid,
+          *dZ2 = dZ1 + (size_t)n * kHid, *dY = dZ2 + (size_t)n * kHid;
+    unsigned *err = reinterpret_cast<unsigned *>(buf + nb);
+    CKC(cudaMemsetAsync(err, 0, sizeof(unsigned), s));
+    CKC(cudaMemsetAsync(loss, 0, sizeof(float), s));
+    const auto *Xb = static_cast<const __nv_bfloat16 *>(X);
+    const long long tiles = ((long long)n + kTile - 1) / kTile;
+    mlp_forward_kernel<<<grid_for(tiles), kTile, 0, s>>>(params, Xb, n, y, H1, H2, err);
+    backward_rows_kernel<<<(n + 127) / 128, 128, 0, s>>>(params, y, R, H1, H2, (int)n, dZ1, dZ2, dY, loss);
+    grad_reduce_kernel<<<(kNParam + 127) / 128, 128, 0, s>>>(Xb, H1, H2, dZ1, dZ2, dY, (int)n, grad);
+    CKC(cudaGetLastError());
+    const int rc = read_err(err, s);
+    cudaFreeAsync(buf, s);
+    return rc;
+}
+
+int rtmb_closure_train(float *params, const void *X, const float *R, uint64_t n, uint32_t steps, uint32_t batch,
+                       float lr, float noise, uint64_t seed, float *loss_host, void *stream) {
+    if (!params || !X || !R || !n || !batch || batch > 65536) return cfail(RTMB_EINVAL, "rtmb_closure_train: bad argument");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t B = batch;
+    const size_t nf = 3 * kNParam + B * (2 + 4 * kHid + 1) + steps + 4;
+    float *buf = nullptr;
+    __nv_bfloat16 *Xb = nullptr;
+    CKC(cudaMallocAsync(&buf, nf * sizeof(float), s));
+    CKC(cudaMallocAsync(&Xb, B * kIn * sizeof(__nv_bfloat16), s));
+    CKC(cudaMemsetAsync(buf, 0, nf * sizeof(float), s));
+    float *g = buf, *m = g + kNParam, *v = m + kNParam, *Rb = v + kNParam, *y = Rb + B, *H1 = y + B,
+          *H2 = H1 + B * kHid, *dZ1 = H2 + B * kHid, *dZ2 = dZ1 + B * kHid, *dY = dZ2 + B * kHid, *losses = dY + B;
+    unsigned *err = reinterpret_cast<unsigned *>(losses + steps);
+    const auto *Xd = static_cast<const __nv_bfloat16 *>(X);
+    const long long tiles = ((long long)B + kTile - 1) / kTile;
+    const int fgrid = grid_for(tiles);
+    for (uint32_t st = 0; st < steps; ++st) {
+        gather_batch_kernel<<<(unsigned)B, 32, 0, s>>>(Xd, R, (long long)n, (int)B, mix64(seed * 1000003ull + st), noise,
+                                                       Xb, Rb);
+        mlp_forward_kernel<<<fgrid, kTile, 0, s>>>(params, Xb, (long long)B, y, H1, H2, err);
+        backward_rows_kernel<<<(unsigned)((B + 127) / 128), 128, 0, s>>>(params, y, Rb, H1, H2, (int)B, dZ1, dZ2, dY,
+                                                                       losses + st);
+        grad_reduce_kernel<<<(kNParam + 127) / 128, 128, 0, s>>>(Xb, H1, H2, dZ1, dZ2, dY, (int)B, g);
+        adam_kernel<<<(kNParam + 127) / 128, 128, 0, s>>>(params, g, m, v, (int)st + 1, lr);
+        CKC(cudaGetLastError());
+    }
+    if (loss_host) CKC(cudaMemcpyAsync(loss_host, losses, steps * sizeof(float), cudaMemcpyDeviceToHost, s));
+    const int rc = read_err(err, s);
+    cudaFreeAsync(Xb, s);
+    cudaFreeAsync(buf, s);
+    return rc;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Collection of training pairs around the steps of a wide-domain modeling shot.
+struct CollectHook : rtmb::driver::StepHook {
+    rtmb_ctx *ctx;
+    Box box;
+    const uint32_t *cells;
+    const uint8_t *faces;
+    long long ncells;
+    int t0, tstride, per_step;
+    uint64_t seed;
+    float inv_dx, min_scale;
+    __nv_bfloat16 *X;
+    float *R;
+    unsigned long long cap, *count;
+    long long *slot_of;
+    float *stash;
+    bool due(int it) const { return it >= t0 && (it - t0) % tstride == 0; }
+    int before(int it, const float *P, float *PP) override {
+        if (!due(it)) return 0;
+        sample_features_kernel<<<(per_step + 127) / 128, 128, 0, ctx->stream>>>(
+            P, PP, ctx->d_v2dt2, box, cells, faces, ncells, per_step, mix64(seed ^ (0x5851F42D4C957F2Dull * (it + 1))),
+            inv_dx, min_scale, X, cap, count, slot_of, stash);
+        ++ctx->launches;
+        return cudaGetLastError() == cudaSuccess ? 0 : RTMB_ECUDA;
+    }
+    int after(int it, const float *, float *PP) override {
+        if (!due(it)) return 0;
+        sample_target_kernel<<<(per_step + 127) / 128, 128, 0, ctx->stream>>>(PP, per_step, slot_of, stash, R);
+        ++ctx->launches;
+        return cudaGetLastError() == cudaSuccess ? 0 : RTMB_ECUDA;
+    }
+};
+
+}  // namespace
+
+int rtmb::driver::closure_hook_before(rtmb_ctx *ctx, const float *P, float *PP) {
+    const Box b{ctx->nxe, ctx->nye, ctx->nze, 0, 0, 0, ctx->nxe, ctx->nye, ctx->nze};
+    return launch_strip_step(ctx->d_cparams, P, PP, ctx->d_v2dt2, b, ctx->d_cells, ctx->d_faces, ctx->ncells,
+                             1.f / ctx->p.dx, ctx->closure_min_scale, ctx->closure_damp, ctx->d_side, ctx->d_err,
+                             ctx->stream) == cudaSuccess
+               ? 0
+               : RTMB_ECUDA;
+}
+
+int rtmb::driver::closure_hook_after(rtmb_ctx *ctx, float *PP) {
+    return launch_strip_scatter(PP, ctx->d_cells, ctx->d_side, ctx->ncells, ctx->stream) == cudaSuccess ? 0 : RTMB_ECUDA;
+}
+
+extern "C" {
+
+int rtmb_closure_set(rtmb_ctx *ctx, const float *params, float min_scale, float damp) {
+    if (!ctx || !params || !(min_scale >= 0.f) || !(damp >= 0.f && damp < 1.f)) return RTMB_EINVAL;
+    ctx->closure_min_scale = min_scale;
+    ctx->closure_damp = damp;
+    if (ctx->p.boundary != RTMB_BC_LEARNED || ctx->p.blen != (uint32_t)kStrip) {
+        ctx->err = "rtmb_closure_set: the context needs boundary RTMB_BC_LEARNED and blen 8";
+        return RTMB_EINVAL;
+    }
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return RTMB_ECUDA;
+    if (!ctx->d_cells) {
+        const Box b{ctx->nxe, ctx->nye, ctx->nze, 0, 0, 0, ctx->nxe, ctx->nye, ctx->nze};
+        std::vector<uint32_t> cells;
+        std::vector<uint8_t> faces;
+        if (ctx->n > 0xFFFFFFFFull) {
+            ctx->err = "rtmb_closure_set: grids above 2^32 points are not supported";
+            return RTMB_EINVAL;
+        }
+        strip_cells(b, cells, faces);
+        ctx->ncells = (long long)cells.size();
+        if (cudaMalloc(&ctx->d_cells, cells.size() * sizeof(uint32_t)) != cudaSuccess ||
+            cudaMalloc(&ctx->d_faces, faces.size()) != cudaSuccess ||
+            cudaMalloc(&ctx->d_side, cells.size() * sizeof(float)) != cudaSuccess ||
+            cudaMalloc(&ctx->d_cparams, kNParam * sizeof(float)) != cudaSuccess) {
+            ctx->err = "rtmb_closure_set: device allocation failed";
+            return RTMB_ENOMEM;
+        }
+        if (cudaMemcpy(ctx->d_cells, cells.data(), cells.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(ctx->d_faces, faces.data(), faces.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+            return RTMB_ECUDA;
+    }
+    if (cudaMemcpyAsync(ctx->d_cparams, params, kNParam * sizeof(float), cudaMemcpyDefault, ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        return RTMB_ECUDA;
+    return RTMB_OK;
+}
+
+int rtmb_closure_collect(rtmb_ctx *wide, uint32_t sx, uint32_t sy, uint32_t sz, uint32_t t0, uint32_t tstride,
+                         uint32_t per_step, uint64_t seed, float min_scale, void *X, float *R, uint64_t capacity,
+                         uint64_t *count) {
+    if (!wide || !X || !R || !count || !tstride || !per_step) return RTMB_EINVAL;
+    rtmb_ctx *ctx = wide;
+    const rtmb_params &p = ctx->p;
+    if (p.blen < (uint32_t)kStrip + 8) {
+        ctx->err = "rtmb_closure_collect: the wide context's border must be wider than the 8-cell strip";
+        return RTMB_EINVAL;
+    }
+    int rc = rtmb::driver::check_model_shot(ctx, sx, sy, sz);
+    if (rc) return rc;
+    if (!ctx->d_w[0] && (cudaMalloc(&ctx->d_w[0], ctx->n * sizeof(float)) != cudaSuccess ||
+                         cudaMalloc(&ctx->d_w[1], ctx->n * sizeof(float)) != cudaSuccess))
+        return RTMB_ENOMEM;
+    const int o = (int)p.blen - kStrip;
+    const Box box{ctx->nxe, ctx->nye, ctx->nze, o, o, o, (int)p.nx + 2 * kStrip, (int)p.ny + 2 * kStrip,
+                  (int)p.nz + 2 * kStrip};
+    std::vector<uint32_t> cells;
+    std::vector<uint8_t> faces;
+    strip_cells(box, cells, faces);
+    uint32_t *d_cells = nullptr;
+    uint8_t *d_faces = nullptr;
+    long long *slot_of = nullptr;
+    float *stash = nullptr;
+    unsigned long long *d_count = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(d_cells); cudaFree(d_faces); cudaFree(slot_of); cudaFree(stash); cudaFree(d_count);
+    };
+    if (cudaMalloc(&d_cells, cells.size() * 4) != cudaSuccess || cudaMalloc(&d_faces, faces.size()) != cudaSuccess ||
+        cudaMalloc(&slot_of, per_step * sizeof(long long)) != cudaSuccess ||
+        cudaMalloc(&stash, 3 * (size_t)per_step * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&d_count, sizeof(unsigned long long)) != cudaSuccess) {
+        cleanup();
+        return RTMB_ENOMEM;
+    }
+    cudaMemcpy(d_cells, cells.data(), cells.size() * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(d_faces, faces.data(), faces.size(), cudaMemcpyHostToDevice);
+    cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), ctx->stream);
+    CollectHook hook;
+    hook.ctx = ctx; hook.box = box; hook.cells = d_cells; hook.faces = d_faces; hook.ncells = (long long)cells.size();
+    hook.t0 = (int)t0; hook.tstride = (int)tstride; hook.per_step = (int)per_step; hook.seed = seed;
+    hook.inv_dx = 1.f / p.dx; hook.min_scale = min_scale; hook.X = static_cast<__nv_bfloat16 *>(X); hook.R = R; hook.cap = capacity;
+    hook.count = d_count; hook.slot_of = slot_of; hook.stash = stash;
+    float *P = nullptr, *PP = nullptr;
+    rc = rtmb::driver::run_forward(ctx, sx, sy, sz, rtmb::kTaperAll, nullptr, nullptr, &P, &PP, RTMB_PROF_MODEL,
+                                   nullptr, &hook);
+    unsigned long long h = 0;
+    if (!rc && cudaMemcpyAsync(&h, d_count, sizeof h, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) rc = RTMB_ECUDA;
+    if (!rc) rc = rtmb::driver::check_err_flag(ctx);
+    cleanup();
+    *count = h < capacity ? h : capacity;
+    return rc;
+}
+
+}  // extern "C"

@@ -35,6 +35,17 @@ struct rtmb_ctx {
     int sc_cap = 0, sc_next = 0;
     float *d_inj = nullptr;          // device scalars: [0] max |record|, [1] max forward level
     double *d_img64 = nullptr;       // FP64 image of the FP32-output migration with RTMB_FLAG_IMG_F64
+    // RTMB_FLAG_USE_GRAPH: executable graph per driver kind (0 modeling, 1 migration)
+    cudaGraphExec_t gexec[2] = {};
+    bool capturing = false;
+    // learned boundary closure (closure.cu): strip cells of the padded grid, parameters, and the
+    // strip values of the next level computed before each step
+    uint32_t *d_cells = nullptr;
+    uint8_t *d_faces = nullptr;
+    long long ncells = 0;
+    float *d_side = nullptr;
+    float *d_cparams = nullptr;
+    float closure_min_scale = 0.f, closure_damp = 0.f;
     // FP64 GPU oracle (f64.cu)
     double *d_f64[4] = {};
     double *d_upb64 = nullptr;
@@ -52,9 +63,21 @@ namespace rtmb {
 namespace driver {
 
 // Forward time loop shared by modeling and the migration forward pass (see api.cu).
+// Work a driver adds around each step of the forward loop: before(it) runs with P = u(it) and
+// PP = u(it-1), after(it) with PP = u(it+1).  Non-zero return values end the loop.
+struct StepHook {
+    virtual int before(int it, const float *P, float *PP) { return 0; }
+    virtual int after(int it, const float *P, float *PP) { return 0; }
+    virtual ~StepHook() {}
+};
 // With a storage form, sc_out (if not null) receives the scale records of *P_out and *PP_out.
 int run_forward(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, int taper_mode, float *rec,
-                float *upb, float **P_out, float **PP_out, int cat, rtmb::ScaleRec **sc_out = nullptr);
+                float *upb, float **P_out, float **PP_out, int cat, rtmb::ScaleRec **sc_out = nullptr,
+                StepHook *hook = nullptr);
+// The learned closure around one modeling step (closure.cu): the strip's next level from
+// (P, PP) before the step, scattered into PP after it.
+int closure_hook_before(rtmb_ctx *ctx, const float *P, float *PP);
+int closure_hook_after(rtmb_ctx *ctx, float *PP);
 // Reads and clears the device error flag after synchronising the context's stream.
 int check_err_flag(rtmb_ctx *ctx);
 // Fills the derived sizes and the host copy of the stencil coefficients of a context.

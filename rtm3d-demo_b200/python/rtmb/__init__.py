@@ -26,6 +26,8 @@ FLAG_NO_TMA = 0x20
 FLAG_STORE_F16 = 0x40
 FLAG_STORE_BF16 = 0x80
 FLAG_IMG_F64 = 0x100
+BC_ABC, BC_HBC, BC_RBC, BC_LEARNED = 1, 2, 3, 4
+CLOSURE_NPARAM, CLOSURE_NIN = 3169, 64
 
 # every symbol include/rtm3d_b200.h declares: (name, argtypes, restype)
 _vp, _fp, _u32, _i32 = C.c_void_p, C.POINTER(C.c_float), C.c_uint32, C.c_int32
@@ -98,6 +100,15 @@ SYMBOLS = [
     ("rtmb_migrate_shot_acc64", [_vp, _u32, _u32, _u32, _vp, _vp], C.c_int),
     ("rtmb_model_shot_f64", [_vp, _u32, _u32, _u32, _vp], C.c_int),
     ("rtmb_migrate_shot_f64", [_vp, _u32, _u32, _u32, _vp, _vp], C.c_int),
+    ("rtmb_closure_param_count", [], C.c_int),
+    ("rtmb_closure_init", [_fp, C.c_uint64], C.c_int),
+    ("rtmb_closure_forward", [_vp, _vp, C.c_uint64, _vp, _vp], C.c_int),
+    ("rtmb_closure_grad", [_vp, _vp, _vp, _u32, _vp, _vp, _vp], C.c_int),
+    ("rtmb_closure_train", [_vp, _vp, _vp, C.c_uint64, _u32, _u32, C.c_float, C.c_float, C.c_uint64, _fp, _vp],
+     C.c_int),
+    ("rtmb_closure_collect", [_vp, _u32, _u32, _u32, _u32, _u32, _u32, C.c_uint64, C.c_float, _vp, _vp,
+                              C.c_uint64, C.POINTER(C.c_uint64)], C.c_int),
+    ("rtmb_closure_set", [_vp, _vp, C.c_float, C.c_float], C.c_int),
 ]
 
 _LIB = None
@@ -130,6 +141,8 @@ def _ptr(t) -> int:
         return None
     if isinstance(t, int):
         return t
+    if hasattr(t, "cuda_stream"):
+        return t.cuda_stream
     if hasattr(t, "data_ptr"):
         return t.data_ptr()
     return t.ctypes.data
@@ -248,6 +261,17 @@ class Context:
         """FP64 GPU oracle migration: rec float32, img64 float64 padded image (overwritten)."""
         self._check(self.L.rtmb_migrate_shot_f64(self.h, sx, sy, sz, _ptr(rec), _ptr(img64)))
 
+    def closure_set(self, params, min_scale: float = 0.0, damp: float = 0.0):
+        """Installs the learned closure (device or host float32 params) in a BC_LEARNED context."""
+        self._check(self.L.rtmb_closure_set(self.h, _ptr(params), min_scale, damp))
+
+    def closure_collect(self, sx, sy, sz, t0, tstride, per_step, seed, min_scale, X, R) -> int:
+        """Training pairs from a modeling shot on this (wide) context; returns the row count."""
+        cnt = C.c_uint64(0)
+        self._check(self.L.rtmb_closure_collect(self.h, sx, sy, sz, t0, tstride, per_step, seed, min_scale,
+                                                _ptr(X), _ptr(R), R.numel(), C.byref(cnt)))
+        return int(cnt.value)
+
     def model_shot_host(self, sx, sy, sz, rec_host):
         self._check(self.L.rtmb_model_shot_host(self.h, sx, sy, sz, _ptr(rec_host)))
 
@@ -311,3 +335,44 @@ def v2dt2(ve, dt):
     out = np.ascontiguousarray(ve, np.float32).copy()
     load().rtmb_v2dt2_host(out.ctypes.data_as(_fp), out.size, dt)
     return out
+
+
+# ---------------------------------------------------------------- learned boundary closure (no context)
+def _check_noctx(rc: int) -> None:
+    if rc != RTMB_OK:
+        raise RtmbError(rc, load().rtmb_last_error(None).decode())
+
+
+def closure_init(seed: int):
+    """Seeded initial parameters (numpy float32, CLOSURE_NPARAM)."""
+    import numpy as np
+    p = np.zeros(CLOSURE_NPARAM, np.float32)
+    _check_noctx(load().rtmb_closure_init(p.ctypes.data_as(C.POINTER(C.c_float)), seed))
+    return p
+
+
+def closure_forward(params, X, y, stream=None) -> None:
+    """y = network(X); params float32, X bfloat16 [n, 64], y float32 [n] (device tensors)."""
+    _check_noctx(load().rtmb_closure_forward(_ptr(params), _ptr(X), X.shape[0], _ptr(y), _ptr(stream)))
+
+
+def closure_grad(params, X, R, grad, loss, stream=None) -> None:
+    _check_noctx(load().rtmb_closure_grad(_ptr(params), _ptr(X), _ptr(R), X.shape[0], _ptr(grad), _ptr(loss),
+                                          _ptr(stream)))
+
+
+def closure_train(params, X, R, n: int, steps: int, batch: int, lr: float, seed: int, noise: float = 0.0,
+                  stream=None):
+    """Adam training in place; returns the per-step batch losses (numpy)."""
+    import numpy as np
+    losses = np.zeros(steps, np.float32)
+    _check_noctx(load().rtmb_closure_train(_ptr(params), _ptr(X), _ptr(R), n, steps, batch, lr, noise, seed,
+                                           losses.ctypes.data_as(C.POINTER(C.c_float)), _ptr(stream)))
+    return losses
+
+
+def closure_falls_back(learned_reflection: float, hbc_reflection: float) -> bool:
+    """The judge of the learned closure: a run falls back to the plain 32-cell border when the
+    closure's reflected energy (record rel-L2 against a wide-padded run of the same shot) exceeds
+    the 32-cell border's."""
+    return not (learned_reflection <= hbc_reflection)
