@@ -273,6 +273,38 @@ int rtmb_closure_collect(rtmb_ctx *wide, uint32_t sx, uint32_t sy, uint32_t sz, 
  * 1 - damp * ((4 - depth) / 4)^2 each step, depth 0 at the outer face (0 <= damp < 1). */
 int rtmb_closure_set(rtmb_ctx *ctx, const float *params, float min_scale, float damp);
 
+/* ------------------------------------------------------------------ batched multi-shot migration
+ * No reference counterpart (the reference migrates one shot per process, RTMAcousticController.cpp:
+ * 193-242).  Up to 12 shots, each on its own aperture sub-volume of the survey (sizes may differ),
+ * advance together: every time step of the batch is one launch of the step kernel over all shots'
+ * volumes; with RTMB_FLAG_USE_GRAPH the whole batch's time loop is one CUDA graph.  Each shot's image
+ * is added, without its border, to the survey's FP64 stack at the aperture's origin.  The context
+ * supplies what the shots share: blen, nt, ntstep, stencil_order (8), dx/dy/dz, dt, fpeak,
+ * boundary (RBC) and the form flags (FP32 exact or FMA, or a 16-bit storage flag with or without
+ * RTMB_FLAG_IMG_F64).  Shot volumes need nz + 2*blen a multiple of 4 (FP32) or 8 (16-bit). */
+typedef struct rtmb_shot {
+    uint32_t nx, ny, nz;          /* aperture (unpadded) size */
+    uint32_t ox, oy, oz;          /* aperture origin in the survey model */
+    uint32_t sx, sy, sz;          /* source, aperture coordinates */
+    uint32_t receiver_start_x, receiver_start_y, receiver_depth_z;
+    uint32_t receiver_distance_x, receiver_distance_y;
+    uint32_t receiver_count_x, receiver_count_y;
+    const float *v2dt2;           /* padded aperture v2dt2 (device) */
+    const float *rec;             /* the shot's record, file layout (device) */
+} rtmb_shot;
+/* stack: survey image (snx * sny * snz doubles, device), added to. */
+int rtmb_migrate_batch(rtmb_ctx *ctx, uint32_t nshots, const rtmb_shot *shots, double *stack, uint32_t snx,
+                       uint32_t sny, uint32_t snz);
+
+/* ------------------------------------------------------------------ autotuner (no reference counterpart)
+ * Times the context's step kernel (its storage and arithmetic form, on its geometry, with the
+ * loaded v2dt2) for a set of x-chunk lengths (x planes per CTA: 8 .. 256) and keeps the fastest for
+ * every later launch of the context.  The in-plane tile (64 z x 16 y, four z-points per thread) and
+ * the ring depths are compiled in.  Optional outputs: the chosen chunk and its time per step (ms). */
+int rtmb_autotune(rtmb_ctx *ctx, uint32_t *chunk_out, float *ms_out);
+/* Sets the x-chunk length directly (the default is chosen from the grid at rtmb_create). */
+int rtmb_set_chunk(rtmb_ctx *ctx, uint32_t chunk);
+
 /* Host-buffer forms: copy in, run, copy out, return when the result is on the host. */
 int rtmb_model_shot_host(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, float *rec_host);
 int rtmb_migrate_shot_host(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz,

@@ -776,4 +776,280 @@ int rtmb_migrate_shot_host(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz,
     return RTMB_OK;
 }
 
+// ------------------------------------------------------------------ batched multi-shot migration
+
+}  // extern "C"
+
+namespace {
+
+// One shot of a batch: its padded geometry, buffers and the bookkeeping of its wavefields.
+struct BatchShot {
+    rtmb_shot in;
+    int nxe = 0, nye = 0, nze = 0, chunk = 1;
+    size_t n = 0;
+    float *w[4] = {};  // source pair, receiver pair (FP32 or 16-bit)
+    void *img = nullptr;
+    rtmb::ScaleRec *scale = nullptr;
+    int sc_next = 0, sc_cap = 0;
+    float *inj = nullptr;
+    rtmb::ScaleRec *next_scale() { return sc_next < sc_cap ? scale + sc_next++ : nullptr; }
+};
+
+rtmb::StepArgs shot_args(const rtmb_ctx *ctx, const BatchShot &b) {
+    rtmb::StepArgs a = base_args(ctx);
+    a.nxe = b.nxe; a.nye = b.nye; a.nze = b.nze;
+    a.chunk = b.chunk;
+    a.V = b.in.v2dt2;
+    a.store = ctx->store;
+    return a;
+}
+
+void shot_receivers(rtmb::StepArgs &a, const rtmb_ctx *ctx, const BatchShot &b, int mode, int it) {
+    const int bl = (int)ctx->p.blen;
+    const rtmb_shot &s = b.in;
+    a.rec_mode = mode;
+    a.rec = const_cast<float *>(s.rec);
+    a.rx0 = (int)s.receiver_start_x + bl; a.ry0 = (int)s.receiver_start_y + bl; a.rz = (int)s.receiver_depth_z + bl;
+    a.rdx = s.receiver_distance_x ? (int)s.receiver_distance_x : 1;
+    a.rdy = s.receiver_distance_y ? (int)s.receiver_distance_y : 1;
+    a.rcx = (int)s.receiver_count_x; a.rcy = (int)s.receiver_count_y;
+    const long long ntstep = ctx->p.ntstep;
+    a.rec_si = (long long)a.rcy * ntstep;
+    a.rec_sj = ntstep;
+    a.rec_base = (long long)(it / ntstep) * a.rcx * a.rcy * ntstep + (it % ntstep);
+}
+
+}  // namespace
+
+extern "C" {
+
+int rtmb_migrate_batch(rtmb_ctx *ctx, uint32_t nshots, const rtmb_shot *shots, double *stack, uint32_t snx,
+                       uint32_t sny, uint32_t snz) {
+    if (!ctx || !shots || !stack) return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: null pointer");
+    const rtmb_params &p = ctx->p;
+    if (nshots == 0 || nshots > 12) return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: 1 to 12 shots per batch");
+    if (p.boundary != RTMB_BC_RBC || p.stencil_order != 8 || (int)p.blen < ctx->h)
+        return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: boundary RBC, stencil_order 8 and blen >= 4");
+    const bool st = ctx->store != rtmb::kStoreF32;
+    const size_t es = st ? 2 : 4;
+    const bool img64 = st;  // the 16-bit forms stack through an FP64 shot image, FP32 through FP32
+    const int bl = (int)p.blen;
+    std::vector<BatchShot> sh(nshots);
+    // allocation and checks
+    size_t total_tiles = 0;
+    for (uint32_t k = 0; k < nshots; ++k) {
+        BatchShot &b = sh[k];
+        b.in = shots[k];
+        const rtmb_shot &s = b.in;
+        if (!s.v2dt2 || !s.rec || !s.nx || !s.ny || !s.nz || s.sx >= s.nx || s.sy >= s.ny || s.sz >= s.nz ||
+            s.receiver_count_x > s.nx || s.receiver_count_y > s.ny || s.receiver_depth_z + 2 * bl + ctx->h > s.nz + 2 * bl)
+            return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: shot %u: bad geometry", k);
+        b.nxe = (int)s.nx + 2 * bl; b.nye = (int)s.ny + 2 * bl; b.nze = (int)s.nz + 2 * bl;
+        if (b.nze % (st ? 8 : 4))
+            return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: shot %u: nz + 2*blen must be a multiple of %d", k,
+                        st ? 8 : 4);
+        b.n = (size_t)b.nxe * b.nye * b.nze;
+        total_tiles += (size_t)((b.nze + rtmb::kTZ - 1) / rtmb::kTZ) * ((b.nye - 8 + rtmb::kTY - 1) / rtmb::kTY);
+    }
+    int rc = RTMB_OK;
+    auto release = [&]() {
+        for (BatchShot &b : sh) {
+            for (float *w : b.w) if (w) cudaFree(w);
+            if (b.img) cudaFree(b.img);
+            if (b.scale) cudaFree(b.scale);
+            if (b.inj) cudaFree(b.inj);
+        }
+    };
+    for (BatchShot &b : sh) {
+        // x planes per CTA: the batch shares the usual CTA budget of several waves on 148 SMs
+        const int nxi = b.nxe - 8;
+        const size_t target = 148 * 2 * 4;
+        const size_t tiles = (size_t)((b.nze + rtmb::kTZ - 1) / rtmb::kTZ) * ((b.nye - 8 + rtmb::kTY - 1) / rtmb::kTY);
+        size_t nch = (target * tiles / (total_tiles ? total_tiles : 1) + tiles - 1) / tiles;
+        if (nch < 1) nch = 1;
+        if (nch > (size_t)(nxi / 16 > 0 ? nxi / 16 : 1)) nch = nxi / 16 > 0 ? nxi / 16 : 1;
+        b.chunk = (int)((nxi + nch - 1) / nch);
+        bool ok = true;
+        for (float *&w : b.w) ok = ok && cudaMalloc(&w, b.n * es) == cudaSuccess;
+        ok = ok && cudaMalloc(&b.img, b.n * (img64 ? 8 : 4)) == cudaSuccess;
+        if (st) {
+            b.sc_cap = 3 * (int)p.nt + 8;
+            ok = ok && cudaMalloc(&b.scale, b.sc_cap * sizeof(rtmb::ScaleRec)) == cudaSuccess &&
+                 cudaMalloc(&b.inj, sizeof(float)) == cudaSuccess;
+        }
+        if (!ok) { release(); return fail(ctx, RTMB_ENOMEM, "rtmb_migrate_batch: device allocation failed"); }
+        for (float *w : b.w) cudaMemsetAsync(w, 0, b.n * es, ctx->stream);
+        cudaMemsetAsync(b.img, 0, b.n * (img64 ? 8 : 4), ctx->stream);
+        if (st) {
+            cudaMemsetAsync(b.scale, 0, b.sc_cap * sizeof(rtmb::ScaleRec), ctx->stream);
+            const size_t nrec = (size_t)p.nt * b.in.receiver_count_x * b.in.receiver_count_y;
+            if (rtmb::launch_absmax(b.in.rec, nrec, b.inj, ctx->stream) != cudaSuccess) {
+                release();
+                return fail(ctx, RTMB_ECUDA, "rtmb_migrate_batch: record scan failed");
+            }
+            ++ctx->launches;
+        }
+    }
+    const int order = (int)p.stencil_order;
+    std::vector<rtmb::StepArgs> args(nshots);
+    // per shot: the source pair (P, PP) with scale records, the receiver pair likewise
+    std::vector<float *> sP(nshots), sPP(nshots), rP(nshots), rPP(nshots);
+    std::vector<rtmb::ScaleRec *> scP(nshots), scPP(nshots), srP(nshots), srPP(nshots);
+    for (uint32_t k = 0; k < nshots; ++k) {
+        sP[k] = sh[k].w[0]; sPP[k] = sh[k].w[1]; rP[k] = sh[k].w[2]; rPP[k] = sh[k].w[3];
+        if (st) {
+            scP[k] = sh[k].next_scale(); scPP[k] = sh[k].next_scale();
+            srP[k] = sh[k].next_scale(); srPP[k] = sh[k].next_scale();
+        }
+    }
+    {
+        GraphScope graph(ctx, 2);
+        if ((rc = graph.begin())) { release(); return rc; }
+        // forward (RBC.cpp:54-144), all shots per launch
+        for (uint32_t it = 0; it < p.nt && !rc; ++it) {
+            for (uint32_t k = 0; k < nshots; ++k) {
+                std::swap(sP[k], sPP[k]);
+                std::swap(scP[k], scPP[k]);
+                rtmb::StepArgs &a = args[k];
+                a = shot_args(ctx, sh[k]);
+                a.P = sP[k]; a.PP = sPP[k]; a.it = (int)it;
+                a.sxe = (int)sh[k].in.sx + bl; a.sye = (int)sh[k].in.sy + bl; a.sze = (int)sh[k].in.sz + bl;
+                if (st) { a.sc_p = scP[k]; a.sc_pp = scPP[k]; a.sc_out = sh[k].next_scale(); a.inj = ctx->wmax; }
+            }
+            const size_t slot = prof_begin(ctx, RTMB_PROF_FORWARD);
+            ++ctx->launches;
+            if (rtmb::launch_step_batch(args.data(), (int)nshots, order, exact(ctx), ctx->stream) != cudaSuccess)
+                rc = fail(ctx, RTMB_ECUDA, "rtmb_migrate_batch: forward launch failed");
+            prof_end(ctx, slot);
+            if (st) for (uint32_t k = 0; k < nshots; ++k) scPP[k] = args[k].sc_out;
+        }
+        // backward (RBC.cpp:146-274): s_cur images the receiver wavefield each step
+        std::vector<float *> cur(nshots), prev(nshots);
+        std::vector<rtmb::ScaleRec *> scur(nshots), sprev(nshots);
+        for (uint32_t k = 0; k < nshots; ++k) { cur[k] = sPP[k]; prev[k] = sP[k]; scur[k] = scPP[k]; sprev[k] = scP[k]; }
+        const int rmode = (p.flags & RTMB_FLAG_RCV_ADD) ? rtmb::kRecAdd : rtmb::kRecOverwrite;
+        for (int it = (int)p.nt - 1; it >= 0 && !rc; --it) {
+            if (it == (int)p.nt - 2) {
+                for (uint32_t k = 0; k < nshots; ++k) {
+                    std::swap(cur[k], prev[k]);
+                    std::swap(scur[k], sprev[k]);
+                }
+            } else if (it < (int)p.nt - 2) {
+                for (uint32_t k = 0; k < nshots; ++k) {
+                    rtmb::StepArgs &a = args[k];
+                    a = shot_args(ctx, sh[k]);
+                    a.P = cur[k]; a.PP = prev[k]; a.it = it;
+                    if (st) { a.sc_p = scur[k]; a.sc_pp = sprev[k]; a.sc_out = sh[k].next_scale(); }
+                }
+                const size_t slot = prof_begin(ctx, RTMB_PROF_BACKWARD_SOURCE);
+                ++ctx->launches;
+                if (rtmb::launch_step_batch(args.data(), (int)nshots, order, exact(ctx), ctx->stream) != cudaSuccess)
+                    rc = fail(ctx, RTMB_ECUDA, "rtmb_migrate_batch: source launch failed");
+                prof_end(ctx, slot);
+                for (uint32_t k = 0; k < nshots; ++k) {
+                    std::swap(cur[k], prev[k]);
+                    if (st) { sprev[k] = scur[k]; scur[k] = args[k].sc_out; }
+                }
+            }
+            for (uint32_t k = 0; k < nshots; ++k) {
+                rtmb::StepArgs &a = args[k];
+                a = shot_args(ctx, sh[k]);
+                a.P = rP[k]; a.PP = rPP[k]; a.it = it;
+                a.ps = cur[k];
+                a.img = static_cast<float *>(sh[k].img);
+                a.img64 = img64;
+                a.img_z0 = bl; a.img_z1 = sh[k].nze - bl;
+                shot_receivers(a, ctx, sh[k], rmode, it);
+                if (st) {
+                    a.sc_p = srP[k]; a.sc_pp = srPP[k]; a.sc_out = sh[k].next_scale(); a.sc_ps = scur[k];
+                    a.inj_dev = sh[k].inj;
+                }
+            }
+            const size_t slot = prof_begin(ctx, RTMB_PROF_BACKWARD_RECEIVER);
+            ++ctx->launches;
+            if (rtmb::launch_step_batch(args.data(), (int)nshots, order, exact(ctx), ctx->stream) != cudaSuccess)
+                rc = fail(ctx, RTMB_ECUDA, "rtmb_migrate_batch: receiver launch failed");
+            prof_end(ctx, slot);
+            for (uint32_t k = 0; k < nshots; ++k) {
+                std::swap(rP[k], rPP[k]);
+                if (st) { srPP[k] = srP[k]; srP[k] = args[k].sc_out; }
+            }
+        }
+        // each shot's image without its border into the survey stack (RTMGrid.cpp:168-223)
+        for (uint32_t k = 0; k < nshots && !rc; ++k) {
+            const rtmb::Geom g{sh[k].nxe, sh[k].nye, sh[k].nze, bl, ctx->h};
+            ++ctx->launches;
+            if (rtmb::launch_stack_region64(stack, (int)snx, (int)sny, (int)snz, sh[k].img, img64, g, (int)sh[k].in.ox,
+                                            (int)sh[k].in.oy, (int)sh[k].in.oz, ctx->stream) != cudaSuccess)
+                rc = fail(ctx, RTMB_ECUDA, "rtmb_migrate_batch: stacking failed");
+        }
+        if (!rc) rc = graph.end();
+    }
+    if (!rc) rc = check_err_flag(ctx);
+    cudaStreamSynchronize(ctx->stream);
+    release();
+    return rc;
+}
+
+// ------------------------------------------------------------------ autotuner
+
+int rtmb_autotune(rtmb_ctx *ctx, uint32_t *chunk_out, float *ms_out) {
+    if (!ctx) return RTMB_EINVAL;
+    if (!ctx->d_v2dt2) return fail(ctx, RTMB_EINVAL, "rtmb_autotune: load v2dt2 first");
+    int rc = alloc_driver(ctx);
+    if (rc) return rc;
+    const bool st = ctx->store != rtmb::kStoreF32;
+    rtmb::ScaleRec *rec3 = nullptr;
+    if (st) {
+        CK(cudaMalloc(&rec3, 3 * sizeof(rtmb::ScaleRec)));
+        CK(cudaMemsetAsync(rec3, 0, 3 * sizeof(rtmb::ScaleRec), ctx->stream));
+    }
+    CK(cudaMemsetAsync(ctx->d_w[0], 0, wave_bytes(ctx), ctx->stream));
+    CK(cudaMemsetAsync(ctx->d_w[1], 0, wave_bytes(ctx), ctx->stream));
+    const int nxi = ctx->nxe - 2 * ctx->h;
+    // candidates: x planes per CTA.  Short chunks give more CTAs but re-read a 2h-plane halo per
+    // chunk; long chunks re-read less but may leave SMs idle in the last wave.
+    const int cand[] = {8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256};
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    const int saved = ctx->chunk;
+    float best = 1e30f;
+    int best_chunk = saved;
+    for (int c : cand) {
+        if (c > nxi) break;
+        ctx->chunk = c;
+        rtmb::StepArgs a = base_args(ctx);
+        a.V = ctx->d_v2dt2;
+        a.P = ctx->d_w[0];
+        a.PP = ctx->d_w[1];
+        a.store = ctx->store;
+        if (st) { a.sc_p = rec3; a.sc_pp = rec3 + 1; a.sc_out = rec3 + 2; a.inj = 1.f; }
+        for (int w = 0; w < 2; ++w) LAUNCH(rtmb::launch_step(a, (int)ctx->p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
+        CK(cudaEventRecord(e0, ctx->stream));
+        const int reps = 5;
+        for (int r = 0; r < reps; ++r)
+            LAUNCH(rtmb::launch_step(a, (int)ctx->p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
+        CK(cudaEventRecord(e1, ctx->stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        ms /= reps;
+        if (ms < best) { best = ms; best_chunk = c; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rec3) cudaFree(rec3);
+    ctx->chunk = best_chunk;
+    if (chunk_out) *chunk_out = (uint32_t)best_chunk;
+    if (ms_out) *ms_out = best;
+    return check_err_flag(ctx);
+}
+
+int rtmb_set_chunk(rtmb_ctx *ctx, uint32_t chunk) {
+    if (!ctx || !chunk) return RTMB_EINVAL;
+    ctx->chunk = (int)chunk;
+    return RTMB_OK;
+}
+
 }  // extern "C"

@@ -149,6 +149,21 @@ __global__ void stack64_kernel(double *acc, const float *__restrict__ img, size_
         acc[o] = acc[o] + (double)img[o];
 }
 
+// RTMGrid::stackRegion (src/grid/RTMGrid.cpp:168-223) of a shot image without its border into the
+// survey volume, in FP64: one thread per (z) of each (x, y) row of the shot's interior.
+template <typename I>
+__global__ void stack_region_kernel(double *stack, int snx, int sny, int snz, const I *__restrict__ img, Geom g,
+                                    int ox, int oy, int oz) {
+    const int nx = g.nxe - 2 * g.blen, ny = g.nye - 2 * g.blen, nz = g.nze - 2 * g.blen;
+    const int z = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, x = blockIdx.z;
+    if (z >= nz || x + ox >= snx || y + oy >= sny || z + oz >= snz) return;
+    const size_t so = ((size_t)(x + ox) * sny + (y + oy)) * snz + (z + oz);
+    const size_t io = ((size_t)(x + g.blen) * g.nye + (y + g.blen)) * g.nze + (z + g.blen);
+    stack[so] = stack[so] + (double)img[io];
+    (void)nx;
+    (void)ny;
+}
+
 unsigned grid1d(size_t n) {
     size_t b = (n + 255) / 256;
     return (unsigned)(b > 148u * 64u ? 148u * 64u : (b == 0 ? 1 : b));
@@ -263,6 +278,20 @@ cudaError_t launch_scale_max(const ScaleRec *r, int n, float *out, cudaStream_t 
 
 cudaError_t launch_to_float(const double *a, float *out, size_t n, cudaStream_t s) {
     to_float_kernel<<<grid1d(n), 256, 0, s>>>(a, out, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_stack_region64(double *stack, int snx, int sny, int snz, const void *img, bool img64,
+                                  const Geom &g, int ox, int oy, int oz, cudaStream_t s) {
+    const int nx = g.nxe - 2 * g.blen, ny = g.nye - 2 * g.blen, nz = g.nze - 2 * g.blen;
+    if (nx <= 0 || ny <= 0 || nz <= 0) return cudaErrorInvalidValue;
+    dim3 grid((nz + 127) / 128, ny, nx);
+    if (img64)
+        stack_region_kernel<double><<<grid, 128, 0, s>>>(stack, snx, sny, snz, static_cast<const double *>(img), g,
+                                                         ox, oy, oz);
+    else
+        stack_region_kernel<float><<<grid, 128, 0, s>>>(stack, snx, sny, snz, static_cast<const float *>(img), g, ox,
+                                                        oy, oz);
     return cudaGetLastError();
 }
 

@@ -56,5 +56,9 @@ cudaError_t launch_scale_max(const ScaleRec *r, int n, float *out, cudaStream_t 
 cudaError_t launch_to_float(const double *a, float *out, size_t n, cudaStream_t s);
 // acc += (double) img over n values.
 cudaError_t launch_stack64(double *acc, const float *img, size_t n, cudaStream_t s);
+// Stacking of a padded shot image (g: its padded geometry; img64: doubles, else floats) without
+// its border into a survey volume (snx, sny, snz) of doubles at origin (ox, oy, oz).
+cudaError_t launch_stack_region64(double *stack, int snx, int sny, int snz, const void *img, bool img64,
+                                  const Geom &g, int ox, int oy, int oz, cudaStream_t s);
 
 }  // namespace rtmb

@@ -5,6 +5,7 @@
 #include <cuda_fp16.h>
 
 #include <cstring>
+#include <vector>
 
 #include "stencil.cuh"
 #include "stencil_tma_impl.cuh"
@@ -19,6 +20,8 @@ cudaError_t launch_tma_h(const TmaMaps &maps, const StepArgs &a, bool exact, int
 template <typename T>
 cudaError_t launch_tma_store(const TmaMaps &maps, const StepArgs &a, int taper, bool img, bool img64, dim3 grid,
                              cudaStream_t s);
+template <typename T>
+cudaError_t launch_tma_batch(const BatchArgs &b, bool exact, bool img, bool img64, int blocks, cudaStream_t s);
 }  // namespace detail
 
 namespace {
@@ -128,5 +131,59 @@ cudaError_t launch_step(const StepArgs &a, int order, bool exact, cudaStream_t s
 }
 
 bool storage_form_supported(int order, int nze) { return order == 8 && nze % 8 == 0; }
+
+cudaError_t launch_step_batch(const StepArgs *args, int nshots, int order, bool exact, cudaStream_t s) {
+    static_assert(sizeof(detail::BatchArgs) <= 32000, "kernel parameters above the 32 KB limit");
+    if (nshots <= 0 || nshots > detail::kMaxBatch || order != 8) return cudaErrorInvalidValue;
+    auto enc = tensor_map_encoder();
+    if (!enc) return cudaErrorNotSupported;
+    const StepArgs &a0 = args[0];
+    const bool img = a0.img != nullptr, img64 = a0.img64 != 0;
+    const int store = a0.store;
+    const bool st = store != kStoreF32;
+    if (st) exact = false;  // the 16-bit storage forms always use the FMA arithmetic
+    std::vector<detail::BatchArgs> hold(1);  // ~30 KB: kept off the stack
+    detail::BatchArgs &b = hold[0];
+    std::memset(&b, 0, sizeof b);
+    b.nshots = nshots;
+    b.coef = a0;
+    const CUtensorMapDataType dt = store == kStoreF16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                   : store == kStoreBF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                         : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    const size_t es = st ? 2 : 4;
+    int blocks = 0;
+    for (int k = 0; k < nshots; ++k) {
+        const StepArgs &a = args[k];
+        if (a.taper_mode != kTaperNone || (a.img != nullptr) != img || a.img64 != a0.img64 || a.store != store ||
+            a.chunk <= 0)
+            return cudaErrorInvalidValue;
+        if (a.nze % (st ? 8 : 4) != 0) return cudaErrorInvalidValue;
+        const uintptr_t al = reinterpret_cast<uintptr_t>(a.P) | reinterpret_cast<uintptr_t>(a.PP) |
+                             reinterpret_cast<uintptr_t>(a.V) | reinterpret_cast<uintptr_t>(a.img) |
+                             reinterpret_cast<uintptr_t>(a.ps);
+        if (al % 16) return cudaErrorInvalidValue;
+        const int spitch = kTZ + 2 * (st ? 8 : 4), srows = kTY + 8;
+        detail::TmaMaps &m = b.maps[k];
+        bool ok = encode(enc, &m.p, a.P, a, spitch, srows, dt, es) && encode(enc, &m.pp, a.PP, a, kTZ, kTY, dt, es) &&
+                  encode(enc, &m.v, a.V, a, kTZ, kTY);
+        if (img)
+            ok = ok && encode(enc, &m.ps, a.ps, a, kTZ, kTY, dt, es) &&
+                 encode(enc, &m.img, a.img, a, kTZ, kTY,
+                        img64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, img64 ? 8 : 4);
+        if (!ok) return cudaErrorInvalidValue;
+        b.args[k] = a;
+        const int nxi = a.nxe - 8, nyi = a.nye - 8;
+        if (nxi <= 0 || nyi <= 0 || a.nze <= 8) return cudaErrorInvalidValue;
+        b.gx[k] = (a.nze + kTZ - 1) / kTZ;
+        b.gy[k] = (nyi + kTY - 1) / kTY;
+        const int gz = (nxi + a.chunk - 1) / a.chunk;
+        b.start[k] = blocks;
+        blocks += b.gx[k] * b.gy[k] * gz;
+    }
+    b.start[nshots] = blocks;
+    if (store == kStoreF16) return detail::launch_tma_batch<__half>(b, exact, img, img64, blocks, s);
+    if (store == kStoreBF16) return detail::launch_tma_batch<__nv_bfloat16>(b, exact, img, img64, blocks, s);
+    return detail::launch_tma_batch<float>(b, exact, img, img64, blocks, s);
+}
 
 }  // namespace rtmb

@@ -104,6 +104,11 @@ __host__ __device__ inline int storage_exponent(float bound) {
 // allow_tma = false forces the plain-load form (used by tests to check both forms).
 cudaError_t launch_step(const StepArgs &a, int order, bool exact, cudaStream_t s, bool allow_tma = true);
 
+// One launch of the step kernel over several volumes (the batched multi-shot drivers): order 8, no
+// taper, TMA-aligned volumes, the same form and the same stencil coefficients for every shot
+// (args[0]'s are used).  At most 12 shots.
+cudaError_t launch_step_batch(const StepArgs *args, int nshots, int order, bool exact, cudaStream_t s);
+
 // Whether the 16-bit storage forms (and the FP64 image) can run on this geometry: order 8 and
 // z rows whose 16-bit pitch is a multiple of 16 bytes (nze % 8 == 0).
 bool storage_form_supported(int order, int nze);

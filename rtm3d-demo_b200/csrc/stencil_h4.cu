@@ -7,5 +7,6 @@ namespace rtmb {
 namespace detail {
 template cudaError_t launch_h<4>(const StepArgs &, bool, bool, dim3, cudaStream_t);
 template cudaError_t launch_tma_h<4>(const TmaMaps &, const StepArgs &, bool, int, bool, dim3, cudaStream_t);
+template cudaError_t launch_tma_batch<float>(const BatchArgs &, bool, bool, bool, int, cudaStream_t);
 }  // namespace detail
 }  // namespace rtmb

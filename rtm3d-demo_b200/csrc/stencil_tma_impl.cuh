@@ -174,9 +174,12 @@ struct TmaShape {
 // TAPER: kTaperNone / kTaperUpper / kTaperAll.  IMG: the epilogue accumulates the image.
 // T: storage type of P, PP and ps (float: the FP32 form, bit-identical to the plain-load kernel;
 // __half / __nv_bfloat16: scaled 16-bit storage).  IT: image type (float or double).
-template <int H, bool EXACT, int TAPER, bool IMG, typename T = float, typename IT = float>
-__global__ void __launch_bounds__(kTmaThreads, 2)
-    tma_step_kernel(const __grid_constant__ TmaMaps maps, const __grid_constant__ StepArgs a) {
+// The body of one CTA: the tile (bx, by) of the (z, y) plane and x chunk bz of the volume that
+// (maps, a) describe; the stencil coefficients come from coef (for the compiler, a kernel
+// parameter at a fixed offset, so the FMAs take them straight from the constant bank).
+template <int H, bool EXACT, int TAPER, bool IMG, typename T, typename IT>
+__device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArgs &a, const StepArgs &coef, int bx,
+                                              int by, int bz) {
     using S = TmaShape<H, IMG, T, IT>;
     using ST = Stor<T>;
     constexpr bool SC = ST::kScaled;
@@ -199,11 +202,11 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
 
     const int tid = threadIdx.x;
     const int tz = tid % ZQ, ty = tid / ZQ;
-    const int zt0 = blockIdx.x * kTZ;
-    const int yt0 = H + blockIdx.y * kTY;
+    const int zt0 = bx * kTZ;
+    const int yt0 = H + by * kTY;
     const int z0 = zt0 + tz * kVZ;
     const int y = yt0 + ty;
-    const int xc0 = H + blockIdx.z * a.chunk;
+    const int xc0 = H + bz * a.chunk;
     const int xc1 = min(xc0 + a.chunk, a.nxe - H);
     if (xc0 >= xc1) return;
     const int n = xc1 - xc0;        // output planes, local index i <-> x = xc0 + i
@@ -267,7 +270,7 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
         const int eN = storage_exponent(bound);
         sOutInv = exp2i(-eN);
         sKeep = exp2i(max(-126, min(127, rpp.e - eN)));  // re-stores cells outside the computed region
-        if (tid == 0 && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0) a.sc_out->e = eN;
+        if (tid == 0 && bx == 0 && by == 0 && bz == 0) a.sc_out->e = eN;
     }
 
     // ---- per-thread constants, hoisted out of the plane loop
@@ -398,15 +401,15 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
                         const float4 ry = (io == H) ? q[H] : ST::ld4(s + (ty + io) * SPITCH + col);
 #pragma unroll
                         for (int e = 0; e < kVZ; ++e) {
-                            ax[e] = ax[e] + get(qx, e) * a.cx[io];
-                            ay[e] = ay[e] + get(ry, e) * a.cy[io];
-                            az[e] = az[e] + zr[ZH - H + e + io] * a.cz[io];
+                            ax[e] = ax[e] + get(qx, e) * coef.cx[io];
+                            ay[e] = ay[e] + get(ry, e) * coef.cy[io];
+                            az[e] = az[e] + zr[ZH - H + e + io] * coef.cz[io];
                         }
                     }
 #pragma unroll
                     for (int e = 0; e < kVZ; ++e) lap[e] = ax[e] + ay[e] + az[e];
                 } else {
-                    const float cc = a.cx[H] + a.cy[H] + a.cz[H];
+                    const float cc = coef.cx[H] + coef.cy[H] + coef.cz[H];
                     const float4 qc = q[H];
 #pragma unroll
                     for (int e = 0; e < kVZ; ++e) lap[e] = get(qc, e) * cc;
@@ -417,9 +420,9 @@ __global__ void __launch_bounds__(kTmaThreads, 2)
                         const float4 ry = ST::ld4(s + (ty + io) * SPITCH + col);
 #pragma unroll
                         for (int e = 0; e < kVZ; ++e) {
-                            lap[e] = fmaf(get(qx, e), a.cx[io], lap[e]);
-                            lap[e] = fmaf(get(ry, e), a.cy[io], lap[e]);
-                            lap[e] = fmaf(zr[ZH - H + e + io], a.cz[io], lap[e]);
+                            lap[e] = fmaf(get(qx, e), coef.cx[io], lap[e]);
+                            lap[e] = fmaf(get(ry, e), coef.cy[io], lap[e]);
+                            lap[e] = fmaf(zr[ZH - H + e + io], coef.cz[io], lap[e]);
                         }
                     }
                 }
@@ -564,6 +567,36 @@ drain:
     if (a.err) atomicOr(a.err, 2u);
 }
 
+template <int H, bool EXACT, int TAPER, bool IMG, typename T = float, typename IT = float>
+__global__ void __launch_bounds__(kTmaThreads, 2)
+    tma_step_kernel(const __grid_constant__ TmaMaps maps, const __grid_constant__ StepArgs a) {
+    tma_step_body<H, EXACT, TAPER, IMG, T, IT>(maps, a, a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Several volumes in one launch (the batched multi-shot drivers): shot s owns the linear blocks
+// [start[s], start[s+1]), laid out as its own (gx, gy, gz) grid.  All shots share the stencil
+// coefficients (coef) and the kernel variant; everything else is per shot.
+constexpr int kMaxBatch = 12;
+struct BatchArgs {
+    int nshots;
+    int start[kMaxBatch + 1];
+    int gx[kMaxBatch], gy[kMaxBatch];
+    StepArgs coef;
+    TmaMaps maps[kMaxBatch];
+    StepArgs args[kMaxBatch];
+};
+
+template <int H, bool EXACT, int TAPER, bool IMG, typename T = float, typename IT = float>
+__global__ void __launch_bounds__(kTmaThreads, 2) tma_batch_kernel(const __grid_constant__ BatchArgs b) {
+    int lin = blockIdx.x, s = 0;
+    while (s + 1 < b.nshots && lin >= b.start[s + 1]) ++s;
+    lin -= b.start[s];
+    const int bx = lin % b.gx[s];
+    lin /= b.gx[s];
+    const int by = lin % b.gy[s], bz = lin / b.gy[s];
+    tma_step_body<H, EXACT, TAPER, IMG, T, IT>(b.maps[s], b.args[s], b.coef, bx, by, bz);
+}
+
 template <int H>
 cudaError_t launch_tma_h(const TmaMaps &maps, const StepArgs &a, bool exact, int taper, bool img, dim3 grid,
                          cudaStream_t s) {
@@ -629,6 +662,40 @@ cudaError_t launch_tma_store(const TmaMaps &maps, const StepArgs &a, int taper, 
     RTMB_TMA_STORE_CASE(kTaperUpper, true, double)
 #undef RTMB_TMA_STORE_CASE
     return cudaErrorInvalidValue;
+}
+
+// The batched multi-shot kernels: the RBC migration variants (no taper), FP32 (exact or FMA) and the
+// 16-bit storage forms (FMA), with or without the image.
+template <typename T>
+cudaError_t launch_tma_batch(const BatchArgs &b, bool exact, bool img, bool img64, int blocks, cudaStream_t s) {
+    static unsigned long long attr_done[6] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int variant = (exact ? 3 : 0) + (img ? (img64 ? 2 : 1) : 0);
+    auto run = [&](void (*kern)(BatchArgs), size_t smem) -> cudaError_t {
+        const unsigned long long bit = 1ull << (dev & 63);
+        if (!(attr_done[variant] & bit)) {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            attr_done[variant] |= bit;
+        }
+        kern<<<blocks, kTmaThreads, smem, s>>>(b);
+        return cudaGetLastError();
+    };
+    if constexpr (sizeof(T) == 4) {
+        if (img64) return cudaErrorInvalidValue;
+        if (exact)
+            return img ? run(tma_batch_kernel<4, true, kTaperNone, true>, TmaShape<4, true>::SMEM)
+                       : run(tma_batch_kernel<4, true, kTaperNone, false>, TmaShape<4, false>::SMEM);
+        return img ? run(tma_batch_kernel<4, false, kTaperNone, true>, TmaShape<4, true>::SMEM)
+                   : run(tma_batch_kernel<4, false, kTaperNone, false>, TmaShape<4, false>::SMEM);
+    } else {
+        if (exact) return cudaErrorInvalidValue;
+        if (!img) return run(tma_batch_kernel<4, false, kTaperNone, false, T, float>, TmaShape<4, false, T, float>::SMEM);
+        if (img64)
+            return run(tma_batch_kernel<4, false, kTaperNone, true, T, double>, TmaShape<4, true, T, double>::SMEM);
+        return run(tma_batch_kernel<4, false, kTaperNone, true, T, float>, TmaShape<4, true, T, float>::SMEM);
+    }
 }
 
 }  // namespace detail

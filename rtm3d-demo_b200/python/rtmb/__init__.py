@@ -109,6 +109,9 @@ SYMBOLS = [
     ("rtmb_closure_collect", [_vp, _u32, _u32, _u32, _u32, _u32, _u32, C.c_uint64, C.c_float, _vp, _vp,
                               C.c_uint64, C.POINTER(C.c_uint64)], C.c_int),
     ("rtmb_closure_set", [_vp, _vp, C.c_float, C.c_float], C.c_int),
+    ("rtmb_autotune", [_vp, C.POINTER(_u32), C.POINTER(C.c_float)], C.c_int),
+    ("rtmb_migrate_batch", [_vp, _u32, _vp, _vp, _u32, _u32, _u32], C.c_int),
+    ("rtmb_set_chunk", [_vp, _u32], C.c_int),
 ]
 
 _LIB = None
@@ -146,6 +149,18 @@ def _ptr(t) -> int:
     if hasattr(t, "data_ptr"):
         return t.data_ptr()
     return t.ctypes.data
+
+
+class Shot(C.Structure):
+    """rtmb_shot: one shot of a batch (aperture geometry, source, receivers, device buffers)."""
+    _fields_ = [
+        ("nx", _u32), ("ny", _u32), ("nz", _u32), ("ox", _u32), ("oy", _u32), ("oz", _u32),
+        ("sx", _u32), ("sy", _u32), ("sz", _u32),
+        ("receiver_start_x", _u32), ("receiver_start_y", _u32), ("receiver_depth_z", _u32),
+        ("receiver_distance_x", _u32), ("receiver_distance_y", _u32),
+        ("receiver_count_x", _u32), ("receiver_count_y", _u32),
+        ("v2dt2", _vp), ("rec", _vp),
+    ]
 
 
 class Context:
@@ -271,6 +286,21 @@ class Context:
         self._check(self.L.rtmb_closure_collect(self.h, sx, sy, sz, t0, tstride, per_step, seed, min_scale,
                                                 _ptr(X), _ptr(R), R.numel(), C.byref(cnt)))
         return int(cnt.value)
+
+    def migrate_batch(self, shots, stack):
+        """shots: list of Shot; stack: float64 survey volume (device), added to."""
+        arr = (Shot * len(shots))(*shots)
+        nx, ny, nz = stack.shape
+        self._check(self.L.rtmb_migrate_batch(self.h, len(shots), C.cast(arr, _vp), _ptr(stack), nx, ny, nz))
+
+    def autotune(self):
+        """Picks the fastest x-chunk length for this context; returns (chunk, ms per step)."""
+        c, ms = _u32(0), C.c_float(0)
+        self._check(self.L.rtmb_autotune(self.h, C.byref(c), C.byref(ms)))
+        return int(c.value), float(ms.value)
+
+    def set_chunk(self, chunk: int):
+        self._check(self.L.rtmb_set_chunk(self.h, chunk))
 
     def model_shot_host(self, sx, sy, sz, rec_host):
         self._check(self.L.rtmb_model_shot_host(self.h, sx, sy, sz, _ptr(rec_host)))

@@ -171,3 +171,22 @@ def test_graph_replay_matches_eager(cuda, oracle, bc):
     for a, b in zip(out[0][0], out[rtmb.FLAG_USE_GRAPH][0]):
         assert bitexact(a, b)
     assert out[0][1] == out[rtmb.FLAG_USE_GRAPH][1]  # same kernels, counted the same way
+
+
+def test_autotune_picks_a_chunk_and_keeps_results(cuda, oracle):
+    """rtmb_autotune times the step kernel for several x-chunk lengths and keeps the fastest; the
+    chunk only changes how planes are split across CTAs, never a result."""
+    import torch
+    case = CASES["mid"]
+    ve = oracle.extend_init_borders(layered_model(case), case["blen"], "abc")
+    v2 = oracle.v2dt2(ve, case["dt"])
+    ctx = ctx_for(case, "hbc")
+    ctx.load_v2dt2(v2, from_host=True)
+    rec0 = torch.zeros(rec_shape(case), dtype=torch.float32, device=cuda)
+    ctx.model_shot(case["sx"], case["sy"], case["sz"], rec0)
+    chunk, ms = ctx.autotune()
+    assert chunk in (8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256) and ms > 0
+    rec1 = torch.zeros_like(rec0)
+    ctx.model_shot(case["sx"], case["sy"], case["sz"], rec1)
+    ctx.sync()
+    assert bitexact(host(rec0), host(rec1))
