@@ -17,6 +17,12 @@ host-buffer C-ABI call (record copied in, padded image copied out, inside the ti
 
 --impl reference times the reference's own CPU program (oracle/_ref/RTM3D.bin, built from its
 sources) on a truncated-nt sample of the same workload on this host's cores.
+
+The line's "forms" object compares, on the same grid and shot with nt cut to --forms-nt steps, the
+plain FP32 form (bit-exact with the reference CPU path), the FMA form and the 16-bit storage forms:
+device time per sweep, the seconds per shot that gives at the full nt, and the image rel-L2 against
+the FP64 GPU oracle run on the same grid and record.  "chosen" is the fastest form whose image
+stays within rel-L2 1e-3 of the FP64 oracle.
 """
 from __future__ import annotations
 
@@ -222,13 +228,68 @@ def build_inputs(p: dict, with_abc: bool):
     return v, vpe, v2, v2m
 
 
+FORMS = ("fp32_exact", "fp32_fma", "fp16", "bf16", "fp16_img64", "bf16_img64")
+
+
+def form_flags(rtmb, form: str) -> int:
+    return {"fp32_exact": 0, "fp32_fma": rtmb.FLAG_FAST_FMA, "fp16": rtmb.FLAG_STORE_F16,
+            "bf16": rtmb.FLAG_STORE_BF16, "fp16_img64": rtmb.FLAG_STORE_F16 | rtmb.FLAG_IMG_F64,
+            "bf16_img64": rtmb.FLAG_STORE_BF16 | rtmb.FLAG_IMG_F64}[form]
+
+
+def compare_forms(p: dict, v2: np.ndarray, rec_full, dev, nt_cmp: int) -> dict:
+    """Per-form timing and image error against the FP64 GPU oracle on the first nt_cmp steps."""
+    import torch
+    import rtmb
+    q = dict(p, nt=nt_cmp, ntstep=nt_cmp)
+    rec = rec_full[..., :nt_cmp].contiguous()
+    sx, sy, sz = q["sx"], q["sy"], q["sz"]
+    ctx = rtmb.Context(rtmb.Params.from_input(q, device=dev.index or 0))
+    ctx.load_v2dt2(v2, from_host=True)
+    shape = ctx.padded_shape
+    ref = torch.zeros(shape, dtype=torch.float64, device=dev)
+    t0 = time.time()
+    ctx.migrate_shot_f64(sx, sy, sz, rec, ref)
+    ctx.sync()
+    f64_s = time.time() - t0
+    ctx.close()
+    ref_norm = float(torch.linalg.vector_norm(ref))
+    forms = {f: form_flags(rtmb, f) for f in FORMS}
+    sweeps_cmp = 3 * nt_cmp - 2
+    sweeps_full = 3 * p["nt"] - 2
+    out = {}
+    img = torch.zeros(shape, dtype=torch.float32, device=dev)
+    for name, fl in forms.items():
+        c = rtmb.Context(rtmb.Params.from_input(q, flags=fl, device=dev.index or 0))
+        c.load_v2dt2(v2, from_host=True)
+        c.migrate_shot(sx, sy, sz, rec, img)  # allocation and warm-up
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        c.migrate_shot(sx, sy, sz, rec, img)
+        e1.record()
+        c.sync()
+        ms = e0.elapsed_time(e1)
+        err = float(torch.linalg.vector_norm(img.double() - ref)) / (ref_norm if ref_norm > 0 else 1.0)
+        per_sweep = ms / sweeps_cmp
+        out[name] = {"ms_per_sweep": round(per_sweep, 4), "s_per_shot": round(per_sweep * sweeps_full / 1e3, 3),
+                     "gpt_s": round(n_points(p) / (per_sweep * 1e-3) / 1e9, 2),
+                     "image_rel_l2_vs_fp64": float("%.3e" % err)}
+        c.close()
+    ok = {k: v for k, v in out.items() if v["image_rel_l2_vs_fp64"] <= 1e-3}
+    chosen = min(ok, key=lambda k: ok[k]["ms_per_sweep"]) if ok else "fp32_exact"
+    return {"nt": nt_cmp, "note": f"s_per_shot scaled to nt={p['nt']} from the nt={nt_cmp} run; FP64 oracle "
+                                  f"run took {f64_s:.1f} s", "forms": out, "chosen": chosen,
+            "chosen_vs_plain": round(out["fp32_exact"]["ms_per_sweep"] / out[chosen]["ms_per_sweep"], 3)}
+
+
 def run_b200(args, rank: int, world: int, local_rank: int) -> dict | None:
     import torch
     import rtmb
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     p = workload(args.size, args.nt)
-    flags = 0 if args.exact else rtmb.FLAG_FAST_FMA
+    flags = form_flags(rtmb, args.form)
     params = rtmb.Params.from_input(p, flags=flags, device=local_rank)
     v, vpe, v2, v2m = build_inputs(p, with_abc=True)
     stream = torch.cuda.Stream(device=dev)
@@ -325,11 +386,11 @@ def run_b200(args, rank: int, world: int, local_rank: int) -> dict | None:
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32" + ("" if args.exact else "-fma"),
+        "dtype": {"fp32_exact": "f32", "fp32_fma": "f32-fma"}.get(args.form, args.form + "-storage/f32-math"),
         "data": "synthetic (seeded salt model; record from this library's modeling pass)",
         "config": {"workload": f"rtm_rbc_{args.size}^3_nt{args.nt}", "grid": list(shape), "nt": p["nt"],
                    "stencil_order": 8, "boundary": "rbc", "shots_per_step_per_gpu": 1,
-                   "form": "exact" if args.exact else "fma",
+                   "form": args.form,
                    "l2": "inputs larger than L2 (%.0f MB per wavefield)" % (n_points(p) * 4 / 1e6),
                    "parallelism": f"shot-parallel x{world}"},
         "e2e": {"value": round(e2e_value, 3), "unit": "Gpt/s",
@@ -343,6 +404,11 @@ def run_b200(args, rank: int, world: int, local_rank: int) -> dict | None:
                     if v_["launches"]},
         "clocks": clk,
     }
+    if world == 1 and args.forms_nt > 0:
+        try:
+            out["forms"] = compare_forms(p, v2, rec, dev, min(args.forms_nt, p["nt"]))
+        except Exception as exc:  # report, do not fail the headline measurement
+            out["forms"] = {"failed": f"{exc}"[:300]}
     if world == 1 and not args.no_cpu_baseline:
         try:
             with tempfile.TemporaryDirectory() as wd:
@@ -357,6 +423,177 @@ def run_b200(args, rank: int, world: int, local_rank: int) -> dict | None:
             out["cpu_baseline"] = {"value": None, "unit": "Gpt/s", "cores": os.cpu_count(), "kind": "reference",
                                    "sample": f"failed: {exc}"[:300]}
     return out
+
+
+# ------------------------------------------------------------------------------------------ batch
+def survey_model(nx: int, ny: int, nz: int, dz: float, seed: int = 1234) -> np.ndarray:
+    """Seeded survey velocity: v(z) = 1500 + 0.6 z_m clipped at 4500 and a 4500 m/s salt ellipsoid
+    (semi-axes nx/8, ny/10, nz/8 cells) centred at 60% depth."""
+    z = np.arange(nz, dtype=np.float32) * dz
+    v = np.broadcast_to(np.minimum(1500.0 + 0.6 * z, 4500.0), (nx, ny, nz)).astype(np.float32)
+    cx, cy, cz = np.arange(nx) - nx / 2, np.arange(ny) - ny / 2, np.arange(nz) - 0.6 * nz
+    salt = ((cx / (nx / 8))[:, None, None] ** 2 + (cy / (ny / 10))[None, :, None] ** 2 +
+            (cz / (nz / 8))[None, None, :] ** 2) <= 1.0
+    v[salt] = 4500.0
+    rng = np.random.default_rng(seed)
+    v *= (1.0 + 0.01 * rng.standard_normal(v.shape)).astype(np.float32)
+    return np.clip(v, 1500.0, 4500.0).astype(np.float32)
+
+
+def run_batch(args) -> dict:
+    """Shots on uneven aperture sub-volumes of a survey, batched (rtmb_migrate_batch: one launch per
+    step for all shots, graph-captured time loop) against the single-shot driver one by one."""
+    import torch
+    import rtmb
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    snx, sny, snz = 2 * args.batch_size, 2 * args.batch_size, args.batch_size
+    blen, nt, dx = 40, args.batch_nt, 12.5
+    v = survey_model(snx, sny, snz, dx)
+    half = args.batch_size // 2  # apertures +-half cells around the source, clipped at the survey edges
+    grid = [(int(snx * (i + 0.5) / 4), int(sny * (j + 0.5) / 3)) for i in range(4) for j in range(3)]
+    flags = form_flags(rtmb, args.form) | rtmb.FLAG_USE_GRAPH
+    keep, shots = [], []
+    rng = np.random.default_rng(7)
+    for k, (gx, gy) in enumerate(grid):
+        x0, x1 = max(0, gx - half), min(snx, gx + half)
+        y0, y1 = max(0, gy - half), min(sny, gy + half)
+        nx, ny = x1 - x0, y1 - y0
+        ve = rtmb.prepare_velocity(v[x0:x1, y0:y1, :], blen, "rbc", seed=100 + k)
+        v2 = torch.from_numpy(rtmb.v2dt2(ve, 0.001)).to(dev)
+        rcx, rcy = nx // 2, ny // 2
+        rec = torch.from_numpy((rng.standard_normal((1, rcx, rcy, nt)) * 1e-3).astype(np.float32)).to(dev)
+        keep += [v2, rec]
+        shots.append(rtmb.Shot(nx=nx, ny=ny, nz=snz, ox=x0, oy=y0, oz=0, sx=gx - x0, sy=gy - y0, sz=0,
+                               receiver_start_x=0, receiver_start_y=0, receiver_depth_z=0, receiver_distance_x=2,
+                               receiver_distance_y=2, receiver_count_x=rcx, receiver_count_y=rcy,
+                               v2dt2=v2.data_ptr(), rec=rec.data_ptr()))
+    base = dict(nx=snx, ny=sny, nz=snz, blen=blen, nt=nt, ntstep=nt, stencil_order=8, dx=dx, dy=dx, dz=dx, dt=0.001,
+                fpeak=10.0, taper_factor=0.2, receiver_start_x=0, receiver_start_y=0, receiver_depth_z=0,
+                receiver_distance_x=2, receiver_distance_y=2, receiver_count_x=1, receiver_count_y=1,
+                boundary_condition="rbc")
+    ctx = rtmb.Context(rtmb.Params.from_input(base, flags=flags, device=0))
+    stack = torch.zeros((snx, sny, snz), dtype=torch.float64, device=dev)
+    ctx.migrate_batch(shots, stack)  # warm-up: graph capture and instantiation
+    ctx.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = ctx.launches
+    e0.record()
+    ctx.migrate_batch(shots, stack)
+    e1.record()
+    ctx.sync()
+    ms_batch = e0.elapsed_time(e1)
+    launches_batch = ctx.launches - l0
+    # one by one: the single-shot driver per aperture, images stacked in FP64
+    ms_single = 0.0
+    pts = 0
+    for s in shots:
+        q = dict(base, nx=s.nx, ny=s.ny, receiver_count_x=s.receiver_count_x, receiver_count_y=s.receiver_count_y)
+        c = rtmb.Context(rtmb.Params.from_input(q, flags=form_flags(rtmb, args.form), device=0))
+        c.load_v2dt2(s.v2dt2, from_host=False)
+        acc = torch.zeros(c.padded_shape, dtype=torch.float64, device=dev)
+        c.migrate_shot_acc64(s.sx, s.sy, s.sz, s.rec, acc)
+        c.sync()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record()
+        c.migrate_shot_acc64(s.sx, s.sy, s.sz, s.rec, acc)
+        a1.record()
+        c.sync()
+        ms_single += a0.elapsed_time(a1)
+        pts += int(np.prod(c.padded_shape))
+        c.close()
+    upd = pts * (3 * nt - 2)
+    sizes = sorted({(s.nx, s.ny) for s in shots})
+    return {"metric": "s per migrated shot, batched aperture shots", "workload": "batch",
+            "config": {"survey": [snx, sny, snz], "dx_m": dx, "shots": len(shots), "apertures_xy": sizes,
+                       "blen": blen, "nt": nt, "form": args.form, "fpeak_hz": 10.0},
+            "batched": {"s_per_shot": round(ms_batch / 1e3 / len(shots), 4), "gpt_s": round(upd / ms_batch / 1e6, 2),
+                        "launches": launches_batch},
+            "one_by_one": {"s_per_shot": round(ms_single / 1e3 / len(shots), 4),
+                           "gpt_s": round(upd / ms_single / 1e6, 2)},
+            "speedup": round(ms_single / ms_batch, 3)}
+
+
+# ------------------------------------------------------------------------------------------ closure
+def run_closure(args) -> dict:
+    """The learned 8-cell boundary closure against the tapered borders of 8 and 32 cells: reflected
+    energy = shot-record rel-L2 against the same shot on a domain padded so widely that no boundary
+    reflection returns within nt; wall time of a modeling shot on each grid."""
+    import torch
+    import rtmb
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    n, nt, wide = args.closure_size, args.closure_nt, args.closure_wide
+    v = salt_model(n)
+
+    def prm(blen, bc="hbc"):
+        return dict(nx=n, ny=n, nz=n, blen=blen, nt=nt, ntstep=nt, stencil_order=8, dx=10.0, dy=10.0, dz=10.0,
+                    dt=0.001, fpeak=15.0, taper_factor=0.2, receiver_start_x=0, receiver_start_y=0,
+                    receiver_depth_z=2, receiver_distance_x=2, receiver_distance_y=2, receiver_count_x=n // 2,
+                    receiver_count_y=n // 2, boundary_condition=bc)
+
+    def model(blen, shot, closure=None, min_scale=0.0, damp=0.0):
+        par = rtmb.Params.from_input(prm(blen), flags=rtmb.FLAG_FAST_FMA, device=0)
+        if closure is not None:
+            par.boundary = rtmb.BC_LEARNED
+        c = rtmb.Context(par)
+        c.load_v2dt2(rtmb.v2dt2(rtmb.prepare_velocity(v, blen, "abc"), 0.001), from_host=True)
+        if closure is not None:
+            c.closure_set(closure, min_scale, damp)
+        rec = torch.zeros((1, n // 2, n // 2, nt), device=dev)
+        c.model_shot(*shot, rec)  # warm-up
+        c.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        c.model_shot(*shot, rec)
+        e1.record()
+        c.sync()
+        ms = e0.elapsed_time(e1)
+        c.close()
+        return rec, ms
+
+    rng = np.random.default_rng(2024)
+    pos = lambda: (int(rng.integers(n // 6, n - n // 6)), int(rng.integers(n // 6, n - n // 6)), int(rng.integers(1, n // 8)))
+    train = [pos() for _ in range(args.closure_train_shots)]
+    held = [pos() for _ in range(args.closure_eval_shots)]
+    t0 = time.time()
+    pilot, _ = model(wide, train[0])
+    min_scale = 1e-4 * float(pilot.abs().max())
+    per_step, ts0, tstride = 4096, nt // 6, 2
+    cap = len(train) * per_step * ((nt - ts0) // tstride + 1)
+    X = torch.zeros((cap, rtmb.CLOSURE_NIN), dtype=torch.bfloat16, device=dev)
+    R = torch.zeros(cap, dtype=torch.float32, device=dev)
+    rows = 0
+    for k, sh in enumerate(train):
+        c = rtmb.Context(rtmb.Params.from_input(prm(wide), flags=rtmb.FLAG_FAST_FMA, device=0))
+        c.load_v2dt2(rtmb.v2dt2(rtmb.prepare_velocity(v, wide, "abc"), 0.001), from_host=True)
+        rows += c.closure_collect(*sh, ts0, tstride, per_step, 1000 + k, min_scale, X[rows:], R[rows:])
+        c.close()
+    t_collect = time.time() - t0
+    params = torch.from_numpy(rtmb.closure_init(17)).to(dev)
+    t1 = time.time()
+    losses = rtmb.closure_train(params, X, R, rows, args.closure_steps, 8192, 2e-3, 23, noise=0.05)
+    torch.cuda.synchronize()
+    t_train = time.time() - t1
+    res = {"learned_8": [], "taper_8": [], "taper_32": []}
+    ms = {k: [] for k in res}
+    for sh in held:
+        ref, _ = model(wide, sh)
+        for key, blen, cl in (("learned_8", 8, params), ("taper_8", 8, None), ("taper_32", 32, None)):
+            r, t = model(blen, sh, cl, min_scale, 0.3) if cl is not None else model(blen, sh)
+            res[key].append(float(torch.linalg.vector_norm((r - ref).double()) / torch.linalg.vector_norm(ref.double())))
+            ms[key].append(t)
+    mean = {k: float(np.mean(x)) for k, x in res.items()}
+    return {"metric": "reflected energy (record rel-L2 vs wide-padded run) and modeling time", "workload": "closure",
+            "config": {"model": [n, n, n], "nt": nt, "wide_border": wide, "fpeak_hz": 15.0,
+                       "train_shots": len(train), "eval_shots": len(held), "rows": rows,
+                       "train_steps": args.closure_steps, "batch": 8192},
+            "reflected_energy": {k: round(x, 4) for k, x in mean.items()},
+            "modeling_ms": {k: round(float(np.mean(x)), 2) for k, x in ms.items()},
+            "grid": {"learned_8": (n + 16) ** 3, "taper_8": (n + 16) ** 3, "taper_32": (n + 64) ** 3},
+            "falls_back_to_hbc": rtmb.closure_falls_back(mean["learned_8"], mean["taper_32"]),
+            "loss": {"first": float(losses[:10].mean()), "last": float(losses[-50:].mean())},
+            "seconds": {"collect": round(t_collect, 1), "train": round(t_train, 1)}}
 
 
 def run_reference_arm(args, rank: int) -> dict | None:
@@ -404,10 +641,26 @@ def main():
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--size", type=int, default=512, help="model edge in cells (workload: 512)")
     ap.add_argument("--nt", type=int, default=3000)
-    ap.add_argument("--exact", action="store_true", help="bit-exact stencil form instead of the FMA form")
+    ap.add_argument("--form", choices=FORMS, default="fp32_fma", help="arithmetic/storage form of the timed shots")
+    ap.add_argument("--exact", action="store_true", help="same as --form fp32_exact")
+    ap.add_argument("--workload", choices=("rtm", "batch", "closure"), default="rtm",
+                    help="rtm: the single-shot RTM line (default); batch: batched aperture shots against "
+                         "one-by-one; closure: the learned boundary closure against the tapered borders")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-size", type=int, default=256, help="batch workload: survey 2s x 2s x s cells")
+    ap.add_argument("--batch-nt", type=int, default=500)
+    ap.add_argument("--closure-size", type=int, default=96)
+    ap.add_argument("--closure-nt", type=int, default=600)
+    ap.add_argument("--closure-wide", type=int, default=120)
+    ap.add_argument("--closure-train-shots", type=int, default=8)
+    ap.add_argument("--closure-eval-shots", type=int, default=4)
+    ap.add_argument("--closure-steps", type=int, default=4000)
+    ap.add_argument("--forms-nt", type=int, default=300,
+                    help="nt of the storage-form comparison against the FP64 oracle (0: skip)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.exact:
+        args.form = "fp32_exact"
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -416,6 +669,8 @@ def main():
 
     if args.impl == "reference":
         out = run_reference_arm(args, rank)
+    elif args.workload != "rtm":
+        out = (run_batch if args.workload == "batch" else run_closure)(args) if rank == 0 else None
     else:
         if world > 1:
             import datetime

@@ -169,6 +169,9 @@ struct TmaShape {
     static_assert(2 * H <= D && D >= H + 2, "warm-up planes and the lookahead must fit in the P ring");
     static constexpr size_t PRING_BYTES = (size_t)D * STRIDE * sizeof(T);
     static constexpr size_t SMEM = PRING_BYTES + (size_t)R * CSLOT + 2 * (D + R) * sizeof(uint64_t);
+    // batched launches: one shot's StepArgs copied past the rings
+    static constexpr size_t ARGS_OFF = (SMEM + 15) / 16 * 16;
+    static constexpr size_t SMEM_BATCH = ARGS_OFF + sizeof(StepArgs);
 };
 
 // TAPER: kTaperNone / kTaperUpper / kTaperAll.  IMG: the epilogue accumulates the image.
@@ -594,7 +597,18 @@ __global__ void __launch_bounds__(kTmaThreads, 2) tma_batch_kernel(const __grid_
     const int bx = lin % b.gx[s];
     lin /= b.gx[s];
     const int by = lin % b.gy[s], bz = lin / b.gy[s];
-    tma_step_body<H, EXACT, TAPER, IMG, T, IT>(b.maps[s], b.args[s], b.coef, bx, by, bz);
+    // this shot's arguments in shared memory: read through a dynamic index the parameter space
+    // would be reloaded after every global store of the plane loop; shared memory cannot alias them.
+    // The copy sits in the dynamic region past the body's rings (a static __shared__ variable would
+    // move the dynamic base off the 128-byte alignment the TMA destinations need).
+    using S = TmaShape<H, IMG, T, IT>;
+    extern __shared__ __align__(128) unsigned char smem_b[];
+    StepArgs *sa = reinterpret_cast<StepArgs *>(smem_b + S::ARGS_OFF);
+    static_assert(sizeof(StepArgs) % 4 == 0, "copied as words");
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(&b.args[s]);
+    for (int i = threadIdx.x; i < (int)(sizeof(StepArgs) / 4); i += blockDim.x) reinterpret_cast<uint32_t *>(sa)[i] = src[i];
+    __syncthreads();
+    tma_step_body<H, EXACT, TAPER, IMG, T, IT>(b.maps[s], *sa, b.coef, bx, by, bz);
 }
 
 template <int H>
@@ -685,16 +699,16 @@ cudaError_t launch_tma_batch(const BatchArgs &b, bool exact, bool img, bool img6
     if constexpr (sizeof(T) == 4) {
         if (img64) return cudaErrorInvalidValue;
         if (exact)
-            return img ? run(tma_batch_kernel<4, true, kTaperNone, true>, TmaShape<4, true>::SMEM)
-                       : run(tma_batch_kernel<4, true, kTaperNone, false>, TmaShape<4, false>::SMEM);
-        return img ? run(tma_batch_kernel<4, false, kTaperNone, true>, TmaShape<4, true>::SMEM)
-                   : run(tma_batch_kernel<4, false, kTaperNone, false>, TmaShape<4, false>::SMEM);
+            return img ? run(tma_batch_kernel<4, true, kTaperNone, true>, TmaShape<4, true>::SMEM_BATCH)
+                       : run(tma_batch_kernel<4, true, kTaperNone, false>, TmaShape<4, false>::SMEM_BATCH);
+        return img ? run(tma_batch_kernel<4, false, kTaperNone, true>, TmaShape<4, true>::SMEM_BATCH)
+                   : run(tma_batch_kernel<4, false, kTaperNone, false>, TmaShape<4, false>::SMEM_BATCH);
     } else {
         if (exact) return cudaErrorInvalidValue;
-        if (!img) return run(tma_batch_kernel<4, false, kTaperNone, false, T, float>, TmaShape<4, false, T, float>::SMEM);
+        if (!img) return run(tma_batch_kernel<4, false, kTaperNone, false, T, float>, TmaShape<4, false, T, float>::SMEM_BATCH);
         if (img64)
-            return run(tma_batch_kernel<4, false, kTaperNone, true, T, double>, TmaShape<4, true, T, double>::SMEM);
-        return run(tma_batch_kernel<4, false, kTaperNone, true, T, float>, TmaShape<4, true, T, float>::SMEM);
+            return run(tma_batch_kernel<4, false, kTaperNone, true, T, double>, TmaShape<4, true, T, double>::SMEM_BATCH);
+        return run(tma_batch_kernel<4, false, kTaperNone, true, T, float>, TmaShape<4, true, T, float>::SMEM_BATCH);
     }
 }
 
