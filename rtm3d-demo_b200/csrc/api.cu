@@ -107,10 +107,12 @@ rtmb::StepArgs base_args(const rtmb_ctx *c) {
     a.nxe = c->nxe; a.nye = c->nye; a.nze = c->nze; a.blen = (int)c->p.blen;
     a.chunk = c->chunk;
     const int o = (int)c->p.stencil_order;
+    a.iso = 1;
     for (int i = 0; i <= o; ++i) {
         a.cx[i] = c->coefs[i];
         a.cy[i] = c->coefs[(o + 1) + i];
         a.cz[i] = c->coefs[2 * (o + 1) + i];
+        a.iso &= a.cx[i] == a.cy[i] && a.cx[i] == a.cz[i] && c->coefs[i] == c->coefs[o - i];
     }
     a.taper = c->d_taper;
     a.wavelet = c->d_wavelet;

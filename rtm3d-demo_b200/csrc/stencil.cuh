@@ -86,6 +86,7 @@ struct StepArgs {
     ScaleRec *sc_out;           // record of the level this launch writes into PP
     float inj;                  // bound on |values| written by injection (source, receivers, border)
     const float *inj_dev;       // optional device scalar added to inj
+    int iso;                    // cx == cy == cz, symmetric: the FMA form may use the packed symmetric sum
 };
 
 // Exponent of a produced level: the smallest e with bound * 2^-e < 2^15.  bound is
