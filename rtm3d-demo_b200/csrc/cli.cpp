@@ -6,8 +6,10 @@
 // with the same types, plus "verbose"), and runs the same process as the reference program
 // (src/Main.cpp:11-48 -> RTMAcousticProcess::rtm, src/process/RTMAcousticProcess.cpp:8-60):
 //   modeling   one shot record per shot, written as .seism chunks of ntstep steps into datdir
+//              (by a background task, while the next shot runs)
 //              (RTMAcousticController::rtmDistShotModeling, src/controller/RTMAcousticController.cpp:129-170);
-//   migration  .seism chunks read back per shot, HBC or RBC migration, images stacked, order-2
+//   migration  .seism chunks read back per shot (the next shot's by a background task while this
+//              one runs), HBC or RBC migration, images stacked, order-2
 //              Laplacian filter, borders removed, RTMIMG file written into outdir
 //              (rtmDistShotMigration, :172-269).
 // Velocity preparation follows RTMController::loadRTMVelocitiesModel (src/controller/RTMController.cpp:27-119):
@@ -26,6 +28,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <future>
 #include <iostream>
 #include <sstream>
 #include <string>
@@ -226,50 +229,82 @@ int run(const Param &p) {
 
     const size_t chunk = (size_t)p.receiver_count_x * p.receiver_count_y * p.ntstep;
     const size_t nchunks = p.nt / p.ntstep;
-    std::vector<float> rec(chunk * nchunks);
+    const size_t nrec = chunk * nchunks;
     float *d_rec = nullptr, *d_img = nullptr, *d_stack = nullptr, *d_out = nullptr;
     struct DevFree { float **ps[4]; ~DevFree() { for (auto p : ps) if (*p) cudaFree(*p); } } dfree{{&d_rec, &d_img, &d_stack, &d_out}};
-    unsigned nshots = p.source_count_x * p.source_count_y;
+    // two pinned host records: the shot being computed and the one being read (migration) or
+    // written (modeling) by the I/O thread at the same time
+    float *h_rec[2] = {nullptr, nullptr};
+    struct HostFree { float **ps[2]; ~HostFree() { for (auto p : ps) if (*p) cudaFreeHost(*p); } } hfree{{&h_rec[0], &h_rec[1]}};
+    for (auto &h : h_rec)
+        if (cudaMallocHost(&h, std::max<size_t>(nrec, 1) * sizeof(float)) != cudaSuccess)
+            throw Error("pinned host allocation failed");
+    const unsigned nshots = p.source_count_x * p.source_count_y;
     double t_total = 0.0;
     if (mig) {
-        if (cudaMalloc(&d_rec, std::max<size_t>(rec.size(), 1) * sizeof(float)) != cudaSuccess ||
+        if (cudaMalloc(&d_rec, std::max<size_t>(nrec, 1) * sizeof(float)) != cudaSuccess ||
             cudaMalloc(&d_img, n * sizeof(float)) != cudaSuccess || cudaMalloc(&d_stack, n * sizeof(float)) != cudaSuccess ||
             cudaMalloc(&d_out, (size_t)p.nx * p.ny * p.nz * sizeof(float)) != cudaSuccess ||
             cudaMemset(d_stack, 0, n * sizeof(float)) != cudaSuccess)
             throw Error("device allocation failed");
     }
-    unsigned shot = 0;
-    for (unsigned ix = 0; ix < p.source_count_x; ++ix) {      // RTMController.cpp:139-165
+    // the shots in the reference's order (RTMController.cpp:139-165)
+    struct Shot { unsigned sx, sy, sz; };
+    std::vector<Shot> shots;
+    for (unsigned ix = 0; ix < p.source_count_x; ++ix)
         for (unsigned iy = 0; iy < p.source_count_y; ++iy) {
-            const unsigned sx = ix * p.source_distance_x + p.source_start_x;
-            const unsigned sy = iy * p.source_distance_y + p.source_start_y;
-            const unsigned sz = p.source_depth_z;
-            if (sx >= p.nx || sy >= p.ny || sz >= p.nz)
-                throw Error("[ Invalid Source Position: (" + std::to_string(sx) + "," + std::to_string(sy) + "," +
-                            std::to_string(sz) + ") ]");
-            ++shot;
-            say(p, "Shot " + std::to_string(shot) + "/" + std::to_string(nshots) + " (" + std::to_string(sx) +
-                       "," + std::to_string(sy) + "," + std::to_string(sz) + "):");
+            const Shot s{ix * p.source_distance_x + p.source_start_x, iy * p.source_distance_y + p.source_start_y,
+                         p.source_depth_z};
+            if (s.sx >= p.nx || s.sy >= p.ny || s.sz >= p.nz)
+                throw Error("[ Invalid Source Position: (" + std::to_string(s.sx) + "," + std::to_string(s.sy) + "," +
+                            std::to_string(s.sz) + ") ]");
+            shots.push_back(s);
+        }
+    // record I/O off the compute path: one background task at a time reads the next shot's
+    // .seism chunks (migration) or writes the previous shot's (modeling) while the GPU runs
+    auto read_record = [&](const Shot &s, float *dst) {
+        for (size_t c = 0; c < nchunks; ++c) {
+            std::ifstream f(seismogram_name(p, s.sx, s.sy, s.sz, (unsigned)(c * p.ntstep)), std::ios::binary);
+            if (!f) throw Error("Input grid file '" + seismogram_name(p, s.sx, s.sy, s.sz, (unsigned)(c * p.ntstep)) +
+                                "' doesn't exist! Please check.");
+            f.read(reinterpret_cast<char *>(dst + c * chunk), chunk * sizeof(float));
+            if (static_cast<size_t>(f.gcount()) != chunk * sizeof(float)) throw Error("seismogram file too short");
+        }
+    };
+    auto write_record = [&](const Shot &s, const float *src) {
+        for (size_t c = 0; c < nchunks; ++c)
+            write_floats(seismogram_name(p, s.sx, s.sy, s.sz, (unsigned)(c * p.ntstep)), src + c * chunk, chunk);
+    };
+    std::future<void> io, wr[2];  // io: the reader; wr[b]: the writer of host buffer b
+    if (mig && !shots.empty()) io = std::async(std::launch::async, read_record, shots[0], h_rec[0]);
+    for (size_t k = 0; k < shots.size(); ++k) {
+        const Shot &s = shots[k];
+        say(p, "Shot " + std::to_string(k + 1) + "/" + std::to_string(nshots) + " (" + std::to_string(s.sx) + "," +
+                   std::to_string(s.sy) + "," + std::to_string(s.sz) + "):");
+        float *rec = h_rec[k & 1];
+        if (p.modeling) {
+            // buffer k & 1 may still be written out for shot k-2; shot k-1's files are written
+            // meanwhile from the other buffer while this shot runs
+            if (wr[k & 1].valid()) wr[k & 1].get();
             const auto t0 = std::chrono::steady_clock::now();
-            if (p.modeling) {
-                check(rtmb_model_shot_host(ctx, sx, sy, sz, rec.data()), ctx, "modeling");
-                t_total += seconds_since(t0);
-                for (size_t c = 0; c < nchunks; ++c)
-                    write_floats(seismogram_name(p, sx, sy, sz, (unsigned)(c * p.ntstep)), rec.data() + c * chunk, chunk);
-            } else if (mig) {
-                for (size_t c = 0; c < nchunks; ++c) {
-                    std::vector<float> part = read_floats(seismogram_name(p, sx, sy, sz, (unsigned)(c * p.ntstep)), chunk);
-                    std::copy(part.begin(), part.end(), rec.begin() + c * chunk);
-                }
-                if (cudaMemcpy(d_rec, rec.data(), rec.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
-                    throw Error("record upload failed");
-                check(rtmb_migrate_shot(ctx, sx, sy, sz, d_rec, d_img), ctx, "migration");
-                check(rtmb_image_stack(ctx, d_stack, d_img), ctx, "image stack");
-                check(rtmb_sync(ctx), ctx, "sync");
-                t_total += seconds_since(t0);
-            }
+            check(rtmb_model_shot_host(ctx, s.sx, s.sy, s.sz, rec), ctx, "modeling");
+            t_total += seconds_since(t0);
+            wr[k & 1] = std::async(std::launch::async, write_record, s, rec);
+        } else if (mig) {
+            io.get();  // this shot's record is on the host
+            if (k + 1 < shots.size()) io = std::async(std::launch::async, read_record, shots[k + 1], h_rec[(k + 1) & 1]);
+            const auto t0 = std::chrono::steady_clock::now();
+            if (cudaMemcpy(d_rec, rec, nrec * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+                throw Error("record upload failed");
+            check(rtmb_migrate_shot(ctx, s.sx, s.sy, s.sz, d_rec, d_img), ctx, "migration");
+            check(rtmb_image_stack(ctx, d_stack, d_img), ctx, "image stack");
+            check(rtmb_sync(ctx), ctx, "sync");
+            t_total += seconds_since(t0);
         }
     }
+    if (io.valid()) io.get();
+    for (auto &w : wr)
+        if (w.valid()) w.get();
     if (mig) {
         check(rtmb_image_finalize(ctx, d_stack, d_out), ctx, "image filter");
         check(rtmb_sync(ctx), ctx, "sync");
