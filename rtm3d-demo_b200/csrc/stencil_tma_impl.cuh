@@ -325,6 +325,7 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
         }
     }
     const bool special = src_e >= 0 || rec_e >= 0 || umask != 0 || qmask != 0;
+    const float wsrc = src_e >= 0 ? __ldg(a.wavelet + a.it) : 0.f;  // this launch's Ricker sample
     bool tile_taper_yz = false;  // does this CTA's tile touch the taper region (x border aside)?
     if (TAPER == kTaperAll)
         tile_taper_yz = (yt0 - H < a.blen) || (yt0 + kTY + H > a.nye - a.blen) || (zt0 - ZH < a.blen) ||
@@ -412,6 +413,17 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
         {
             const int x = xc0 + i;
             const int kin = i + 2 * H;
+            // the record value the receiver step injects: loaded now so that its latency (a strided
+            // gather) overlaps the stencil instead of stalling the warp at the end of the plane
+            const float *rec_p = nullptr;
+            float rec_v = 0.f;
+            if (special) {
+                const int dxr = x - a.rx0;
+                if (rec_e >= 0 && dxr >= 0 && dxr % a.rdx == 0 && dxr / a.rdx < a.rcx) {
+                    rec_p = a.rec + a.rec_base + (dxr / a.rdx) * a.rec_si + rec_j * a.rec_sj;
+                    if (IMG && a.rec_mode != kRecSample) rec_v = __ldg(rec_p);  // read-only in this launch
+                }
+            }
             wait_p(s_in, ph_in);
             const T *s = pring + s_mid * STRIDE;  // the centre plane's tile
             if constexpr (CB) {
@@ -561,15 +573,12 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
 #pragma unroll
                 for (int e = 0; e < kVZ; ++e) {
                     const int z = z0 + e;
-                    if (e == src_e && x == a.sxe) npp[e] = npp[e] + a.wavelet[a.it];
-                    if (e == rec_e) {
-                        const int dxr = x - a.rx0;
-                        if (dxr >= 0 && dxr % a.rdx == 0 && dxr / a.rdx < a.rcx) {
-                            float *rp = a.rec + a.rec_base + (dxr / a.rdx) * a.rec_si + rec_j * a.rec_sj;
-                            if (a.rec_mode == kRecSample) *rp = npp[e];
-                            else if (a.rec_mode == kRecOverwrite) npp[e] = *rp;
-                            else npp[e] = npp[e] + *rp;
-                        }
+                    if (e == src_e && x == a.sxe) npp[e] = npp[e] + wsrc;
+                    if (e == rec_e && rec_p) {
+                        const float rv = IMG ? rec_v : *rec_p;
+                        if (a.rec_mode == kRecSample) *const_cast<float *>(rec_p) = npp[e];
+                        else if (a.rec_mode == kRecOverwrite) npp[e] = rv;
+                        else npp[e] = npp[e] + rv;
                     }
                     if ((umask >> e) & 1u) {
                         float *up = a.upb + ((size_t)x * a.nye + y) * H + (z - (a.blen - H));
