@@ -86,6 +86,12 @@ typedef enum rtmb_boundary {
 /* With a storage flag: accumulate the image over the time steps in FP64 (the caller's FP32 image
  * is written from it at the end of the shot). */
 #define RTMB_FLAG_IMG_F64       0x100u
+/* FP32 migration in the FMA form runs the backward source and receiver steps of each time step as
+ * ONE launch (both wavefields and the image in one pass over the grid: 36 instead of 44 bytes per
+ * point) when stencil_order is 8 and rows are 16-byte aligned; same results as two launches (no
+ * reference counterpart: the reference runs them as separate operators).  This flag keeps the two
+ * launches.  The exact form keeps two launches: in one it is issue-bound and gains nothing. */
+#define RTMB_FLAG_NO_DUAL       0x200u
 
 /* The input.json parameters on the path (include/RTMParam.hpp:188-249). */
 typedef struct rtmb_params {
@@ -125,12 +131,13 @@ uint64_t rtmb_launch_count(const rtmb_ctx *ctx);
  * millisecond wall times per phase, src/kernel/RTMKernel.cpp:11-80).  When enabled, every driver
  * launch is bracketed by CUDA events on the context's stream; the durations are summed per category
  * at the end of each driver call.  Enabling clears the totals. */
-#define RTMB_PROF_CATEGORIES 5
+#define RTMB_PROF_CATEGORIES 6
 #define RTMB_PROF_MODEL 0             /* modeling step (taper, source, receivers fused) */
 #define RTMB_PROF_FORWARD 1           /* migration forward step */
 #define RTMB_PROF_BACKWARD_SOURCE 2   /* backward source-wavefield reconstruction step */
 #define RTMB_PROF_BACKWARD_RECEIVER 3 /* backward receiver step with receiver injection and imaging */
 #define RTMB_PROF_OTHER 4
+#define RTMB_PROF_BACKWARD_DUAL 5     /* source and receiver steps with imaging in one launch */
 int rtmb_profile(rtmb_ctx *ctx, int enable);
 /* ms[RTMB_PROF_CATEGORIES]: summed kernel time; launches[RTMB_PROF_CATEGORIES]: launch counts. */
 int rtmb_profile_read(const rtmb_ctx *ctx, double *ms, uint64_t *launches);

@@ -353,6 +353,8 @@ void rtmb::driver::init_geometry(rtmb_ctx *ctx) {
     const int nxi = ctx->nxe - 2 * ctx->h, nyi = ctx->nye - 2 * ctx->h;
     const int tiles = ((ctx->nze + rtmb::kTZ - 1) / rtmb::kTZ) * ((nyi + rtmb::kTY - 1) / rtmb::kTY);
     ctx->chunk = pick_chunk(nxi > 0 ? nxi : 1, tiles > 0 ? tiles : 1);
+    const int tiles8 = ((ctx->nze + rtmb::kTZ - 1) / rtmb::kTZ) * ((nyi + 7) / 8);  // the dual step's 64 x 8 tiles
+    ctx->dual_chunk = pick_chunk(nxi > 0 ? nxi : 1, tiles8 > 0 ? tiles8 : 1);
     rtmb_stencil_coefs(p.stencil_order, p.dx, p.dy, p.dz, ctx->coefs);
 }
 
@@ -698,7 +700,26 @@ int migrate_impl(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const flo
     rcv.store = ctx->store;
     rcv.inj_dev = st ? ctx->d_inj : nullptr;
     const int rmode = (p.flags & RTMB_FLAG_RCV_ADD) ? rtmb::kRecAdd : rtmb::kRecOverwrite;
+    // FP32 FMA form: the source and receiver steps of one time step in one launch
+    const bool dual = !st && !exact(ctx) && p.stencil_order == 8 && tma_ok(ctx) && !(p.flags & RTMB_FLAG_NO_DUAL);
     for (int it = (int)p.nt - 1; it >= 0; --it) {
+        if (dual && it < (int)p.nt - 2) {
+            src.P = s_cur; src.PP = s_prev; src.it = it;
+            if (hbc) src.upb = ctx->d_upb + (size_t)it * upb_step;
+            rcv.P = rP; rcv.PP = rPP; rcv.it = it;
+            rcv.ps = nullptr;
+            set_receivers(rcv, ctx, rmode, const_cast<float *>(rec), it);
+            rcv.chunk = ctx->dual_chunk;
+            if (rtmb::dual_step_supported(src, rcv, (int)p.stencil_order)) {
+                LAUNCH_CAT(RTMB_PROF_BACKWARD_DUAL,
+                           rtmb::launch_dual_step(src, rcv, (int)p.stencil_order, exact(ctx), ctx->stream));
+                rcv.chunk = ctx->chunk;
+                std::swap(s_cur, s_prev);
+                std::swap(rP, rPP);
+                continue;
+            }
+            rcv.chunk = ctx->chunk;
+        }
         if (it == (int)p.nt - 2) {
             s_cur = sP;
             s_prev = sPP;

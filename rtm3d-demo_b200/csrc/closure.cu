@@ -345,15 +345,14 @@ __host__ __device__ inline uint64_t mix64(uint64_t x) {
 }
 
 // Training-pair collection, before the step: features of cells_per_step strip cells drawn at
-// random (seeded) from p(t) = P and p(t-1) = PP.  Cells whose neighbourhood max |p| is below
-// min_scale are skipped: far ahead of the wavefront the stencil's numerical tail is orders of
-// magnitude below the waves the closure must absorb.
+// random (seeded) from p(t) = P and p(t-1) = PP, into staging row j.  Cells whose neighbourhood max
+// |p| is below min_scale are marked invalid: far ahead of the wavefront the stencil's numerical tail
+// is orders of magnitude below the waves the closure must absorb.
 __global__ void sample_features_kernel(const float *__restrict__ P, const float *__restrict__ PP,
                                        const float *__restrict__ V, Box b, const uint32_t *__restrict__ cells,
                                        const uint8_t *__restrict__ faces, long long ncells, int per_step,
-                                       uint64_t key, float inv_dx, float min_scale, __nv_bfloat16 *X,
-                                       unsigned long long cap,
-                                       unsigned long long *count, long long *slot_of, float *stash) {
+                                       uint64_t key, float inv_dx, float min_scale, __nv_bfloat16 *Xs,
+                                       long long *slot_of, float *stash) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= per_step) return;
     const long long i = (long long)(mix64(key + (uint64_t)j) % (uint64_t)ncells);
@@ -362,16 +361,59 @@ __global__ void sample_features_kernel(const float *__restrict__ P, const float 
     const int cx = (int)(off / plane) - b.ox, cy = (int)((off % plane) / b.az) - b.oy, cz = (int)(off % b.az) - b.oz;
     float feat[kUsed], base;
     const float s = gather(P, PP, V, b, cx, cy, cz, faces[i], inv_dx, feat, &base);
-    slot_of[j] = -1;
-    if (!(s > 0.f) || s < min_scale) return;
-    const unsigned long long slot = atomicAdd(count, 1ull);
-    if (slot >= cap) return;
-    slot_of[j] = (long long)slot;
+    const bool valid = s > 0.f && s >= min_scale;
+    slot_of[j] = valid ? 1 : 0;
     stash[3 * j] = __uint_as_float(off);
     stash[3 * j + 1] = base;
     stash[3 * j + 2] = s;
-    __nv_bfloat16 *row = X + slot * kIn;
-    for (int k = 0; k < kIn; ++k) row[k] = __float2bfloat16_rn(k < kUsed ? feat[k] : 0.f);
+    __nv_bfloat16 *row = Xs + (long long)j * kIn;
+    for (int k = 0; k < kIn; ++k) row[k] = __float2bfloat16_rn(valid && k < kUsed ? feat[k] : 0.f);
+}
+
+// The valid staging rows of this step appended to (X, count) in staging order, so that the data
+// set (and the training that draws from it) does not depend on thread timing: one block scans the
+// valid flags; slot_of[j] becomes the row's slot, or -1.
+__global__ void __launch_bounds__(1024) compact_rows_kernel(const __nv_bfloat16 *__restrict__ Xs, int per_step,
+                                                             __nv_bfloat16 *X, unsigned long long cap,
+                                                             unsigned long long *count, long long *slot_of) {
+    __shared__ int warp_sums[32];
+    __shared__ unsigned long long base_s;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) base_s = *count;
+    __syncthreads();
+    for (int j0 = 0; j0 < per_step; j0 += 1024) {
+        const int j = j0 + tid;
+        const int v = j < per_step ? (int)slot_of[j] : 0;
+        const unsigned ballot = __ballot_sync(0xffffffffu, v);
+        const int in_warp = __popc(ballot & ((1u << lane) - 1u));
+        if (lane == 31) warp_sums[warp] = in_warp + v;
+        __syncthreads();
+        if (warp == 0) {
+            int w = warp_sums[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o) w += t;
+            }
+            warp_sums[lane] = w;  // inclusive prefix over warps
+        }
+        __syncthreads();
+        const int before = (warp > 0 ? warp_sums[warp - 1] : 0) + in_warp;
+        const unsigned long long slot = base_s + (unsigned long long)before;
+        if (j < per_step) {
+            if (v && slot < cap) {
+                slot_of[j] = (long long)slot;
+                const uint4 *src = reinterpret_cast<const uint4 *>(Xs + (long long)j * kIn);
+                uint4 *dst = reinterpret_cast<uint4 *>(X + slot * kIn);
+                for (int c = 0; c < kIn / 8; ++c) dst[c] = src[c];
+            } else {
+                slot_of[j] = -1;
+            }
+        }
+        __syncthreads();
+        if (tid == 0) base_s += (unsigned long long)warp_sums[31];
+        __syncthreads();
+    }
+    if (tid == 0) *count = base_s;
 }
 
 // ... after the step: the target r = (p(t+1) - base) / s.
@@ -675,7 +717,7 @@ struct CollectHook : rtmb::driver::StepHook {
     int t0, tstride, per_step;
     uint64_t seed;
     float inv_dx, min_scale;
-    __nv_bfloat16 *X;
+    __nv_bfloat16 *X, *Xs;
     float *R;
     unsigned long long cap, *count;
     long long *slot_of;
@@ -685,8 +727,9 @@ struct CollectHook : rtmb::driver::StepHook {
         if (!due(it)) return 0;
         sample_features_kernel<<<(per_step + 127) / 128, 128, 0, ctx->stream>>>(
             P, PP, ctx->d_v2dt2, box, cells, faces, ncells, per_step, mix64(seed ^ (0x5851F42D4C957F2Dull * (it + 1))),
-            inv_dx, min_scale, X, cap, count, slot_of, stash);
-        ++ctx->launches;
+            inv_dx, min_scale, Xs, slot_of, stash);
+        compact_rows_kernel<<<1, 1024, 0, ctx->stream>>>(Xs, per_step, X, cap, count, slot_of);
+        ctx->launches += 2;
         return cudaGetLastError() == cudaSuccess ? 0 : RTMB_ECUDA;
     }
     int after(int it, const float *, float *PP) override {
@@ -775,14 +818,16 @@ int rtmb_closure_collect(rtmb_ctx *wide, uint32_t sx, uint32_t sy, uint32_t sz, 
     uint8_t *d_faces = nullptr;
     long long *slot_of = nullptr;
     float *stash = nullptr;
+    __nv_bfloat16 *Xs = nullptr;
     unsigned long long *d_count = nullptr;
     auto cleanup = [&]() {
-        cudaFree(d_cells); cudaFree(d_faces); cudaFree(slot_of); cudaFree(stash); cudaFree(d_count);
+        cudaFree(d_cells); cudaFree(d_faces); cudaFree(slot_of); cudaFree(stash); cudaFree(d_count); cudaFree(Xs);
     };
     if (cudaMalloc(&d_cells, cells.size() * 4) != cudaSuccess || cudaMalloc(&d_faces, faces.size()) != cudaSuccess ||
         cudaMalloc(&slot_of, per_step * sizeof(long long)) != cudaSuccess ||
         cudaMalloc(&stash, 3 * (size_t)per_step * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&d_count, sizeof(unsigned long long)) != cudaSuccess) {
+        cudaMalloc(&d_count, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&Xs, (size_t)per_step * kIn * sizeof(__nv_bfloat16)) != cudaSuccess) {
         cleanup();
         return RTMB_ENOMEM;
     }
@@ -793,7 +838,7 @@ int rtmb_closure_collect(rtmb_ctx *wide, uint32_t sx, uint32_t sy, uint32_t sz, 
     hook.ctx = ctx; hook.box = box; hook.cells = d_cells; hook.faces = d_faces; hook.ncells = (long long)cells.size();
     hook.t0 = (int)t0; hook.tstride = (int)tstride; hook.per_step = (int)per_step; hook.seed = seed;
     hook.inv_dx = 1.f / p.dx; hook.min_scale = min_scale; hook.X = static_cast<__nv_bfloat16 *>(X); hook.R = R; hook.cap = capacity;
-    hook.count = d_count; hook.slot_of = slot_of; hook.stash = stash;
+    hook.count = d_count; hook.slot_of = slot_of; hook.stash = stash; hook.Xs = Xs;
     float *P = nullptr, *PP = nullptr;
     rc = rtmb::driver::run_forward(ctx, sx, sy, sz, rtmb::kTaperAll, nullptr, nullptr, &P, &PP, RTMB_PROF_MODEL,
                                    nullptr, &hook);

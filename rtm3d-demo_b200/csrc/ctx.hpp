@@ -26,6 +26,7 @@ struct rtmb_ctx {
     float *d_upb = nullptr;      // [nt][nxe][nye][h] (HBC)
     float *d_rec = nullptr, *d_img = nullptr;  // staging for the host-buffer forms
     int chunk = 0;
+    int dual_chunk = 0;  // x planes per CTA of the dual-wavefield backward step (64 x 8 tiles)
     uint64_t launches = 0;
     // storage forms (RTMB_FLAG_STORE_*): element type of d_w, one scale record per stored level
     int store = rtmb::kStoreF32;

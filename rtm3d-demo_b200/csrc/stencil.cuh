@@ -110,6 +110,13 @@ cudaError_t launch_step(const StepArgs &a, int order, bool exact, cudaStream_t s
 // (args[0]'s are used).  At most 12 shots.
 cudaError_t launch_step_batch(const StepArgs *args, int nshots, int order, bool exact, cudaStream_t s);
 
+// The dual-wavefield backward step: src advances the reconstructed source wavefield (no taper,
+// optional upper-border restore), rcv the receiver wavefield with its taper, receiver injection and
+// the image of the new source values (rcv.ps is not read).  One launch instead of two; FP32, order 8,
+// TMA-aligned volumes, rcv.chunk x planes per CTA (64 x 8 tiles).
+bool dual_step_supported(const StepArgs &src, const StepArgs &rcv, int order);
+cudaError_t launch_dual_step(const StepArgs &src, const StepArgs &rcv, int order, bool exact, cudaStream_t s);
+
 // Whether the 16-bit storage forms (and the FP64 image) can run on this geometry: order 8 and
 // z rows whose 16-bit pitch is a multiple of 16 bytes (nze % 8 == 0).
 bool storage_form_supported(int order, int nze);

@@ -1,0 +1,430 @@
+// stencil_dual_impl.cuh -- the dual-wavefield backward step (sm_100a, FP32): one launch advances the
+// reconstructed source wavefield S and the back-propagated receiver wavefield R one step and adds
+// S_new * R_new to the image, which the separate launches do in two passes (the source step, then
+// the receiver step reading S_new back from HBM).  Per point it moves 36 bytes instead of 16 + 28:
+// v2dt2 is read once and S_new never leaves the chip for the image.
+//
+// Same arithmetic per point as the single-wavefield kernel (stencil_tma_impl.cuh), so results are
+// bit-identical to the two launches, in both arithmetic forms.
+//
+// CTA: eight consumer warps and one producer warp, two CTAs per SM.  Warps 0-3 step S, warps 4-7
+// step R, on the same 64 (z) x 8 (y) tile and x chunk.  The producer fills two P rings (S and R halo
+// tiles) and one core ring (S_prev, R_prev, v2dt2, IMG) with TMA; the source warps hand S_new of each
+// plane to the receiver warps through a shared-memory exchange ring with its own full/empty
+// mbarriers.  Every wait is bounded, as in the single-wavefield kernel.
+#pragma once
+#include "stencil_tma_impl.cuh"
+
+namespace rtmb {
+namespace detail {
+
+constexpr int kDTY = 8;                        // tile rows (y)
+constexpr int kGThreads = (kTZ / kVZ) * kDTY;  // consumer threads per wavefield: 128
+constexpr int kDualThreads = 2 * kGThreads + 32;
+
+struct DualMaps {
+    CUtensorMap ps, pr;            // halo boxes of S and R
+    CUtensorMap pps, ppr, v, img;  // core boxes
+};
+
+struct DualArgs {
+    StepArgs s;  // the source step (no taper; upper-border restore for HBC)
+    StepArgs r;  // the receiver step (taper, receiver injection, image)
+};
+
+template <int H>
+struct DualShape {
+    static constexpr int ZH = ((H + 3) / 4) * 4;
+    static constexpr int SROWS = kDTY + 2 * H;
+    static constexpr int SPITCH = kTZ + 2 * ZH;
+    static constexpr int STAGE = SROWS * SPITCH;
+    static constexpr int STRIDE = ((STAGE + 31) / 32) * 32;  // 128-byte slots
+    static constexpr int CORE = kTZ * kDTY;
+    static constexpr int OFF_PPR = CORE * 4, OFF_V = 2 * CORE * 4, OFF_IMG = 3 * CORE * 4, CSLOT = 4 * CORE * 4;
+    static constexpr int D = H + 4, R = 3, E = 3;
+    static_assert(2 * H <= D, "warm-up planes must fit in the P rings");
+    static constexpr size_t RING_BYTES = (size_t)D * STRIDE * 4;
+    static constexpr size_t XOFF = 2 * RING_BYTES + (size_t)R * CSLOT;  // exchange slots
+    static constexpr size_t BOFF = XOFF + (size_t)E * CORE * 4;         // barriers
+    static constexpr size_t SMEM = BOFF + (size_t)(4 * D + 2 * R + 2 * E) * sizeof(uint64_t);
+};
+
+// One wavefield's consumer warps.  ROLE 0: source (S), ROLE 1: receiver (R) with the image.
+template <int H, bool EXACT, int TAPER, int ROLE>
+__device__ __forceinline__ void dual_consumer(const StepArgs &a, const StepArgs &coef, const float *pring,
+                                              const unsigned char *cring, float *xring, uint64_t *pfull,
+                                              uint64_t *pempty, uint64_t *cfull, uint64_t *cempty, uint64_t *xfull,
+                                              uint64_t *xempty, int tid, int zt0, int yt0, int xc0, int n) {
+    using S = DualShape<H>;
+    constexpr int ZH = S::ZH, SPITCH = S::SPITCH, STAGE = S::STAGE, STRIDE = S::STRIDE, D = S::D, R = S::R,
+                  E = S::E, CSLOT = S::CSLOT, CORE = S::CORE;
+    constexpr int NQ = 2 * H + 1;
+    constexpr int ZQ = kTZ / kVZ;
+    constexpr bool RCV = ROLE == 1;
+    constexpr int TP = RCV ? TAPER : kTaperNone;
+    constexpr bool CB = TP != kTaperNone;  // named barrier 2 among the receiver warps
+    const int lane = tid & 31;
+    const int tz = tid % ZQ, ty = tid / ZQ;
+    const int z0 = zt0 + tz * kVZ;
+    const int y = yt0 + ty;
+    const size_t plane = (size_t)a.nye * a.nze;
+
+    auto group_sync = [&]() { asm volatile("bar.sync 2, %0;" ::"n"(kGThreads) : "memory"); };
+    auto group_sync_or = [&](bool v) {
+        uint32_t out;
+        asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, 2, %2, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+                     : "=r"(out)
+                     : "r"((uint32_t)v), "n"(kGThreads)
+                     : "memory");
+        return out != 0;
+    };
+
+    const bool row_ok = y < a.nye && z0 < a.nze;
+    const bool y_ok = y < a.nye - H;
+    unsigned vmask = 0, imask = 0, umask = 0;
+#pragma unroll
+    for (int e = 0; e < kVZ; ++e) {
+        const int z = z0 + e;
+        const bool v = y_ok && z >= H && z < a.nze - H;
+        if (v) vmask |= 1u << e;
+        if (v && RCV && z >= a.img_z0 && z < a.img_z1) imask |= 1u << e;
+        if (v && a.upb_mode != kUpbNone && z >= a.blen - H && z < a.blen) umask |= 1u << e;
+    }
+    int rec_e = -1, rec_j = 0;
+    if (RCV && a.rec_mode != kRecNone && a.rz >= z0 && a.rz < z0 + kVZ && ((vmask >> (a.rz - z0)) & 1u)) {
+        const int dyr = y - a.ry0;
+        if (dyr >= 0 && dyr % a.rdy == 0 && dyr / a.rdy < a.rcy) {
+            rec_e = a.rz - z0;
+            rec_j = dyr / a.rdy;
+        }
+    }
+    const bool special = rec_e >= 0 || umask != 0;
+    bool tile_taper_yz = false;
+    if (TP == kTaperUpper) tile_taper_yz = (zt0 - ZH < a.blen);
+    const bool pp_taper_yz = TP == kTaperUpper && z0 < a.blen;
+    const size_t row_off = (size_t)y * a.nze + z0;
+    float *PPp = a.PP + row_off;
+    const int col = ZH + tz * kVZ;
+    const int ccol = ty * kTZ + tz * kVZ;
+
+    bool bad_wait = false;
+    auto wait_p = [&](int slot, int parity) {
+        bad_wait |= !__all_sync(0xffffffffu, mbar_wait(&pfull[slot], parity));
+    };
+    auto release = [&](uint64_t *bar) {
+        __syncwarp();
+        if (lane == 0) mbar_arrive(bar);
+    };
+    auto taper_stage = [&](int k, int slot) {  // receiver form with the upper taper only
+        if (!tile_taper_yz) return;
+        const int x = xc0 - H + k;
+        float *st = const_cast<float *>(pring) + slot * STRIDE;
+        for (int c = tid; c < STAGE; c += kGThreads) {
+            const int r = c / SPITCH, cc = c % SPITCH;
+            const int yy = yt0 - H + r, zz = zt0 - ZH + cc;
+            if (yy >= a.nye || zz < 0 || zz >= a.nze) continue;
+            st[c] = taper_once(st[c], x, yy, zz, a);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        group_sync();
+    };
+
+    float4 q[NQ];
+    float nanacc = 0.f;
+    // the single-wavefield kernel's packed symmetric form for isotropic grids (same rounding)
+    const bool iso = !EXACT && a.iso;
+    f32x2 cpk[H + 1];
+    cpk[0] = pk2(coef.cx[H] + coef.cy[H] + coef.cz[H], coef.cx[H] + coef.cy[H] + coef.cz[H]);
+#pragma unroll
+    for (int k = 1; k <= H; ++k) cpk[k] = pk2(coef.cx[H + k], coef.cx[H + k]);
+    int s_in = (2 * H) % D, ph_in = ((2 * H) / D) & 1, s_mid = H % D, s_core = 0, ph_core = 0, s_x = 0, ph_x = 0;
+    for (int k = 0; k < 2 * H; ++k) {
+        wait_p(k, 0);
+        if (CB) taper_stage(k, k);
+    }
+    if (CB ? group_sync_or(bad_wait) : bad_wait) goto drain;
+#pragma unroll
+    for (int k = 0; k < 2 * H; ++k) q[k + 1] = ld_f4(pring + k * STRIDE + (ty + H) * SPITCH + col);
+#pragma unroll
+    for (int k = 0; k < H; ++k) release(&pempty[k]);
+
+#pragma unroll 1
+    for (int i = 0; i < n; ++i, s_in = s_in + 1 == D ? (ph_in ^= 1, 0) : s_in + 1, s_mid = s_mid + 1 == D ? 0 : s_mid + 1,
+                           s_core = s_core + 1 == R ? (ph_core ^= 1, 0) : s_core + 1,
+                           s_x = s_x + 1 == E ? (ph_x ^= 1, 0) : s_x + 1) {
+        const int x = xc0 + i;
+        const int kin = i + 2 * H;
+        // the record value this plane injects, loaded now so that its latency overlaps the stencil
+        const float *rec_p = nullptr;
+        float rec_v = 0.f;
+        if (RCV && rec_e >= 0) {
+            const int dxr = x - a.rx0;
+            if (dxr >= 0 && dxr % a.rdx == 0 && dxr / a.rdx < a.rcx) {
+                rec_p = a.rec + a.rec_base + (dxr / a.rdx) * a.rec_si + rec_j * a.rec_sj;
+                rec_v = __ldg(rec_p);
+            }
+        }
+        wait_p(s_in, ph_in);
+        const float *s = pring + s_mid * STRIDE;
+        if constexpr (CB) {
+            if (group_sync_or(bad_wait)) goto drain;
+            taper_stage(kin, s_in);
+        } else if (bad_wait) {
+            goto drain;
+        }
+#pragma unroll
+        for (int k = 0; k < NQ - 1; ++k) q[k] = q[k + 1];
+        q[NQ - 1] = ld_f4(pring + s_in * STRIDE + (ty + H) * SPITCH + col);
+
+        float lap[kVZ] = {0.f, 0.f, 0.f, 0.f};
+        if (row_ok) {
+            float zr[kVZ + 2 * ZH];
+#pragma unroll
+            for (int k = 0; k < (kVZ + 2 * ZH) / 4; ++k) {
+                const float4 t4 = (k == ZH / 4) ? q[H] : ld_f4(s + (ty + H) * SPITCH + col - ZH + 4 * k);
+                zr[4 * k + 0] = t4.x; zr[4 * k + 1] = t4.y; zr[4 * k + 2] = t4.z; zr[4 * k + 3] = t4.w;
+            }
+            if (EXACT) {
+                float ax[kVZ], ay[kVZ], az[kVZ];
+#pragma unroll
+                for (int e = 0; e < kVZ; ++e) { ax[e] = 0.f; ay[e] = 0.f; az[e] = 0.f; }
+#pragma unroll
+                for (int io = 0; io < NQ; ++io) {
+                    const float4 qx = q[io];
+                    const float4 ry = (io == H) ? q[H] : ld_f4(s + (ty + io) * SPITCH + col);
+#pragma unroll
+                    for (int e = 0; e < kVZ; ++e) {
+                        ax[e] = ax[e] + get(qx, e) * coef.cx[io];
+                        ay[e] = ay[e] + get(ry, e) * coef.cy[io];
+                        az[e] = az[e] + zr[ZH - H + e + io] * coef.cz[io];
+                    }
+                }
+#pragma unroll
+                for (int e = 0; e < kVZ; ++e) lap[e] = ax[e] + ay[e] + az[e];
+            } else if (iso) {
+                const float4 qc = q[H];
+                f32x2 l0 = mul2(pk2(qc.x, qc.y), cpk[0]), l1 = mul2(pk2(qc.z, qc.w), cpk[0]);
+#pragma unroll
+                for (int k = 1; k <= H; ++k) {
+                    const float4 xa = q[H + k], xb = q[H - k];
+                    const float4 ya = ld_f4(s + (ty + H + k) * SPITCH + col);
+                    const float4 yb = ld_f4(s + (ty + H - k) * SPITCH + col);
+                    const f32x2 t0 = add2(add2(add2(pk2(xa.x, xa.y), pk2(xb.x, xb.y)), add2(pk2(ya.x, ya.y), pk2(yb.x, yb.y))),
+                                          add2(pk2(zr[ZH + k], zr[ZH + k + 1]), pk2(zr[ZH - k], zr[ZH - k + 1])));
+                    const f32x2 t1 = add2(add2(add2(pk2(xa.z, xa.w), pk2(xb.z, xb.w)), add2(pk2(ya.z, ya.w), pk2(yb.z, yb.w))),
+                                          add2(pk2(zr[ZH + 2 + k], zr[ZH + 3 + k]), pk2(zr[ZH + 2 - k], zr[ZH + 3 - k])));
+                    l0 = fma2(t0, cpk[k], l0);
+                    l1 = fma2(t1, cpk[k], l1);
+                }
+                upk2(l0, lap[0], lap[1]);
+                upk2(l1, lap[2], lap[3]);
+            } else {
+                const float cc = coef.cx[H] + coef.cy[H] + coef.cz[H];
+                const float4 qc = q[H];
+#pragma unroll
+                for (int e = 0; e < kVZ; ++e) lap[e] = get(qc, e) * cc;
+#pragma unroll
+                for (int io = 0; io < NQ; ++io) {
+                    if (io == H) continue;
+                    const float4 qx = q[io];
+                    const float4 ry = ld_f4(s + (ty + io) * SPITCH + col);
+#pragma unroll
+                    for (int e = 0; e < kVZ; ++e) {
+                        lap[e] = fmaf(get(qx, e), coef.cx[io], lap[e]);
+                        lap[e] = fmaf(get(ry, e), coef.cy[io], lap[e]);
+                        lap[e] = fmaf(zr[ZH - H + e + io], coef.cz[io], lap[e]);
+                    }
+                }
+            }
+        }
+        release(&pempty[s_mid]);
+        // core tiles of plane x
+        if (!__all_sync(0xffffffffu, mbar_wait(&cfull[s_core], ph_core))) {
+            bad_wait = true;
+            if (CB) continue;
+            goto drain;
+        }
+        const unsigned char *ct = cring + s_core * CSLOT;
+        const float4 pp_raw = ld_f4(reinterpret_cast<const float *>(ct + (RCV ? S::OFF_PPR : 0)) + ccol);
+        const float4 vv = ld_f4(reinterpret_cast<const float *>(ct + S::OFF_V) + ccol);
+        float4 im4 = pp_raw;
+        if (RCV) im4 = ld_f4(reinterpret_cast<const float *>(ct + S::OFF_IMG) + ccol);
+        release(&cempty[s_core]);
+        // the exchange slot of plane x: the source warps fill it, the receiver warps read it
+        if (!__all_sync(0xffffffffu, mbar_wait(RCV ? &xfull[s_x] : &xempty[s_x], RCV ? ph_x : (ph_x ^ 1)))) {
+            bad_wait = true;
+            if (CB) continue;
+            goto drain;
+        }
+        float4 ps4 = pp_raw;
+        if (RCV) ps4 = ld_f4(xring + s_x * CORE + ccol);
+        if (RCV) release(&xempty[s_x]);
+        float4 out = pp_raw;
+        if (row_ok) {
+            const float4 qc = q[H];
+            float ppv[kVZ] = {pp_raw.x, pp_raw.y, pp_raw.z, pp_raw.w};
+            if (TP == kTaperUpper && pp_taper_yz) {
+#pragma unroll
+                for (int e = 0; e < kVZ; ++e) {
+                    if (!((vmask >> e) & 1u)) continue;
+                    const int z = z0 + e;
+                    ppv[e] = taper_once(taper_once(ppv[e], x, y, z, a), x, y, z, a);
+                }
+            }
+            float npp[kVZ];
+#pragma unroll
+            for (int e = 0; e < kVZ; ++e) {
+                if (EXACT) {
+                    const float two_p = 2.f * get(qc, e);
+                    const float d = two_p - ppv[e];
+                    const float vl = get(vv, e) * lap[e];
+                    npp[e] = d + vl;
+                } else {
+                    npp[e] = fmaf(get(vv, e), lap[e], 2.f * get(qc, e) - ppv[e]);
+                }
+            }
+            if (special) {
+#pragma unroll
+                for (int e = 0; e < kVZ; ++e) {
+                    const int z = z0 + e;
+                    if (RCV && e == rec_e && rec_p) {
+                        if (a.rec_mode == kRecOverwrite) npp[e] = rec_v;
+                        else npp[e] = npp[e] + rec_v;
+                    }
+                    if (!RCV && ((umask >> e) & 1u) && a.upb_mode == kUpbRestore)
+                        npp[e] = a.upb[((size_t)x * a.nye + y) * H + (z - (a.blen - H))];
+                }
+            }
+#pragma unroll
+            for (int e = 0; e < kVZ; ++e) {
+                const float o = ((vmask >> e) & 1u) ? npp[e] : get(pp_raw, e);
+                put(out, e, o);
+                nanacc = fmaf(0.f, o, nanacc);
+            }
+            *reinterpret_cast<float4 *>(PPp + (size_t)x * plane) = out;
+            if (RCV && imask) {
+                float4 im;
+#pragma unroll
+                for (int e = 0; e < kVZ; ++e) {
+                    const float acc = get(im4, e) + get(ps4, e) * get(out, e);
+                    put(im, e, ((imask >> e) & 1u) ? acc : get(im4, e));
+                }
+                *reinterpret_cast<float4 *>(a.img + row_off + (size_t)x * plane) = im;
+            }
+        }
+        if (!RCV) {
+            // S_new of this plane for the receiver warps (cells outside the computed region carry
+            // S_prev, which the image never reads)
+            *reinterpret_cast<float4 *>(xring + s_x * CORE + ccol) = out;
+            release(&xfull[s_x]);
+        }
+    }
+    if (nanacc != nanacc && a.err) atomicOr(a.err, 1u);
+    if (bad_wait && a.err) atomicOr(a.err, 2u);
+    return;
+drain:
+    if (a.err) atomicOr(a.err, 2u);
+}
+
+template <int H, bool EXACT, int TAPER>
+__global__ void __launch_bounds__(kDualThreads, 2)
+    dual_step_kernel(const __grid_constant__ DualMaps maps, const __grid_constant__ DualArgs d) {
+    using S = DualShape<H>;
+    constexpr int ZH = S::ZH, STAGE = S::STAGE, STRIDE = S::STRIDE, D = S::D, R = S::R, E = S::E, CSLOT = S::CSLOT;
+    extern __shared__ __align__(128) unsigned char smem[];
+    float *ring_s = reinterpret_cast<float *>(smem);
+    float *ring_r = ring_s + D * STRIDE;
+    unsigned char *cring = smem + 2 * S::RING_BYTES;
+    float *xring = reinterpret_cast<float *>(smem + S::XOFF);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + S::BOFF);
+    uint64_t *pfull_s = bars, *pfull_r = pfull_s + D, *pempty_s = pfull_r + D, *pempty_r = pempty_s + D;
+    uint64_t *cfull = pempty_r + D, *cempty = cfull + R, *xfull = cempty + R, *xempty = xfull + E;
+    const StepArgs &a = d.r;  // geometry (both wavefields share it)
+
+    const int tid = threadIdx.x;
+    const int zt0 = blockIdx.x * kTZ;
+    const int yt0 = H + blockIdx.y * kDTY;
+    const int xc0 = H + blockIdx.z * a.chunk;
+    const int xc1 = min(xc0 + a.chunk, a.nxe - H);
+    if (xc0 >= xc1) return;
+    const int n = xc1 - xc0;
+    const int nplanes = n + 2 * H;
+    if (tid == 0) {
+        for (int s = 0; s < D; ++s) {
+            mbar_init(&pfull_s[s], 1); mbar_init(&pfull_r[s], 1);
+            mbar_init(&pempty_s[s], kGThreads / 32); mbar_init(&pempty_r[s], kGThreads / 32);
+        }
+        for (int s = 0; s < R; ++s) { mbar_init(&cfull[s], 1); mbar_init(&cempty[s], 2 * kGThreads / 32); }
+        for (int s = 0; s < E; ++s) { mbar_init(&xfull[s], kGThreads / 32); mbar_init(&xempty[s], kGThreads / 32); }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    if (tid >= 2 * kGThreads) {
+        // producer: S and R planes k, then the core tiles of output plane k - 2H
+        if (tid != 2 * kGThreads) return;
+        bool ok = true;
+        int p_issued = 0, c_issued = 0;
+        for (int k = 0; k < nplanes && ok; ++k) {
+            const int s = k % D;
+            if (k >= D && (!(ok = mbar_wait(&pempty_s[s], ((k / D) + 1) & 1)) ||
+                           !(ok = mbar_wait(&pempty_r[s], ((k / D) + 1) & 1))))
+                break;
+            mbar_expect_tx(&pfull_s[s], STAGE * 4);
+            tma_load_3d(ring_s + s * STRIDE, &maps.ps, &pfull_s[s], zt0 - ZH, yt0 - H, xc0 - H + k);
+            mbar_expect_tx(&pfull_r[s], STAGE * 4);
+            tma_load_3d(ring_r + s * STRIDE, &maps.pr, &pfull_r[s], zt0 - ZH, yt0 - H, xc0 - H + k);
+            p_issued = k + 1;
+            if (k >= 2 * H) {
+                const int i = k - 2 * H, cs = i % R;
+                if (i >= R && !(ok = mbar_wait(&cempty[cs], ((i / R) + 1) & 1))) break;
+                unsigned char *dst = cring + cs * CSLOT;
+                mbar_expect_tx(&cfull[cs], CSLOT);
+                tma_load_3d(dst, &maps.pps, &cfull[cs], zt0, yt0, xc0 + i);
+                tma_load_3d(dst + S::OFF_PPR, &maps.ppr, &cfull[cs], zt0, yt0, xc0 + i);
+                tma_load_3d(dst + S::OFF_V, &maps.v, &cfull[cs], zt0, yt0, xc0 + i);
+                tma_load_3d(dst + S::OFF_IMG, &maps.img, &cfull[cs], zt0, yt0, xc0 + i);
+                c_issued = i + 1;
+            }
+        }
+        if (!ok && a.err) atomicOr(a.err, 2u);
+        // stay until every copy this CTA issued has landed (bounded), so none outlives the CTA
+        for (int k = p_issued > D ? p_issued - D : 0; k < p_issued; ++k) {
+            if (!mbar_wait(&pfull_s[k % D], (k / D) & 1)) break;
+            if (!mbar_wait(&pfull_r[k % D], (k / D) & 1)) break;
+        }
+        for (int i = c_issued > R ? c_issued - R : 0; i < c_issued; ++i)
+            if (!mbar_wait(&cfull[i % R], (i / R) & 1)) break;
+        return;
+    }
+    if (tid < kGThreads)
+        dual_consumer<H, EXACT, TAPER, 0>(d.s, d.r, ring_s, cring, xring, pfull_s, pempty_s, cfull, cempty, xfull,
+                                          xempty, tid, zt0, yt0, xc0, n);
+    else
+        dual_consumer<H, EXACT, TAPER, 1>(d.r, d.r, ring_r, cring, xring, pfull_r, pempty_r, cfull, cempty, xfull,
+                                          xempty, tid - kGThreads, zt0, yt0, xc0, n);
+}
+
+template <int H>
+cudaError_t launch_dual_h(const DualMaps &maps, const DualArgs &d, bool exact, int taper, dim3 grid, cudaStream_t s) {
+    static unsigned long long attr_done[4] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int variant = (exact ? 2 : 0) + (taper == kTaperUpper ? 1 : 0);
+    auto run = [&](void (*kern)(DualMaps, DualArgs)) -> cudaError_t {
+        const unsigned long long bit = 1ull << (dev & 63);
+        if (!(attr_done[variant] & bit)) {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DualShape<H>::SMEM);
+            if (e != cudaSuccess) return e;
+            attr_done[variant] |= bit;
+        }
+        kern<<<grid, kDualThreads, DualShape<H>::SMEM, s>>>(maps, d);
+        return cudaGetLastError();
+    };
+    if (taper != kTaperNone && taper != kTaperUpper) return cudaErrorInvalidValue;
+    if (exact) return taper ? run(dual_step_kernel<H, true, kTaperUpper>) : run(dual_step_kernel<H, true, kTaperNone>);
+    return taper ? run(dual_step_kernel<H, false, kTaperUpper>) : run(dual_step_kernel<H, false, kTaperNone>);
+}
+
+}  // namespace detail
+}  // namespace rtmb

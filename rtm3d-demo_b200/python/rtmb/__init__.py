@@ -26,6 +26,7 @@ FLAG_NO_TMA = 0x20
 FLAG_STORE_F16 = 0x40
 FLAG_STORE_BF16 = 0x80
 FLAG_IMG_F64 = 0x100
+FLAG_NO_DUAL = 0x200
 BC_ABC, BC_HBC, BC_RBC, BC_LEARNED = 1, 2, 3, 4
 CLOSURE_NPARAM, CLOSURE_NIN = 3169, 64
 
@@ -202,15 +203,15 @@ class Context:
     def launches(self) -> int:
         return int(self.L.rtmb_launch_count(self.h))
 
-    PROF_NAMES = ("model", "forward", "backward_source", "backward_receiver", "other")
+    PROF_NAMES = ("model", "forward", "backward_source", "backward_receiver", "other", "backward_dual")
 
     def profile(self, enable: bool = True) -> None:
         """Time every driver launch with CUDA events (per category); enabling clears the totals."""
         self._check(self.L.rtmb_profile(self.h, int(enable)))
 
     def profile_read(self) -> dict:
-        ms = (C.c_double * 5)()
-        n = (C.c_uint64 * 5)()
+        ms = (C.c_double * len(self.PROF_NAMES))()
+        n = (C.c_uint64 * len(self.PROF_NAMES))()
         self._check(self.L.rtmb_profile_read(self.h, ms, n))
         return {name: {"ms": ms[k], "launches": int(n[k])} for k, name in enumerate(self.PROF_NAMES)}
 

@@ -135,20 +135,35 @@ def train_closure(case, cuda, shots, wide):
         got = ctx.closure_collect(*shot, t0, tstride, per_step, 100 + k, min_scale, X[n:], R[n:])
         n += got
     assert n > 100000, n
-    p = to_dev(rtmb.closure_init(17), cuda)
-    losses = rtmb.closure_train(p, X, R, n, 3000, 8192, 2e-3, 23, noise=0.05)
-    return p, losses, n, min_scale
+    return X, R, n, min_scale
+
+
+def train_and_select(case, cuda, X, R, n, min_scale, wide, val_shot, seeds=(24, 26)):
+    """Trains one candidate per seed (8000 Adam steps) and keeps the one that reflects least on a
+    validation shot, which is not the shot the test evaluates."""
+    ref, _ = run_model(case, wide, "taper", val_shot, cuda)
+    best = None
+    for seed in seeds:
+        p = to_dev(rtmb.closure_init(17), cuda)
+        losses = rtmb.closure_train(p, X, R, n, 8000, 8192, 2e-3, seed, noise=0.05)
+        rec, _ = run_model(case, 8, "learned", val_shot, cuda, closure=p, min_scale=min_scale, damp=0.3)
+        e = rel_l2(rec, ref)
+        if best is None or e < best[0]:
+            best = (e, p, losses)
+    return best[1], best[2]
 
 
 def test_learned_closure_beats_the_plain_8_cell_border(cuda):
-    """Trained on four source positions, evaluated on a held-out one: the learned 8-cell closure
-    reflects less than the reference's taper with the same 8-cell border (the method without the
-    network), and its reflected energy is reported beside the 32-cell taper's."""
+    """Trained on four source positions (two candidates, the one that reflects least on a validation
+    shot kept), evaluated on a held-out shot: the learned 8-cell closure reflects less than the
+    reference's taper with the same 8-cell border (the method without the network), and its
+    reflected energy is reported beside the 32-cell taper's."""
     case = CASE
     wide = 72  # reflections from this border do not return within nt
     train_shots = [(12, 14, 4), (28, 25, 6), (20, 8, 3), (9, 30, 10)]
-    held_out = (22, 19, 5)
-    params, losses, nrows, min_scale = train_closure(case, cuda, train_shots, wide)
+    val_shot, held_out = (15, 26, 7), (22, 19, 5)
+    X, R, nrows, min_scale = train_closure(case, cuda, train_shots, wide)
+    params, losses = train_and_select(case, cuda, X, R, nrows, min_scale, wide, val_shot)
     assert losses[-50:].mean() < losses[:10].mean() / 3, (losses[:10], losses[-50:])
     ref, _ = run_model(case, wide, "taper", held_out, cuda)
     learned, _ = run_model(case, 8, "learned", held_out, cuda, closure=params, min_scale=min_scale, damp=0.3)

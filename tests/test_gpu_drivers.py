@@ -190,3 +190,28 @@ def test_autotune_picks_a_chunk_and_keeps_results(cuda, oracle):
     ctx.model_shot(case["sx"], case["sy"], case["sz"], rec1)
     ctx.sync()
     assert bitexact(host(rec0), host(rec1))
+
+
+@pytest.mark.parametrize("bc", ["hbc", "rbc"])
+def test_dual_backward_step_matches_two_launches(cuda, oracle, bc):
+    """In the FMA form the backward source and receiver steps run as one dual-wavefield launch by
+    default; it gives the two-launch result (RTMB_FLAG_NO_DUAL) bit for bit, for both boundaries.
+    The exact form keeps two launches."""
+    import torch
+    case = CASES["mid"]
+    p = oracle_params(case)
+    rec, _ = oracle.model_shot(p, oracle.v2dt2(oracle.extend_init_borders(layered_model(case), case["blen"], "abc"),
+                                               case["dt"]))
+    v2 = oracle.v2dt2(oracle.extend_init_borders(layered_model(case), case["blen"], bc, seed=7), case["dt"])
+    out = {}
+    for flags in (rtmb.FLAG_FAST_FMA, rtmb.FLAG_FAST_FMA | rtmb.FLAG_NO_DUAL, 0):
+        ctx = ctx_for(case, bc, flags)
+        ctx.load_v2dt2(v2, from_host=True)
+        img = torch.zeros(ctx.padded_shape, dtype=torch.float32, device=cuda)
+        ctx.profile(True)
+        ctx.migrate_shot(case["sx"], case["sy"], case["sz"], dev(rec, cuda), img)
+        ctx.sync()
+        out[flags] = (host(img), ctx.profile_read()["backward_dual"]["launches"])
+    fma, two, exact = out[rtmb.FLAG_FAST_FMA], out[rtmb.FLAG_FAST_FMA | rtmb.FLAG_NO_DUAL], out[0]
+    assert fma[1] == case["nt"] - 2 and two[1] == 0 and exact[1] == 0
+    assert bitexact(fma[0], two[0])
