@@ -38,6 +38,23 @@ __device__ __forceinline__ float taper_once(float v, int x, int y, int z, const 
     return v * face_factor(a.taper, b, a.nxe, x);
 }
 
+// The taper factor of index i on an axis of n cells (1.0f off the border) and whether i is in the
+// border.  Multiplying by 1.0f is exact, so taper_by_factors below reproduces taper_once.
+__device__ __forceinline__ float taper_factor(const float *t, int b, int n, int i, bool &in) {
+    in = i < b || i >= n - b;
+    return !in ? 1.f : (i < b ? __ldg(t + (b - 1 - i)) : __ldg(t + (i - (n - b))));
+}
+
+// taper_once for a cell whose per-axis factors and border flags are known: the reference's multiply
+// order is y, x, z everywhere except on the x-y edges (x, then y); the upper form tapers only z < blen.
+template <int TAPER>
+__device__ __forceinline__ float taper_by_factors(float v, float fx, float fy, float fz, bool xb, bool yb,
+                                                  bool zb) {
+    if (TAPER == kTaperUpper) return zb ? ((v * fy) * fx) * fz : v;
+    if (xb && yb && !zb) return (v * fx) * fy;
+    return ((v * fy) * fx) * fz;
+}
+
 __device__ __forceinline__ bool quirk_cell(int x, int y, int z, const StepArgs &a) {
     return a.quirk && a.taper_mode == kTaperAll && x < a.blen && y >= a.nye - a.blen &&
            z >= a.blen && z < a.nze - a.blen;

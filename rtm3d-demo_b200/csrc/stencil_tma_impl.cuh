@@ -361,21 +361,36 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
         else need = tile_taper_yz;
         if (!need) return;  // uniform across the CTA
         T *st = pring + slot * STRIDE;
-        for (int c = tid; c < STAGE; c += kThreads) {
-            const int r = c / SPITCH, cc = c % SPITCH;
-            const int yy = yt0 - H + r, zz = zt0 - ZH + cc;
-            if (yy >= a.nye || zz < 0 || zz >= a.nze) continue;
-            float v = ST::to_f(st[c]);
-            if (TAPER == kTaperAll && quirk_cell(x, yy, zz, a)) {
-                const float tyy = face_factor(a.taper, a.blen, a.nye, yy);
-                v = ST::to_f(Pg[(size_t)a.blen * plane + (size_t)yy * a.nze + zz]);
-                v = v * tyy;
-                v = v * face_factor(a.taper, a.blen, a.nxe, x);
-                v = v * tyy;
-            } else {
-                v = taper_once(v, x, yy, zz, a);
+        bool xb;
+        const float fx = taper_factor(a.taper, a.blen, a.nxe, x, xb);
+        constexpr int U = SPITCH / 4;  // four cells per unit
+        for (int w = tid; w < S::SROWS * U; w += kThreads) {
+            const int r = w / U, u = w - r * U;
+            const int yy = yt0 - H + r;
+            if (yy >= a.nye) continue;
+            bool yb;
+            const float fy = taper_factor(a.taper, a.blen, a.nye, yy, yb);
+            T *p4 = st + r * SPITCH + 4 * u;
+            float4 v4 = ST::ld4(p4);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int zz = zt0 - ZH + 4 * u + e;
+                if (zz < 0 || zz >= a.nze) continue;
+                bool zb;
+                const float fz = taper_factor(a.taper, a.blen, a.nze, zz, zb);
+                if (TAPER == kTaperUpper) zb = zz < a.blen;
+                float v = get(v4, e);
+                if (TAPER == kTaperAll && quirk_cell(x, yy, zz, a)) {
+                    v = ST::to_f(Pg[(size_t)a.blen * plane + (size_t)yy * a.nze + zz]);
+                    v = v * fy;
+                    v = v * fx;
+                    v = v * fy;
+                } else {
+                    v = taper_by_factors<TAPER>(v, fx, fy, fz, xb, yb, zb);
+                }
+                put(v4, e, v);
             }
-            st[c] = ST::from_f(v);
+            ST::st4(p4, v4);
         }
         // the slot is refilled by TMA later: order these generic-proxy writes before that
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -535,21 +550,27 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
             if (TAPER != kTaperNone) {
                 const bool pp_taper = pp_taper_yz || (TAPER == kTaperAll && (x < a.blen || x >= a.nxe - a.blen));
                 if (pp_taper) {
+                    bool xb, yb;
+                    const float fx = taper_factor(a.taper, a.blen, a.nxe, x, xb);
+                    const float fy = taper_factor(a.taper, a.blen, a.nye, y, yb);
 #pragma unroll
                     for (int e = 0; e < kVZ; ++e) {
                         if (!((vmask >> e) & 1u)) continue;
                         const int z = z0 + e;
                         float pp = ppv[e];
                         if (TAPER == kTaperAll && quirk_cell(x, y, z, a)) {
-                            const float ty_ = face_factor(a.taper, a.blen, a.nye, y);
                             pp = a.quirk_in[(size_t)(y - (a.nye - a.blen)) * (a.nze - 2 * a.blen) + (z - a.blen)];
                             if (SC) pp = pp * sPPinv;  // the side buffer holds values, not stored units
-                            pp = pp * ty_;
-                            pp = pp * ty_;
-                            pp = pp * face_factor(a.taper, a.blen, a.nxe, x);
-                            pp = pp * ty_;
+                            pp = pp * fy;
+                            pp = pp * fy;
+                            pp = pp * fx;
+                            pp = pp * fy;
                         } else {
-                            pp = taper_once(taper_once(pp, x, y, z, a), x, y, z, a);
+                            bool zb;
+                            const float fz = taper_factor(a.taper, a.blen, a.nze, z, zb);
+                            if (TAPER == kTaperUpper) zb = z < a.blen;
+                            pp = taper_by_factors<TAPER>(taper_by_factors<TAPER>(pp, fx, fy, fz, xb, yb, zb), fx, fy, fz,
+                                                         xb, yb, zb);
                         }
                         ppv[e] = pp;
                     }
