@@ -267,8 +267,10 @@ void set_receivers(rtmb::StepArgs &a, const rtmb_ctx *c, int mode, float *rec, i
 }  // namespace
 
 // Forward time loop shared by modeling and the migration forward pass.  Leaves the last two
-// wavefields in (*P, *PP) raw (untapered): *P = u(nt-1), *PP = u(nt).  Every buffer it uses must
-// already be set in the context except the taper side buffers, which it allocates when missing.
+// wavefields in (*P, *PP): *P = u(nt-1), *PP = u(nt), raw (untapered) except in a taper-all run
+// without a hook on the TMA kernel, which stores every level tapered (T(u), StepArgs::tw).  Every
+// buffer it uses must already be set in the context except the taper side buffers, which it
+// allocates when missing.
 int rtmb::driver::run_forward(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, int taper_mode, float *rec,
                 float *upb, float **P_out, float **PP_out, int cat, rtmb::ScaleRec **sc_out,
                 StepHook *hook) {
@@ -298,6 +300,11 @@ int rtmb::driver::run_forward(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t 
     if (st && (!(scP = new_scale(ctx)) || !(scPP = new_scale(ctx))))
         return fail(ctx, RTMB_EINVAL, "scale record pool exhausted");
     const size_t upb_step = (size_t)ctx->nxe * ctx->nye * ctx->h;
+    // taper-all runs keep the fields tapered in HBM (StepArgs::tw) when the TMA kernel runs; a hook
+    // reads the fields between steps, so it gets the raw form
+    const bool tw = taper_mode == rtmb::kTaperAll && !hook && tma_ok(ctx) && p.stencil_order <= 8 &&
+                    ctx->nze % 4 == 0 && !(p.flags & RTMB_FLAG_NO_TAPER_STORE);
+    a.tw = tw ? 1 : 0;
     for (uint32_t it = 0; it < p.nt; ++it) {
         std::swap(P, PP);
         std::swap(scP, scPP);

@@ -117,6 +117,7 @@ cudaError_t launch_step(const StepArgs &a, int order, bool exact, cudaStream_t s
         }
         if (used || e != cudaSuccess) return e;
     }
+    if (a.tw) return cudaErrorInvalidValue;  // tapered storage is a form of the TMA kernel only
     switch (h) {
     case 1: return detail::launch_h<1>(a, exact, aligned, grid, s);
     case 2: return detail::launch_h<2>(a, exact, aligned, grid, s);

@@ -55,6 +55,29 @@ __device__ __forceinline__ float taper_by_factors(float v, float fx, float fy, f
     return ((v * fy) * fx) * fz;
 }
 
+// Factor of a cell known to lie in the border of its axis (i < b or i >= n - b).
+__device__ __forceinline__ float taper_factor_in(const float *t, int b, int n, int i) {
+    return __ldg(t + (i < b ? b - 1 - i : i - (n - b)));
+}
+
+// The factors of taper_by_factors as three products in a fixed order: T(v) = ((v f1) f2) f3, with
+// ones where taper_by_factors multiplies fewer times (a product by 1 is exact).  ALL: every face
+// (kTaperAll); otherwise the upper slab (zb: z < blen).
+template <bool ALL>
+__device__ __forceinline__ void taper_factors3(float fx, float fy, float fz, bool xb, bool yb, bool zb, float &f1,
+                                               float &f2, float &f3) {
+    if (ALL) {
+        const bool sw = xb && yb && !zb;  // the x-y edge off the z borders: (v fx) fy
+        f1 = sw ? fx : fy;
+        f2 = sw ? fy : fx;
+        f3 = sw ? 1.f : fz;
+    } else {
+        f1 = zb ? fy : 1.f;
+        f2 = zb ? fx : 1.f;
+        f3 = zb ? fz : 1.f;
+    }
+}
+
 __device__ __forceinline__ bool quirk_cell(int x, int y, int z, const StepArgs &a) {
     return a.quirk && a.taper_mode == kTaperAll && x < a.blen && y >= a.nye - a.blen &&
            z >= a.blen && z < a.nze - a.blen;

@@ -105,6 +105,7 @@ struct Stor<float> {
     __device__ static float to_f(float v) { return v; }
     __device__ static float from_f(float v) { return v; }
     __device__ static void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
+    __device__ static void st1(float *p, float v) { *p = v; }
 };
 template <>
 struct Stor<__half> {
@@ -124,6 +125,7 @@ struct Stor<__half> {
         u.y = *reinterpret_cast<const uint32_t *>(&b);
         *reinterpret_cast<uint2 *>(p) = u;
     }
+    __device__ static void st1(__half *p, float v) { *p = from_f(v); }
 };
 template <>
 struct Stor<__nv_bfloat16> {
@@ -143,6 +145,7 @@ struct Stor<__nv_bfloat16> {
         u.y = *reinterpret_cast<const uint32_t *>(&b);
         *reinterpret_cast<uint2 *>(p) = u;
     }
+    __device__ static void st1(__nv_bfloat16 *p, float v) { *p = from_f(v); }
 };
 
 // 2^e as a float for -126 <= e <= 127 (exact).
@@ -197,9 +200,64 @@ struct TmaShape {
     // batched launches: one shot's StepArgs copied past the rings
     static constexpr size_t ARGS_OFF = (SMEM + 15) / 16 * 16;
     static constexpr size_t SMEM_BATCH = ARGS_OFF + sizeof(StepArgs);
+    // taper forms: the taper factors of the P tile's SROWS rows, then of its SPITCH columns, past
+    // the rings; a factor is stored negated (sign bit set) where the row / column is in a tapered
+    // border, so one load gives both
+    static constexpr size_t TAB_OFF = (SMEM + 15) / 16 * 16;
+    static constexpr size_t SMEM_TAPER = TAB_OFF + (size_t)(SROWS + SPITCH) * sizeof(float);
+    static constexpr size_t smem(int taper) { return taper == kTaperNone ? SMEM : SMEM_TAPER; }
 };
 
-// TAPER: kTaperNone / kTaperUpper / kTaperAll.  IMG: the epilogue accumulates the image.
+// Taper of one P tile in shared memory, in place and in stored units (kTaperUpper / kTaperAll):
+// plane x, rows yt0 - H .., columns zt0 - ZH ..; tab holds the tile's row and column factors
+// (TmaShape::TAB_OFF).  Every consumer thread tapers a share of the tile; the caller ends the pass
+// with a consumer barrier.
+template <int H, int TAPER, bool IMG, typename T, typename IT>
+__device__ __forceinline__ void taper_tile(T *st, const float *tab, const StepArgs &a, int x, int yt0, int zt0, int tid) {
+    using S = TmaShape<H, IMG, T, IT>;
+    using ST = Stor<T>;
+    constexpr int ZH = S::ZH, SPITCH = S::SPITCH;
+    const T *Pg = reinterpret_cast<const T *>(a.P);
+    const size_t plane = (size_t)a.nye * a.nze;
+    bool xb;
+    const float fx = taper_factor(a.taper, a.blen, a.nxe, x, xb);
+    constexpr int U = SPITCH / 4;  // four cells per unit
+    for (int w = tid; w < S::SROWS * U; w += kThreads) {
+        const int r = w / U, u = w - r * U;
+        const int yy = yt0 - H + r;
+        if (yy >= a.nye) continue;
+        const float tyv = tab[r];
+        const float fy = fabsf(tyv);
+        const bool yb = signbit(tyv);
+        const float4 tz4 = *reinterpret_cast<const float4 *>(tab + S::SROWS + 4 * u);
+        T *p4 = st + r * SPITCH + 4 * u;
+        float4 v4 = ST::ld4(p4);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int zz = zt0 - ZH + 4 * u + e;
+            if (zz < 0 || zz >= a.nze) continue;
+            const float fz = fabsf(get(tz4, e));
+            const bool zb = signbit(get(tz4, e));
+            float v = get(v4, e);
+            if (TAPER == kTaperAll && quirk_cell(x, yy, zz, a)) {
+                v = ST::to_f(Pg[(size_t)a.blen * plane + (size_t)yy * a.nze + zz]);
+                v = v * fy;
+                v = v * fx;
+                v = v * fy;
+            } else {
+                v = taper_by_factors<TAPER>(v, fx, fy, fz, xb, yb, zb);
+            }
+            put(v4, e, v);
+        }
+        ST::st4(p4, v4);
+    }
+    // the slot is refilled by TMA later: order these generic-proxy writes before that
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// TAPER: kTaperNone / kTaperUpper / kTaperAll (raw fields, tapered on load) / kTaperAllStored
+// (every face tapered, the fields stored tapered: no pass over the P tile, no consumer barrier).
+// IMG: the epilogue accumulates the image.
 // T: storage type of P, PP and ps (float: the FP32 form, bit-identical to the plain-load kernel;
 // __half / __nv_bfloat16: scaled 16-bit storage).  IT: image type (float or double).
 // The body of one CTA: the tile (bx, by) of the (z, y) plane and x chunk bz of the volume that
@@ -211,9 +269,12 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
     using S = TmaShape<H, IMG, T, IT>;
     using ST = Stor<T>;
     constexpr bool SC = ST::kScaled;
+    // ALL: every face tapered (kTaperAll, kTaperAllStored); TWS: the fields are stored tapered
+    constexpr bool ALL = TAPER == kTaperAll || TAPER == kTaperAllStored;
+    constexpr bool TWS = TAPER == kTaperAllStored;
     // CB: the consumers meet at named barriers (taper passes), so a timed-out wait must be seen by
     // all of them at the next barrier instead of one warp leaving alone
-    constexpr bool CB = TAPER != kTaperNone;
+    constexpr bool CB = TAPER == kTaperUpper || TAPER == kTaperAll;
     static_assert(!(SC && EXACT), "the 16-bit storage forms use the FMA arithmetic");
     constexpr int ZH = S::ZH, SPITCH = S::SPITCH, STAGE = S::STAGE, STRIDE = S::STRIDE, D = S::D, R = S::R;
     constexpr int CSLOT = S::CSLOT;
@@ -241,6 +302,20 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
     const int nplanes = n + 2 * H;  // P planes, local index k <-> x = xc0 - H + k
     const size_t plane = (size_t)a.nye * a.nze;
 
+    float *tab = reinterpret_cast<float *>(smem + S::TAB_OFF);  // taper forms only
+    if (TAPER != kTaperNone && tid < S::SROWS + SPITCH) {
+        const bool row = tid < S::SROWS;
+        const int i = row ? yt0 - H + tid : zt0 - ZH + (tid - S::SROWS);
+        const int n_ax = row ? a.nye : a.nze;
+        float f = 1.f;
+        if (i >= 0 && i < n_ax) {
+            bool in;
+            f = taper_factor(a.taper, a.blen, n_ax, i, in);
+            if (TAPER == kTaperUpper && !row) in = i < a.blen;
+            if (in) f = -f;
+        }
+        tab[tid] = f;
+    }
     if (tid == 0) {
         for (int s = 0; s < D; ++s) { mbar_init(&pfull[s], 1); mbar_init(&pempty[s], NCW); }
         for (int s = 0; s < R; ++s) { mbar_init(&cfull[s], 1); mbar_init(&cempty[s], NCW); }
@@ -283,7 +358,6 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
         return;
     }
     const int lane = tid & 31;
-    const T *Pg = reinterpret_cast<const T *>(a.P);
 
     // ---- scales of the 16-bit forms: the stored levels hold value * 2^-e
     float sP = 1.f, sPP = 1.f, sPS = 1.f, sOutInv = 1.f, sPPinv = 1.f, sKeep = 1.f;
@@ -327,15 +401,14 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
     const bool special = src_e >= 0 || rec_e >= 0 || umask != 0 || qmask != 0;
     const float wsrc = src_e >= 0 ? __ldg(a.wavelet + a.it) : 0.f;  // this launch's Ricker sample
     bool tile_taper_yz = false;  // does this CTA's tile touch the taper region (x border aside)?
-    if (TAPER == kTaperAll)
+    if (ALL)
         tile_taper_yz = (yt0 - H < a.blen) || (yt0 + kTY + H > a.nye - a.blen) || (zt0 - ZH < a.blen) ||
                         (zt0 + kTZ + ZH > a.nze - a.blen);
     if (TAPER == kTaperUpper) tile_taper_yz = (zt0 - ZH < a.blen);
-    bool pp_taper_yz = false;    // T o T needed on this thread's own PP values?
-    if (TAPER == kTaperAll)
+    bool pp_taper_yz = false;    // are this thread's own cells in the y or z taper region?
+    if (ALL)
         pp_taper_yz = (y < a.blen) || (y >= a.nye - a.blen) || (z0 < a.blen) || (z0 + kVZ > a.nze - a.blen);
     if (TAPER == kTaperUpper) pp_taper_yz = z0 < a.blen;
-
     const size_t row_off = (size_t)y * a.nze + z0;
     T *PPp = reinterpret_cast<T *>(a.PP) + row_off;
     const int col = ZH + tz * kVZ;
@@ -345,56 +418,24 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
     // P slot k % D holds plane k; its "full" phase for plane k has parity (k / D) & 1.  The plane
     // loop keeps these as running counters instead of dividing.
     auto wait_p = [&](int slot, int parity) {  // warp-uniform outcome, so a warp never splits at a timeout
+        // after a timeout (taper forms) the warp runs on without waiting, on undefined data, until
+        // the next consumer barrier tells every warp to stop: so no warp leaves a barrier short
+        if (CB && bad_wait) return;
         bad_wait |= !__all_sync(0xffffffffu, mbar_wait(&pfull[slot], parity));
     };
     auto release_p = [&](int slot) {  // this warp no longer reads the plane in this slot
         __syncwarp();
         if (lane == 0) mbar_arrive(&pempty[slot]);
     };
-    // taper of the tile of P plane k, in place and in stored units (TAPER forms).  The pass is
-    // collective: every consumer thread tapers a share of the tile, so it ends with the consumer
-    // barrier.
-    auto taper_stage = [&](int k, int slot) {
+    // does the tile of P plane k need a pass before the stencil reads it?  Uniform across the CTA.
+    auto plane_needs_taper = [&](int k) {
         const int x = xc0 - H + k;
-        bool need;
-        if (TAPER == kTaperAll) need = tile_taper_yz || x < a.blen || x >= a.nxe - a.blen;
-        else need = tile_taper_yz;
-        if (!need) return;  // uniform across the CTA
-        T *st = pring + slot * STRIDE;
-        bool xb;
-        const float fx = taper_factor(a.taper, a.blen, a.nxe, x, xb);
-        constexpr int U = SPITCH / 4;  // four cells per unit
-        for (int w = tid; w < S::SROWS * U; w += kThreads) {
-            const int r = w / U, u = w - r * U;
-            const int yy = yt0 - H + r;
-            if (yy >= a.nye) continue;
-            bool yb;
-            const float fy = taper_factor(a.taper, a.blen, a.nye, yy, yb);
-            T *p4 = st + r * SPITCH + 4 * u;
-            float4 v4 = ST::ld4(p4);
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int zz = zt0 - ZH + 4 * u + e;
-                if (zz < 0 || zz >= a.nze) continue;
-                bool zb;
-                const float fz = taper_factor(a.taper, a.blen, a.nze, zz, zb);
-                if (TAPER == kTaperUpper) zb = zz < a.blen;
-                float v = get(v4, e);
-                if (TAPER == kTaperAll && quirk_cell(x, yy, zz, a)) {
-                    v = ST::to_f(Pg[(size_t)a.blen * plane + (size_t)yy * a.nze + zz]);
-                    v = v * fy;
-                    v = v * fx;
-                    v = v * fy;
-                } else {
-                    v = taper_by_factors<TAPER>(v, fx, fy, fz, xb, yb, zb);
-                }
-                put(v4, e, v);
-            }
-            ST::st4(p4, v4);
-        }
-        // the slot is refilled by TMA later: order these generic-proxy writes before that
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        consumer_sync();
+        if (TAPER == kTaperAll) return tile_taper_yz || x < a.blen || x >= a.nxe - a.blen;
+        return tile_taper_yz;
+    };
+    // taper of the tile of P plane k (kTaperUpper / kTaperAll)
+    auto taper_stage = [&](int k, int slot) {
+        taper_tile<H, TAPER, IMG, T, IT>(pring + slot * STRIDE, tab, a, xc0 - H + k, yt0, zt0, tid);
     };
 
     float4 q[NQ];
@@ -414,7 +455,7 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
     // warm-up: P planes 0 .. 2H-1 into the queue; planes 0 .. H-1 are not computed here
     for (int k = 0; k < 2 * H; ++k) {  // 2H <= D: slots 0 .. 2H-1, first phase
         wait_p(k, 0);
-        if (TAPER != kTaperNone) taper_stage(k, k);
+        if (CB && plane_needs_taper(k)) taper_stage(k, k);
     }
     if (CB ? consumer_sync_or(bad_wait) : bad_wait) goto drain;
 #pragma unroll
@@ -428,22 +469,24 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
         {
             const int x = xc0 + i;
             const int kin = i + 2 * H;
-            // the record value the receiver step injects: loaded now so that its latency (a strided
-            // gather) overlaps the stencil instead of stalling the warp at the end of the plane
-            const float *rec_p = nullptr;
+            // the record value the receiver step injects (image forms): loaded now so that its
+            // latency (a strided gather) overlaps the stencil instead of stalling the warp at the end
+            // of the plane.  Only the flag and the value stay live across the stencil.
+            bool rec_here = false;
             float rec_v = 0.f;
-            if (special) {
+            if (special && rec_e >= 0) {
                 const int dxr = x - a.rx0;
-                if (rec_e >= 0 && dxr >= 0 && dxr % a.rdx == 0 && dxr / a.rdx < a.rcx) {
-                    rec_p = a.rec + a.rec_base + (dxr / a.rdx) * a.rec_si + rec_j * a.rec_sj;
-                    if (IMG && a.rec_mode != kRecSample) rec_v = __ldg(rec_p);  // read-only in this launch
-                }
+                rec_here = dxr >= 0 && dxr % a.rdx == 0 && dxr / a.rdx < a.rcx;
+                if (IMG && rec_here && a.rec_mode != kRecSample)  // read-only in this launch
+                    rec_v = __ldg(a.rec + a.rec_base + (dxr / a.rdx) * a.rec_si + rec_j * a.rec_sj);
             }
             wait_p(s_in, ph_in);
             const T *s = pring + s_mid * STRIDE;  // the centre plane's tile
             if constexpr (CB) {
-                if (consumer_sync_or(bad_wait)) goto drain;  // the taper pass is collective
-                taper_stage(kin, s_in);
+                if (plane_needs_taper(kin)) {  // the pass is collective: all warps take this branch
+                    taper_stage(kin, s_in);
+                    if (consumer_sync_or(bad_wait)) goto drain;
+                }
             } else if (bad_wait) {
                 goto drain;  // a timed-out wait leaves the data undefined; stop without computing
             }
@@ -519,6 +562,7 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
             release_p(s_mid);  // the tile of plane x is no longer read
             // core tiles of plane x
             const int cs = s_core;
+            if (CB && bad_wait) continue;  // run on to the next barrier (see wait_p)
             if (!__all_sync(0xffffffffu, mbar_wait(&cfull[cs], ph_core))) {
                 bad_wait = true;
                 if (CB) continue;  // the other warps learn of it at the next barrier
@@ -547,33 +591,41 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
 
             const float4 qc = q[H];
             float ppv[kVZ] = {pp_raw.x, pp_raw.y, pp_raw.z, pp_raw.w};  // stored units
+            // the taper of this thread's cells of plane x: T(v) = ((v f1) f2) f3 (the factor order of
+            // taper_by_factors; a factor of 1 is exact).  PP holds T(u) (TWS: one more T) or the raw
+            // u (T o T); the factors are re-derived where they are needed, not kept live.
+            bool tap = false, xb = false;
             if (TAPER != kTaperNone) {
-                const bool pp_taper = pp_taper_yz || (TAPER == kTaperAll && (x < a.blen || x >= a.nxe - a.blen));
-                if (pp_taper) {
-                    bool xb, yb;
-                    const float fx = taper_factor(a.taper, a.blen, a.nxe, x, xb);
-                    const float fy = taper_factor(a.taper, a.blen, a.nye, y, yb);
+                xb = x < a.blen || x >= a.nxe - a.blen;  // uniform over the CTA
+                tap = pp_taper_yz || (ALL && xb);
+            }
+            if (TAPER != kTaperNone && tap) {
+                const float fx = xb ? taper_factor_in(a.taper, a.blen, a.nxe, x) : 1.f;
+                const float tyv = tab[H + ty];  // this thread's row
+                const float fy = fabsf(tyv);
+                const bool yb = signbit(tyv);
+                const float4 tz4 = *reinterpret_cast<const float4 *>(tab + S::SROWS + ZH + tz * kVZ);
+                const bool qx = ALL && a.quirk && x < a.blen && y >= a.nye - a.blen;
 #pragma unroll
-                    for (int e = 0; e < kVZ; ++e) {
-                        if (!((vmask >> e) & 1u)) continue;
-                        const int z = z0 + e;
-                        float pp = ppv[e];
-                        if (TAPER == kTaperAll && quirk_cell(x, y, z, a)) {
-                            pp = a.quirk_in[(size_t)(y - (a.nye - a.blen)) * (a.nze - 2 * a.blen) + (z - a.blen)];
-                            if (SC) pp = pp * sPPinv;  // the side buffer holds values, not stored units
-                            pp = pp * fy;
-                            pp = pp * fy;
-                            pp = pp * fx;
-                            pp = pp * fy;
-                        } else {
-                            bool zb;
-                            const float fz = taper_factor(a.taper, a.blen, a.nze, z, zb);
-                            if (TAPER == kTaperUpper) zb = z < a.blen;
-                            pp = taper_by_factors<TAPER>(taper_by_factors<TAPER>(pp, fx, fy, fz, xb, yb, zb), fx, fy, fz,
-                                                         xb, yb, zb);
-                        }
-                        ppv[e] = pp;
+                for (int e = 0; e < kVZ; ++e) {
+                    if (!((vmask >> e) & 1u)) continue;
+                    const int z = z0 + e;
+                    float pp = ppv[e];
+                    if (qx && z >= a.blen && z < a.nze - a.blen) {
+                        // the x = blen redirect, twice: from the raw u(blen, y, z) of PP's level
+                        pp = a.quirk_in[(size_t)(y - (a.nye - a.blen)) * (a.nze - 2 * a.blen) + (z - a.blen)];
+                        if (SC) pp = pp * sPPinv;  // the side buffer holds values, not stored units
+                        pp = pp * fy;
+                        pp = pp * fy;
+                        pp = pp * fx;
+                        pp = pp * fy;
+                    } else {
+                        float f1, f2, f3;
+                        taper_factors3<ALL>(fx, fy, fabsf(get(tz4, e)), xb, yb, signbit(get(tz4, e)), f1, f2, f3);
+                        pp = ((pp * f1) * f2) * f3;
+                        if (!TWS) pp = ((pp * f1) * f2) * f3;
                     }
+                    ppv[e] = pp;
                 }
             }
             float npp[kVZ];
@@ -595,9 +647,10 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                 for (int e = 0; e < kVZ; ++e) {
                     const int z = z0 + e;
                     if (e == src_e && x == a.sxe) npp[e] = npp[e] + wsrc;
-                    if (e == rec_e && rec_p) {
+                    if (e == rec_e && rec_here) {
+                        float *rec_p = a.rec + a.rec_base + ((x - a.rx0) / a.rdx) * a.rec_si + rec_j * a.rec_sj;
                         const float rv = IMG ? rec_v : *rec_p;
-                        if (a.rec_mode == kRecSample) *const_cast<float *>(rec_p) = npp[e];
+                        if (a.rec_mode == kRecSample) *rec_p = npp[e];
                         else if (a.rec_mode == kRecOverwrite) npp[e] = rv;
                         else npp[e] = npp[e] + rv;
                     }
@@ -608,6 +661,42 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                     }
                     if (((qmask >> e) & 1u) && x == a.blen)
                         a.quirk_out[(size_t)(y - (a.nye - a.blen)) * (a.nze - 2 * a.blen) + (z - a.blen)] = npp[e];
+                }
+                if (TWS && qmask && x == a.blen) {
+                    // stored tapered, the quirk cells (x' < blen) of the new level hold
+                    // ((u(blen, y, z) fy) fx') fy: written here, where u(blen, y, z) is known, and
+                    // skipped by the CTAs that compute plane x'
+                    const float fy = fabsf(tab[H + ty]);
+                    T *qp = PPp;
+                    for (int xq = 0; xq < a.blen; ++xq, qp += plane) {
+                        const float fxq = __ldg(a.taper + (a.blen - 1 - xq));
+                        float4 o4;
+#pragma unroll
+                        for (int e = 0; e < kVZ; ++e) {
+                            float v = ((npp[e] * fy) * fxq) * fy;
+                            if (SC) v = v * sOutInv;
+                            put(o4, e, v);
+                        }
+                        if (qmask == 0xFu) {
+                            ST::st4(qp, o4);
+                        } else {
+#pragma unroll
+                            for (int e = 0; e < kVZ; ++e)
+                                if ((qmask >> e) & 1u) ST::st1(qp + e, get(o4, e));
+                        }
+                    }
+                }
+            }
+            if (TWS && tap) {  // store T(u_new): the receivers and the side buffer saw u_new
+                const float fx = xb ? taper_factor_in(a.taper, a.blen, a.nxe, x) : 1.f;
+                const float tyv = tab[H + ty];
+                const float4 tz4 = *reinterpret_cast<const float4 *>(tab + S::SROWS + ZH + tz * kVZ);
+#pragma unroll
+                for (int e = 0; e < kVZ; ++e) {
+                    float f1, f2, f3;
+                    taper_factors3<true>(fx, fabsf(tyv), fabsf(get(tz4, e)), xb, signbit(tyv), signbit(get(tz4, e)), f1,
+                                         f2, f3);
+                    npp[e] = ((npp[e] * f1) * f2) * f3;
                 }
             }
             float4 out;
@@ -625,7 +714,13 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                 }
                 put(out, e, o);
             }
-            ST::st4(PPp + (size_t)x * plane, out);
+            if (TWS && qmask && x < a.blen) {  // the quirk cells are written by plane blen's CTA
+#pragma unroll
+                for (int e = 0; e < kVZ; ++e)
+                    if (!((qmask >> e) & 1u)) ST::st1(PPp + (size_t)x * plane + e, get(out, e));
+            } else {
+                ST::st4(PPp + (size_t)x * plane, out);
+            }
             if (IMG && imask) {
                 IT *ig = reinterpret_cast<IT *>(a.img) + row_off + (size_t)x * plane;
                 IT res[kVZ];
@@ -704,10 +799,11 @@ template <int H>
 cudaError_t launch_tma_h(const TmaMaps &maps, const StepArgs &a, bool exact, int taper, bool img, dim3 grid,
                          cudaStream_t s) {
     // the dynamic shared-memory opt-in, once per (variant, device)
-    static unsigned long long attr_done[12] = {};
+    static unsigned long long attr_done[16] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    const int variant = (exact ? 6 : 0) + (img ? 3 : 0) + taper;
+    if (taper == kTaperAll && a.tw) taper = kTaperAllStored;
+    const int variant = (exact ? 8 : 0) + (img ? 4 : 0) + taper;
     auto run = [&](void (*kern)(TmaMaps, StepArgs), size_t smem) -> cudaError_t {
         const unsigned long long bit = 1ull << (dev & 63);
         if (!(attr_done[variant] & bit)) {
@@ -719,15 +815,17 @@ cudaError_t launch_tma_h(const TmaMaps &maps, const StepArgs &a, bool exact, int
         return cudaGetLastError();
     };
 #define RTMB_TMA_CASE(EX, TP, IM) \
-    if (exact == EX && taper == TP && img == IM) return run(tma_step_kernel<H, EX, TP, IM>, TmaShape<H, IM>::SMEM);
+    if (exact == EX && taper == TP && img == IM) return run(tma_step_kernel<H, EX, TP, IM>, TmaShape<H, IM>::smem(TP));
     RTMB_TMA_CASE(true, kTaperNone, false)
     RTMB_TMA_CASE(true, kTaperUpper, false)
     RTMB_TMA_CASE(true, kTaperAll, false)
+    RTMB_TMA_CASE(true, kTaperAllStored, false)
     RTMB_TMA_CASE(true, kTaperNone, true)
     RTMB_TMA_CASE(true, kTaperUpper, true)
     RTMB_TMA_CASE(false, kTaperNone, false)
     RTMB_TMA_CASE(false, kTaperUpper, false)
     RTMB_TMA_CASE(false, kTaperAll, false)
+    RTMB_TMA_CASE(false, kTaperAllStored, false)
     RTMB_TMA_CASE(false, kTaperNone, true)
     RTMB_TMA_CASE(false, kTaperUpper, true)
 #undef RTMB_TMA_CASE
@@ -739,10 +837,11 @@ cudaError_t launch_tma_h(const TmaMaps &maps, const StepArgs &a, bool exact, int
 template <typename T>
 cudaError_t launch_tma_store(const TmaMaps &maps, const StepArgs &a, int taper, bool img, bool img64, dim3 grid,
                              cudaStream_t s) {
-    static unsigned long long attr_done[8] = {};
+    static unsigned long long attr_done[12] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    const int variant = (img ? (img64 ? 6 : 3) : 0) + taper;
+    if (taper == kTaperAll && a.tw) taper = kTaperAllStored;
+    const int variant = (img ? (img64 ? 8 : 4) : 0) + taper;
     auto run = [&](void (*kern)(TmaMaps, StepArgs), size_t smem) -> cudaError_t {
         const unsigned long long bit = 1ull << (dev & 63);
         if (!(attr_done[variant] & bit)) {
@@ -755,10 +854,11 @@ cudaError_t launch_tma_store(const TmaMaps &maps, const StepArgs &a, int taper, 
     };
 #define RTMB_TMA_STORE_CASE(TP, IM, IT)                                                          \
     if (taper == TP && img == IM && (!IM || img64 == (sizeof(IT) == 8)))                         \
-        return run(tma_step_kernel<4, false, TP, IM, T, IT>, TmaShape<4, IM, T, IT>::SMEM);
+        return run(tma_step_kernel<4, false, TP, IM, T, IT>, TmaShape<4, IM, T, IT>::smem(TP));
     RTMB_TMA_STORE_CASE(kTaperNone, false, float)
     RTMB_TMA_STORE_CASE(kTaperUpper, false, float)
     RTMB_TMA_STORE_CASE(kTaperAll, false, float)
+    RTMB_TMA_STORE_CASE(kTaperAllStored, false, float)
     RTMB_TMA_STORE_CASE(kTaperNone, true, float)
     RTMB_TMA_STORE_CASE(kTaperUpper, true, float)
     RTMB_TMA_STORE_CASE(kTaperNone, true, double)

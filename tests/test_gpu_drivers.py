@@ -50,7 +50,7 @@ def migrate_gpu(case, v2, rec, bc, cuda, flags=0):
     return host(img), host(out)
 
 
-@pytest.mark.parametrize("flags", [0, rtmb.FLAG_NO_TMA], ids=["tma", "plain"])
+@pytest.mark.parametrize("flags", [0, rtmb.FLAG_NO_TAPER_STORE, rtmb.FLAG_NO_TMA], ids=["tma", "tma_raw", "plain"])
 @pytest.mark.parametrize("cname", ["golden", "odd", "mid"])
 def test_model_bitexact(cuda, oracle, cname, flags):
     case = CASES[cname]
@@ -60,6 +60,32 @@ def test_model_bitexact(cuda, oracle, cname, flags):
     assert rc == 0
     got = model_gpu(case, v2, cuda, flags=flags)
     assert bitexact(got, ref), rel_l2(got, ref)
+
+
+@pytest.mark.parametrize("nt", [1, 2, 3, 4, 7])
+@pytest.mark.parametrize("form", ["exact", "fma"])
+def test_tapered_storage_matches_raw_fields(cuda, oracle, form, nt):
+    """Modeling keeps the fields tapered in HBM except the last two levels: the record equals the
+    taper-on-load form's bit for bit, in both arithmetic forms, for runs shorter than, equal to
+    and longer than the raw tail.  The source sits near the front-right x-y
+    edge, whose cells take the taper's x = blen redirect."""
+    import torch
+    case = dict(CASES["golden"], nt=nt, ntstep=nt, sx=3, sy=17, sz=5)
+    ve = oracle.extend_init_borders(layered_model(case), case["blen"], "abc")
+    v2 = oracle.v2dt2(ve, case["dt"])
+    base = rtmb.FLAG_FAST_FMA if form == "fma" else 0
+    out = []
+    for flags in (base, base | rtmb.FLAG_NO_TAPER_STORE):
+        ctx = ctx_for(case, flags=flags)
+        ctx.load_v2dt2(dev(v2, cuda), from_host=False)
+        rec = torch.zeros(rec_shape(case), dtype=torch.float32, device=cuda)
+        ctx.model_shot(case["sx"], case["sy"], case["sz"], rec)
+        out.append(host(rec))
+    assert nt < 3 or np.any(out[0] != 0)
+    assert np.array_equal(out[0], out[1])
+    if form == "exact":
+        ref, rc = oracle.model_shot(oracle_params(case), v2)
+        assert rc == 0 and bitexact(out[0], ref)
 
 
 def test_model_matches_reference_golden(cuda, golden):
