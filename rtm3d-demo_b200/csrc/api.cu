@@ -252,6 +252,16 @@ int check_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz) {
     return RTMB_OK;
 }
 
+// Do all receivers lie off the tapered borders (x, y and z in [blen, n - blen))?  There the
+// taper's factors are all 1, so a level stored tapered holds the raw values.
+bool receivers_untapered(const rtmb_ctx *c) {
+    const rtmb::RcvGeom r = rgeom(c);
+    const long long b = c->p.blen;
+    if (r.rcx <= 0 || r.rcy <= 0) return true;
+    const long long xl = r.rx0 + (long long)(r.rcx - 1) * r.rdx, yl = r.ry0 + (long long)(r.rcy - 1) * r.rdy;
+    return r.rx0 >= b && xl < c->nxe - b && r.ry0 >= b && yl < c->nye - b && r.rz >= b && r.rz < c->nze - b;
+}
+
 void set_receivers(rtmb::StepArgs &a, const rtmb_ctx *c, int mode, float *rec, int it) {
     const rtmb::RcvGeom r = rgeom(c);
     a.rec_mode = mode;
@@ -300,10 +310,18 @@ int rtmb::driver::run_forward(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t 
     if (st && (!(scP = new_scale(ctx)) || !(scPP = new_scale(ctx))))
         return fail(ctx, RTMB_EINVAL, "scale record pool exhausted");
     const size_t upb_step = (size_t)ctx->nxe * ctx->nye * ctx->h;
+    // FP32 storage: the record is gathered from the stored level after each step (one small launch;
+    // the step kernel's forward forms carry no receiver code).  The 16-bit forms sample the FP32
+    // value inside the step, before it is rounded to storage.
+    const bool gather = rec && !st;
+    const rtmb::RcvGeom rg = rgeom(ctx);
+    const rtmb::Geom g = geom(ctx);
     // taper-all runs keep the fields tapered in HBM (StepArgs::tw) when the TMA kernel runs; a hook
-    // reads the fields between steps, so it gets the raw form
+    // reads the fields between steps, so it gets the raw form, and so does a gathered record with a
+    // receiver in the taper region (where the stored T(u) is not u)
     const bool tw = taper_mode == rtmb::kTaperAll && !hook && tma_ok(ctx) && p.stencil_order <= 8 &&
-                    ctx->nze % 4 == 0 && !(p.flags & RTMB_FLAG_NO_TAPER_STORE);
+                    ctx->nze % 4 == 0 && !(p.flags & RTMB_FLAG_NO_TAPER_STORE) &&
+                    (!gather || receivers_untapered(ctx));
     a.tw = tw ? 1 : 0;
     for (uint32_t it = 0; it < p.nt; ++it) {
         std::swap(P, PP);
@@ -314,12 +332,17 @@ int rtmb::driver::run_forward(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t 
             if (!(lvl = new_scale(ctx))) return fail(ctx, RTMB_EINVAL, "scale record pool exhausted");
             a.sc_p = scP; a.sc_pp = scPP; a.sc_out = lvl;
         }
-        if (rec) set_receivers(a, ctx, rtmb::kRecSample, rec, (int)it);
+        if (rec && !gather) set_receivers(a, ctx, rtmb::kRecSample, rec, (int)it);
         if (upb) { a.upb_mode = rtmb::kUpbSave; a.upb = upb + (size_t)it * upb_step; }
         if (quirk) { a.quirk_in = ctx->d_quirk[(it + 1) % 3]; a.quirk_out = ctx->d_quirk[it % 3]; }
         int rc;
         if (hook && (rc = hook->before((int)it, P, PP))) return rc;
         LAUNCH_CAT(cat, rtmb::launch_step(a, (int)p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
+        if (gather) {  // RTMCPUPlatform.cpp:133-150: record(i, j, it) = PP(rx0 + i rdx, ry0 + j rdy, rz)
+            const size_t chunk = (size_t)rg.rcx * rg.rcy * p.ntstep;
+            LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_receivers(PP, rec + (size_t)(it / p.ntstep) * chunk,
+                                                               (int)(it % p.ntstep), 1, rg, g, ctx->stream));
+        }
         if (hook && (rc = hook->after((int)it, P, PP))) return rc;
         if (st) scPP = lvl;
     }

@@ -79,6 +79,9 @@ cudaError_t tma_dispatch(const StepArgs &a, bool exact, dim3 grid, cudaStream_t 
     auto enc = tensor_map_encoder();
     if (!enc) return cudaSuccess;
     if (a.taper_mode == kTaperAll && a.img) return cudaSuccess;  // combination without a TMA form
+    // the FP32 forward forms of the TMA kernel sample no receivers (their drivers gather them from
+    // the stored level): the plain-load form does it in the step
+    if (!a.img && a.rec_mode != kRecNone) return cudaSuccess;
     detail::TmaMaps maps;
     std::memset(&maps, 0, sizeof maps);
     bool ok = encode(enc, &maps.p, a.P, a, S::SPITCH, S::SROWS) && encode(enc, &maps.pp, a.PP, a, kTZ, kTY) &&
@@ -156,7 +159,7 @@ cudaError_t launch_step_batch(const StepArgs *args, int nshots, int order, bool 
     for (int k = 0; k < nshots; ++k) {
         const StepArgs &a = args[k];
         if (a.taper_mode != kTaperNone || (a.img != nullptr) != img || a.img64 != a0.img64 || a.store != store ||
-            a.chunk <= 0)
+            a.chunk <= 0 || (!img && !st && a.rec_mode != kRecNone))
             return cudaErrorInvalidValue;
         if (a.nze % (st ? 8 : 4) != 0) return cudaErrorInvalidValue;
         const uintptr_t al = reinterpret_cast<uintptr_t>(a.P) | reinterpret_cast<uintptr_t>(a.PP) |

@@ -375,31 +375,27 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
         if (tid == 0 && bx == 0 && by == 0 && bz == 0) a.sc_out->e = eN;
     }
 
-    // ---- per-thread constants, hoisted out of the plane loop
+    // ---- per-thread constants, hoisted out of the plane loop.  The rare per-cell work (source,
+    // receivers, upper border, taper side buffer) is found per plane by CTA-uniform tests and its
+    // per-thread details are derived there, so that nothing of it stays live across the stencil.
+    // REC: receivers in the kernel (image forms inject them, 16-bit forms sample them); the FP32
+    // forward forms have none (their drivers sample the stored level with a gather kernel).
+    constexpr bool REC = IMG || SC;
     const bool row_ok = y < a.nye && z0 < a.nze;
     const bool y_ok = y < a.nye - H;
-    unsigned vmask = 0, imask = 0, umask = 0, qmask = 0;
+    unsigned vmask = 0, imask = 0;
 #pragma unroll
     for (int e = 0; e < kVZ; ++e) {
         const int z = z0 + e;
         const bool v = y_ok && z >= H && z < a.nze - H;
         if (v) vmask |= 1u << e;
         if (v && IMG && z >= a.img_z0 && z < a.img_z1) imask |= 1u << e;
-        if (v && a.upb_mode != kUpbNone && z >= a.blen - H && z < a.blen) umask |= 1u << e;
-        if (v && a.quirk_out && y >= a.nye - a.blen && z >= a.blen && z < a.nze - a.blen) qmask |= 1u << e;
     }
-    const int src_e =
-        (y == a.sye && a.sze >= z0 && a.sze < z0 + kVZ && ((vmask >> (a.sze - z0)) & 1u)) ? a.sze - z0 : -1;
-    int rec_e = -1, rec_j = 0;
-    if (a.rec_mode != kRecNone && a.rz >= z0 && a.rz < z0 + kVZ && ((vmask >> (a.rz - z0)) & 1u)) {
-        const int dyr = y - a.ry0;
-        if (dyr >= 0 && dyr % a.rdy == 0 && dyr / a.rdy < a.rcy) {
-            rec_e = a.rz - z0;
-            rec_j = dyr / a.rdy;
-        }
-    }
-    const bool special = src_e >= 0 || rec_e >= 0 || umask != 0 || qmask != 0;
-    const float wsrc = src_e >= 0 ? __ldg(a.wavelet + a.it) : 0.f;  // this launch's Ricker sample
+    // CTA-uniform: which kinds of rare work can fall in this tile
+    const bool src_cta = a.sye >= yt0 && a.sye < yt0 + kTY && a.sze >= zt0 && a.sze < zt0 + kTZ;
+    const bool rec_cta = REC && a.rec_mode != kRecNone && a.rz >= zt0 && a.rz < zt0 + kTZ;
+    const bool upb_cta = a.upb_mode != kUpbNone && zt0 < a.blen && zt0 + kTZ > a.blen - H;
+    const bool q_cta = ALL && a.quirk_out && yt0 + kTY > a.nye - a.blen;
     bool tile_taper_yz = false;  // does this CTA's tile touch the taper region (x border aside)?
     if (ALL)
         tile_taper_yz = (yt0 - H < a.blen) || (yt0 + kTY + H > a.nye - a.blen) || (zt0 - ZH < a.blen) ||
@@ -469,16 +465,20 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
         {
             const int x = xc0 + i;
             const int kin = i + 2 * H;
-            // the record value the receiver step injects (image forms): loaded now so that its
-            // latency (a strided gather) overlaps the stencil instead of stalling the warp at the end
-            // of the plane.  Only the flag and the value stay live across the stencil.
-            bool rec_here = false;
+            // receivers in this plane (REC forms): the record value the receiver step injects is
+            // loaded now so that its latency (a strided gather) overlaps the stencil instead of
+            // stalling the warp at the end of the plane
+            int rec_e = -1;
             float rec_v = 0.f;
-            if (special && rec_e >= 0) {
-                const int dxr = x - a.rx0;
-                rec_here = dxr >= 0 && dxr % a.rdx == 0 && dxr / a.rdx < a.rcx;
-                if (IMG && rec_here && a.rec_mode != kRecSample)  // read-only in this launch
-                    rec_v = __ldg(a.rec + a.rec_base + (dxr / a.rdx) * a.rec_si + rec_j * a.rec_sj);
+            const float *rec_p = nullptr;
+            if (REC && rec_cta) {
+                const int dxr = x - a.rx0, dyr = y - a.ry0, e = a.rz - z0;
+                if (dxr >= 0 && dxr % a.rdx == 0 && dxr / a.rdx < a.rcx && e >= 0 && e < kVZ && ((vmask >> e) & 1u) &&
+                    dyr >= 0 && dyr % a.rdy == 0 && dyr / a.rdy < a.rcy) {
+                    rec_e = e;
+                    rec_p = a.rec + a.rec_base + (dxr / a.rdx) * a.rec_si + (dyr / a.rdy) * a.rec_sj;
+                    if (IMG && a.rec_mode != kRecSample) rec_v = __ldg(rec_p);  // read-only in this launch
+                }
             }
             wait_p(s_in, ph_in);
             const T *s = pring + s_mid * STRIDE;  // the centre plane's tile
@@ -619,6 +619,10 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                         pp = pp * fy;
                         pp = pp * fx;
                         pp = pp * fy;
+                    } else if (ALL && !xb) {  // fx = 1: T(v) = (v fy) fz
+                        const float fz = fabsf(get(tz4, e));
+                        pp = (pp * fy) * fz;
+                        if (!TWS) pp = (pp * fy) * fz;
                     } else {
                         float f1, f2, f3;
                         taper_factors3<ALL>(fx, fy, fabsf(get(tz4, e)), xb, yb, signbit(get(tz4, e)), f1, f2, f3);
@@ -642,33 +646,39 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                     npp[e] = fmaf(get(vv, e), lap[e], 2.f * get(qc, e) - ppv[e]);
                 }
             }
-            if (special) {  // source, receivers, upper border or taper side buffer in this thread's cells
+            // source, receivers, upper border, taper side buffer: CTA-uniform tests first
+            if ((src_cta && x == a.sxe) || rec_e >= 0 || upb_cta || (q_cta && x == a.blen)) {
 #pragma unroll
                 for (int e = 0; e < kVZ; ++e) {
                     const int z = z0 + e;
-                    if (e == src_e && x == a.sxe) npp[e] = npp[e] + wsrc;
-                    if (e == rec_e && rec_here) {
-                        float *rec_p = a.rec + a.rec_base + ((x - a.rx0) / a.rdx) * a.rec_si + rec_j * a.rec_sj;
-                        const float rv = IMG ? rec_v : *rec_p;
-                        if (a.rec_mode == kRecSample) *rec_p = npp[e];
+                    const bool v = (vmask >> e) & 1u;
+                    if (x == a.sxe && y == a.sye && z == a.sze && v) npp[e] = npp[e] + __ldg(a.wavelet + a.it);
+                    if (REC && e == rec_e) {
+                        float *rp = const_cast<float *>(rec_p);
+                        const float rv = IMG ? rec_v : *rp;
+                        if (a.rec_mode == kRecSample) *rp = npp[e];
                         else if (a.rec_mode == kRecOverwrite) npp[e] = rv;
                         else npp[e] = npp[e] + rv;
                     }
-                    if ((umask >> e) & 1u) {
+                    if (upb_cta && v && z >= a.blen - H && z < a.blen) {
                         float *up = a.upb + ((size_t)x * a.nye + y) * H + (z - (a.blen - H));
                         if (a.upb_mode == kUpbSave) *up = npp[e];
                         else npp[e] = *up;
                     }
-                    if (((qmask >> e) & 1u) && x == a.blen)
+                    if (q_cta && x == a.blen && v && y >= a.nye - a.blen && z >= a.blen && z < a.nze - a.blen)
                         a.quirk_out[(size_t)(y - (a.nye - a.blen)) * (a.nze - 2 * a.blen) + (z - a.blen)] = npp[e];
                 }
-                if (TWS && qmask && x == a.blen) {
+                if (TWS && q_cta && x == a.blen && y >= a.nye - a.blen) {
                     // stored tapered, the quirk cells (x' < blen) of the new level hold
                     // ((u(blen, y, z) fy) fx') fy: written here, where u(blen, y, z) is known, and
                     // skipped by the CTAs that compute plane x'
+                    unsigned qm = 0;
+#pragma unroll
+                    for (int e = 0; e < kVZ; ++e)
+                        if (((vmask >> e) & 1u) && z0 + e >= a.blen && z0 + e < a.nze - a.blen) qm |= 1u << e;
                     const float fy = fabsf(tab[H + ty]);
                     T *qp = PPp;
-                    for (int xq = 0; xq < a.blen; ++xq, qp += plane) {
+                    for (int xq = 0; qm && xq < a.blen; ++xq, qp += plane) {
                         const float fxq = __ldg(a.taper + (a.blen - 1 - xq));
                         float4 o4;
 #pragma unroll
@@ -677,26 +687,31 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                             if (SC) v = v * sOutInv;
                             put(o4, e, v);
                         }
-                        if (qmask == 0xFu) {
+                        if (qm == 0xFu) {
                             ST::st4(qp, o4);
                         } else {
 #pragma unroll
                             for (int e = 0; e < kVZ; ++e)
-                                if ((qmask >> e) & 1u) ST::st1(qp + e, get(o4, e));
+                                if ((qm >> e) & 1u) ST::st1(qp + e, get(o4, e));
                         }
                     }
                 }
             }
             if (TWS && tap) {  // store T(u_new): the receivers and the side buffer saw u_new
-                const float fx = xb ? taper_factor_in(a.taper, a.blen, a.nxe, x) : 1.f;
                 const float tyv = tab[H + ty];
                 const float4 tz4 = *reinterpret_cast<const float4 *>(tab + S::SROWS + ZH + tz * kVZ);
+                if (!xb) {  // fx = 1: T(v) = (v fy) fz
 #pragma unroll
-                for (int e = 0; e < kVZ; ++e) {
-                    float f1, f2, f3;
-                    taper_factors3<true>(fx, fabsf(tyv), fabsf(get(tz4, e)), xb, signbit(tyv), signbit(get(tz4, e)), f1,
-                                         f2, f3);
-                    npp[e] = ((npp[e] * f1) * f2) * f3;
+                    for (int e = 0; e < kVZ; ++e) npp[e] = (npp[e] * fabsf(tyv)) * fabsf(get(tz4, e));
+                } else {
+                    const float fx = taper_factor_in(a.taper, a.blen, a.nxe, x);
+#pragma unroll
+                    for (int e = 0; e < kVZ; ++e) {
+                        float f1, f2, f3;
+                        taper_factors3<true>(fx, fabsf(tyv), fabsf(get(tz4, e)), xb, signbit(tyv), signbit(get(tz4, e)),
+                                             f1, f2, f3);
+                        npp[e] = ((npp[e] * f1) * f2) * f3;
+                    }
                 }
             }
             float4 out;
@@ -714,10 +729,13 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                 }
                 put(out, e, o);
             }
-            if (TWS && qmask && x < a.blen) {  // the quirk cells are written by plane blen's CTA
+            if (TWS && q_cta && x < a.blen && y >= a.nye - a.blen) {  // quirk cells: plane blen's CTA writes them
 #pragma unroll
-                for (int e = 0; e < kVZ; ++e)
-                    if (!((qmask >> e) & 1u)) ST::st1(PPp + (size_t)x * plane + e, get(out, e));
+                for (int e = 0; e < kVZ; ++e) {
+                    const int z = z0 + e;
+                    if (!(((vmask >> e) & 1u) && z >= a.blen && z < a.nze - a.blen))
+                        ST::st1(PPp + (size_t)x * plane + e, get(out, e));
+                }
             } else {
                 ST::st4(PPp + (size_t)x * plane, out);
             }
