@@ -81,6 +81,9 @@ class Oracle:
             ("orc_model_shot", [C.POINTER(OrcParams), _fp, _fp], C.c_int),
             ("orc_migrate_hbc", [C.POINTER(OrcParams), _fp, _fp, _fp], C.c_int),
             ("orc_migrate_rbc", [C.POINTER(OrcParams), _fp, _fp, _fp], C.c_int),
+            ("orc_fmig_nw", [C.c_int, C.c_float, C.c_float, C.c_float], C.c_int),
+            ("orc_fmig_tables", [C.c_int, C.c_float, C.c_float, C.c_float, C.c_int, _fp, _fp, _fp], None),
+            ("orc_migrate_fmig", [C.POINTER(OrcParams), _fp, _fp, C.c_float, C.c_float, C.c_int, _fp], C.c_int),
         ]:
             f = getattr(L, name)
             f.argtypes = args
@@ -154,6 +157,21 @@ class Oracle:
         img = np.zeros(v2dt2.shape, np.float32)
         fn = self.L.orc_migrate_hbc if bc == "hbc" else self.L.orc_migrate_rbc
         rc = fn(C.byref(op), fptr(v2dt2), fptr(np.ascontiguousarray(rec, np.float32)), fptr(img))
+        return img, rc
+
+    def fmig_tables(self, nt: int, dt: float, fmin: float, fmax: float):
+        nw = self.L.orc_fmig_nw(nt, dt, fmin, fmax)
+        w2 = np.zeros(max(nw, 1), np.float32)
+        kre = np.zeros((max(nw, 1), nt), np.float32)
+        kim = np.zeros((max(nw, 1), nt), np.float32)
+        self.L.orc_fmig_tables(nt, dt, fmin, fmax, nw, fptr(w2), fptr(kre), fptr(kim))
+        return w2[:nw], kre[:nw], kim[:nw]
+
+    def migrate_fmig(self, p: dict, v2dt2: np.ndarray, rec: np.ndarray, fmin: float, fmax: float, nwstep: int = 0):
+        op = OrcParams.from_dict(p)
+        img = np.zeros(v2dt2.shape, np.float32)
+        rc = self.L.orc_migrate_fmig(C.byref(op), fptr(v2dt2), fptr(np.ascontiguousarray(rec, np.float32)),
+                                     fmin, fmax, nwstep, fptr(img))
         return img, rc
 
 

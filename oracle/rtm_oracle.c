@@ -618,3 +618,112 @@ int orc_migrate_hbc(const orc_params *p, const float *v2dt2, const float *rec, f
 int orc_migrate_rbc(const orc_params *p, const float *v2dt2, const float *rec, float *img) {
     return migrate(p, v2dt2, rec, img, 0);
 }
+
+/* ---------------------------------------------------------------- frequency-domain RTM (fmig) */
+
+/* S/src/kernel/RTMFiniteDifferencesKernel_FreqDomain.cpp:133-137: df = 1 / (nt dt) and
+ * nw = (size_t)((fmax - fmin) / df), in the reference's float / double mix. */
+int orc_fmig_nw(int nt, float dt, float fmin, float fmax) {
+    const float df = (float)(1. / ((nt * 1.0) * dt));
+    const float nf = ((fmax - fmin) / df);
+    return nf > 0.f ? (int)(size_t)nf : 0;
+}
+
+/* ..._FreqDomain.cpp:17-51 and :151-156: the angular frequencies per time step
+ * w[iw] = 2 pi (iw df + fmin) dt, the DFT kernels kre/kim[iw][it] = cos/sin(w[iw] it), and w2 = w^2
+ * (wList->power2()). */
+void orc_fmig_tables(int nt, float dt, float fmin, float fmax, int nw, float *w2, float *kre, float *kim) {
+    const float df = (float)(1. / ((nt * 1.0) * dt));
+    (void)fmax;
+    const float pi = acosf(-1.);
+    for (int iw = 0; iw < nw; ++iw) {
+        const float lw = (float)iw * 1.0;
+        const float w = (float)(2. * pi * ((lw * df) + fmin) * dt);
+        for (int it = 0; it < nt; ++it) {
+            kre[(size_t)iw * nt + it] = cosf((float)(w * (it * 1.0)));
+            kim[(size_t)iw * nt + it] = sinf((float)(w * (it * 1.0)));
+        }
+        w2[iw] = w * w;
+    }
+}
+
+/* ..._FreqDomain.cpp:220-357 (rtmFreqDomainPropagation) with the CPU platform's operators
+ * (S/src/platform/host/RTMCPUPlatform.cpp:20-102, :397-472).  Both wavefields advance together
+ * in forward time st = nt-1-rt: the source one from the Ricker wavelet, the receiver one from the
+ * record read backwards (rt).  Each step: the two steps, the taper of all four fields, the source,
+ * the receivers (overwritten), then for every frequency of the group the running DFT of both
+ * fields over the model interior and img += w2 (sRe rRe - sIm rIm) with the running sums.
+ * nwstep: frequencies per pass over time (0: all nw in one pass, the CPU build's choice,
+ * ..._FreqDomain.cpp:139-149).  img: padded volume, zeroed here (one shot). */
+int orc_migrate_fmig(const orc_params *p, const float *v2dt2, const float *rec, float fmin, float fmax, int nwstep,
+                     float *img) {
+    loopctx c;
+    int rc = loop_init(p, &c), nan = 0;
+    if (rc) return rc;
+    const int nw = orc_fmig_nw(p->nt, p->dt, fmin, fmax);
+    if (nwstep <= 0 || nwstep > nw) nwstep = nw;
+    const int nxe = c.nxe, nye = c.nye, nze = c.nze, b = p->blen, nx = p->nx, ny = p->ny, nz = p->nz;
+    const size_t ni = (size_t)nx * ny * nz;
+    float *w2 = (float *)malloc(sizeof(float) * (nw > 0 ? nw : 1));
+    float *kre = (float *)malloc(sizeof(float) * (size_t)(nw > 0 ? nw : 1) * p->nt);
+    float *kim = (float *)malloc(sizeof(float) * (size_t)(nw > 0 ? nw : 1) * p->nt);
+    orc_fmig_tables(p->nt, p->dt, fmin, fmax, nw, w2, kre, kim);
+    float *P = (float *)calloc(c.n, sizeof(float)), *PP = (float *)calloc(c.n, sizeof(float));
+    float *PR = (float *)calloc(c.n, sizeof(float)), *PPR = (float *)calloc(c.n, sizeof(float));
+    float *sRe = (float *)calloc(ni * (nwstep > 0 ? nwstep : 1), sizeof(float));
+    float *sIm = (float *)calloc(ni * (nwstep > 0 ? nwstep : 1), sizeof(float));
+    float *rRe = (float *)calloc(ni * (nwstep > 0 ? nwstep : 1), sizeof(float));
+    float *rIm = (float *)calloc(ni * (nwstep > 0 ? nwstep : 1), sizeof(float));
+    const size_t chunk = (size_t)p->rcx * p->rcy * p->ntstep;
+    const int sx = p->sx + b, sy = p->sy + b, sz = p->sz + b;
+    memset(img, 0, c.n * sizeof(float));
+    for (int gw = 0; gw < nw; gw += nwstep) {
+        memset(P, 0, c.n * sizeof(float)); memset(PP, 0, c.n * sizeof(float));
+        memset(PR, 0, c.n * sizeof(float)); memset(PPR, 0, c.n * sizeof(float));
+        memset(sRe, 0, ni * nwstep * sizeof(float)); memset(sIm, 0, ni * nwstep * sizeof(float));
+        memset(rRe, 0, ni * nwstep * sizeof(float)); memset(rIm, 0, ni * nwstep * sizeof(float));
+        for (int itstep = p->nt - p->ntstep; itstep >= 0; itstep -= p->ntstep) {
+            const float *rchunk = rec + (size_t)(itstep / p->ntstep) * chunk;
+            for (int lt = p->ntstep - 1; lt >= 0; --lt) {
+                const int rt = itstep + lt, st = p->nt - 1 - rt;
+                nan |= orc_step(nxe, nye, nze, p->order, c.coefs, P, PP, v2dt2);
+                nan |= orc_step(nxe, nye, nze, p->order, c.coefs, PR, PPR, v2dt2);
+                orc_taper_all(nxe, nye, nze, b, c.taper, P);
+                orc_taper_all(nxe, nye, nze, b, c.taper, PP);
+                orc_taper_all(nxe, nye, nze, b, c.taper, PR);
+                orc_taper_all(nxe, nye, nze, b, c.taper, PPR);
+                orc_apply_source(nxe, nye, nze, sx, sy, sz, c.wavelet[st], PP);
+                orc_restore_receivers(p, lt, PPR, rchunk);
+                for (int lw = 0, iw = gw; lw < nwstep && iw < nw; ++lw, ++iw) {
+                    const float kr = kre[(size_t)iw * p->nt + st], ki = kim[(size_t)iw * p->nt + st];
+                    const float w2v = w2[iw];
+                    float *fr = sRe + lw * ni, *fi = sIm + lw * ni, *gr = rRe + lw * ni, *gi = rIm + lw * ni;
+#pragma omp parallel for collapse(2)
+                    for (int ix = 0; ix < nx; ++ix)
+                        for (int iy = 0; iy < ny; ++iy) {
+                            size_t o = IDX(ix + b, iy + b, b), f = ((size_t)ix * ny + iy) * nz;
+                            for (int iz = 0; iz < nz; ++iz, ++o, ++f) {
+                                const float ps = PP[o], pr = PPR[o];
+                                fr[f] += (kr * ps);
+                                fi[f] += (ki * ps);
+                                gr[f] += (kr * pr);
+                                gi[f] += (ki * pr);
+                            }
+                        }
+#pragma omp parallel for collapse(2)
+                    for (int ix = 0; ix < nx; ++ix)
+                        for (int iy = 0; iy < ny; ++iy) {
+                            size_t o = IDX(ix + b, iy + b, b), f = ((size_t)ix * ny + iy) * nz;
+                            for (int iz = 0; iz < nz; ++iz, ++o, ++f)
+                                img[o] += (w2v) * (fr[f] * gr[f] - fi[f] * gi[f]);
+                        }
+                }
+                SWAP(P, PP);
+                SWAP(PR, PPR);
+            }
+        }
+    }
+    free(P); free(PP); free(PR); free(PPR); free(sRe); free(sIm); free(rRe); free(rIm);
+    free(w2); free(kre); free(kim); loop_free(&c);
+    return nan;
+}

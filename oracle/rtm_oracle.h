@@ -66,6 +66,14 @@ int orc_model_shot(const orc_params *p, const float *v2dt2, float *rec);
 int orc_migrate_hbc(const orc_params *p, const float *v2dt2, const float *rec, float *img);
 int orc_migrate_rbc(const orc_params *p, const float *v2dt2, const float *rec, float *img);
 
+/* frequency-domain RTM (S/src/kernel/RTMFiniteDifferencesKernel_FreqDomain.cpp).  nw: number of
+ * frequencies; tables: w2[nw], kre/kim[nw][nt].  orc_migrate_fmig: one shot, img padded (zeroed
+ * here); nwstep frequencies per pass over time (0: all). */
+int orc_fmig_nw(int nt, float dt, float fmin, float fmax);
+void orc_fmig_tables(int nt, float dt, float fmin, float fmax, int nw, float *w2, float *kre, float *kim);
+int orc_migrate_fmig(const orc_params *p, const float *v2dt2, const float *rec, float fmin, float fmax, int nwstep,
+                     float *img);
+
 #ifdef __cplusplus
 }
 #endif

@@ -6,9 +6,11 @@ The reference CPU program (oracle/_ref/RTM3D.bin, built from the reference's sou
   * model_abc.npz  -- modeling shot record (ABC velocity + all-face taper), reference .seism files
   * mig_hbc.npz    -- HBC migration image (RTMIMG file) with the extended velocity it used (vpe)
   * mig_rbc.npz    -- RBC migration image with its extended velocity
+  * mig_fmig.npz   -- frequency-domain RTM image (fmig = true) with its extended velocity
   * ops.npz        -- per-operator vectors from the reference CPU platform (oracle/_ref/librtmref.so)
 
-Run:  python tests/golden/make_golden.py      (needs oracle/_ref, i.e. the reference sources)
+Run:  python tests/golden/make_golden.py [names...]   (needs oracle/_ref, i.e. the reference sources;
+      names: model mig ops fmig, default all)
 """
 from __future__ import annotations
 
@@ -30,7 +32,10 @@ from oracle import REF_BIN, Reference  # noqa: E402
 from rtm_cases import input_json, layered_model, CASES  # noqa: E402
 
 
-def run_reference(case: dict, mode: str, workdir: str, vpe_path: str | None = None):
+FMIG = dict(fmig_min_freq=5.0, fmig_max_freq=40.0, fmig_nwstep=2)
+
+
+def run_reference(case: dict, mode: str, workdir: str, vpe_path: str | None = None, extra: dict | None = None):
     """Run RTM3D.bin for one case. mode: 'model' | 'hbc' | 'rbc'. Returns output arrays."""
     v = layered_model(case)
     vp = os.path.join(workdir, "vel.bin")
@@ -41,6 +46,7 @@ def run_reference(case: dict, mode: str, workdir: str, vpe_path: str | None = No
     else:
         d.update(modeling=False, migration=True, boundary_condition=mode,
                  save_vpe_file=True, vpefile=vpe_path or os.path.join(workdir, f"vpe_{mode}.bin"))
+    d.update(extra or {})
     jp = os.path.join(workdir, f"{mode}.json")
     with open(jp, "w") as f:
         json.dump(d, f)
@@ -57,7 +63,21 @@ def read_record(d: dict):
         n, d["receiver_count_x"], d["receiver_count_y"], d["ntstep"])
 
 
-def main():
+def fmig_fixture(case: dict, rec: np.ndarray, wd: str):
+    """Frequency-domain RTM of the modeled shot (HBC-extended velocity; the CPU build runs every
+    frequency in one pass whatever fmig_nwstep says)."""
+    for f in glob.glob(os.path.join(wd, "out", "RTMIMG_*")):
+        os.remove(f)
+    dm = run_reference(case, "hbc", wd, vpe_path=os.path.join(wd, "vpe_fmig.bin"), extra=dict(fmig=True, **FMIG))
+    img = np.fromfile(glob.glob(os.path.join(wd, "out", "RTMIMG_*"))[0], np.float32)
+    img = img.reshape(case["nx"], case["ny"], case["nz"])
+    vpe = np.fromfile(dm["vpefile"], np.float32).reshape(
+        case["nx"] + 2 * case["blen"], case["ny"] + 2 * case["blen"], case["nz"] + 2 * case["blen"])
+    np.savez_compressed(os.path.join(HERE, "mig_fmig.npz"), img=img, vpe=vpe, rec=rec,
+                        fmin=FMIG["fmig_min_freq"], fmax=FMIG["fmig_max_freq"])
+
+
+def main(names=("model", "mig", "ops", "fmig")):
     if not os.path.exists(REF_BIN):
         raise SystemExit("oracle/_ref/RTM3D.bin missing: run `make -C oracle ref` first")
     rng = np.random.default_rng(7)
@@ -65,8 +85,11 @@ def main():
     with tempfile.TemporaryDirectory() as wd:
         d = run_reference(case, "model", wd)
         rec = read_record(d)
-        np.savez_compressed(os.path.join(HERE, "model_abc.npz"), rec=rec)
-        for bc in ("hbc", "rbc"):
+        if "model" in names:
+            np.savez_compressed(os.path.join(HERE, "model_abc.npz"), rec=rec)
+        if "fmig" in names:
+            fmig_fixture(case, rec, wd)
+        for bc in ("hbc", "rbc") if "mig" in names else ():
             for f in glob.glob(os.path.join(wd, "out", "RTMIMG_*")):
                 os.remove(f)
             dm = run_reference(case, bc, wd)
@@ -76,6 +99,9 @@ def main():
                 case["nx"] + 2 * case["blen"], case["ny"] + 2 * case["blen"], case["nz"] + 2 * case["blen"])
             np.savez_compressed(os.path.join(HERE, f"mig_{bc}.npz"), img=img, vpe=vpe, rec=rec)
 
+    if "ops" not in names:
+        print("golden fixtures written to", HERE)
+        return
     # per-operator vectors from the reference CPU platform
     R = Reference()
     nx, ny, nz, b = 10, 12, 9, 6
@@ -102,4 +128,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]) or ("model", "mig", "ops", "fmig"))

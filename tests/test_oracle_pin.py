@@ -50,6 +50,62 @@ def test_migration_vs_golden(oracle, golden, bc):
     assert bitexact(fin, g["img"])
 
 
+def test_fmig_vs_golden(oracle, golden):
+    """Frequency-domain RTM: the oracle's image equals the reference program's (fmig = true)."""
+    case, p = _golden_case(oracle)
+    g = golden["mig_fmig"]
+    img, rc = oracle.migrate_fmig(p, oracle.v2dt2(g["vpe"], case["dt"]), g["rec"], float(g["fmin"]), float(g["fmax"]))
+    assert rc == 0
+    fin = oracle.filter_remove(img, case["blen"], case["dx"], case["dy"], case["dz"])
+    assert np.abs(fin).max() > 0
+    assert bitexact(fin, g["img"])
+
+
+def test_fmig_tables_and_grouping(oracle):
+    """nw = (fmax - fmin) / df with df = 1 / (nt dt); one pass over all frequencies (nwstep 0) and
+    nwstep = nw are the same run; smaller groups change only the order of the image sums."""
+    w2, kre, kim = oracle.fmig_tables(120, 0.001, 5.0, 40.0)
+    assert len(w2) == 4 and kre.shape == (4, 120)
+    assert kre[0, 0] == 1.0 and kim[0, 0] == 0.0
+    case, p = _golden_case(oracle)
+    ve = oracle.extend_init_borders(layered_model(case), case["blen"], "abc")
+    v2 = oracle.v2dt2(ve, case["dt"])
+    rec, _ = oracle.model_shot(p, v2)
+    a, _ = oracle.migrate_fmig(p, v2, rec, 5.0, 40.0, 0)
+    b, _ = oracle.migrate_fmig(p, v2, rec, 5.0, 40.0, 4)
+    c, _ = oracle.migrate_fmig(p, v2, rec, 5.0, 40.0, 1)
+    assert bitexact(a, b)
+    assert np.linalg.norm(c - a) <= 1e-5 * np.linalg.norm(a)
+
+
+def test_fmig_vs_reference_program(oracle):
+    """A second case run through the reference program itself (order 4, rows of 37 floats)."""
+    import glob
+    import os
+    import sys
+    import tempfile
+    from oracle import REF_BIN
+    if not os.path.exists(REF_BIN):
+        pytest.skip("reference program (oracle/_ref/RTM3D.bin) not present")
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    from make_golden import read_record, run_reference
+    case = CASES["odd"]
+    with tempfile.TemporaryDirectory() as wd:
+        rec = read_record(run_reference(case, "model", wd))
+        d = run_reference(case, "rbc", wd, extra=dict(fmig=True, fmig_min_freq=2.0, fmig_max_freq=30.0,
+                                                      fmig_nwstep=1))
+        want = np.fromfile(glob.glob(os.path.join(wd, "out", "RTMIMG_*"))[0], np.float32)
+        b = case["blen"]
+        vpe = np.fromfile(d["vpefile"], np.float32).reshape(case["nx"] + 2 * b, case["ny"] + 2 * b,
+                                                            case["nz"] + 2 * b)
+    p = oracle_params(case)
+    img, rc = oracle.migrate_fmig(p, oracle.v2dt2(vpe, case["dt"]), rec, 2.0, 30.0)
+    assert rc == 0
+    fin = oracle.filter_remove(img, b, case["dx"], case["dy"], case["dz"])
+    assert np.abs(want).max() > 0
+    assert bitexact(fin, want.reshape(fin.shape))
+
+
 def test_ops_vs_reference_build(oracle, reference):
     rng = np.random.default_rng(123)
     for (nx, ny, nz, b, order) in ((13, 11, 17, 5, 6), (9, 16, 10, 8, 16)):
