@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define RTMB_ABI_VERSION 1
+#define RTMB_ABI_VERSION 2  /* 2: frequency-domain migration, two more profile categories */
 
 typedef enum rtmb_status {
     RTMB_OK = 0,
@@ -138,13 +138,15 @@ uint64_t rtmb_launch_count(const rtmb_ctx *ctx);
  * millisecond wall times per phase, src/kernel/RTMKernel.cpp:11-80).  When enabled, every driver
  * launch is bracketed by CUDA events on the context's stream; the durations are summed per category
  * at the end of each driver call.  Enabling clears the totals. */
-#define RTMB_PROF_CATEGORIES 6
+#define RTMB_PROF_CATEGORIES 8
 #define RTMB_PROF_MODEL 0             /* modeling step (taper, source, receivers fused) */
 #define RTMB_PROF_FORWARD 1           /* migration forward step */
 #define RTMB_PROF_BACKWARD_SOURCE 2   /* backward source-wavefield reconstruction step */
 #define RTMB_PROF_BACKWARD_RECEIVER 3 /* backward receiver step with receiver injection and imaging */
 #define RTMB_PROF_OTHER 4
 #define RTMB_PROF_BACKWARD_DUAL 5     /* source and receiver steps with imaging in one launch */
+#define RTMB_PROF_FMIG_STEP 6         /* frequency-domain migration: wavefield steps */
+#define RTMB_PROF_FMIG_FREQ 7         /* frequency-domain migration: DFT and image update */
 int rtmb_profile(rtmb_ctx *ctx, int enable);
 /* ms[RTMB_PROF_CATEGORIES]: summed kernel time; launches[RTMB_PROF_CATEGORIES]: launch counts. */
 int rtmb_profile_read(const rtmb_ctx *ctx, double *ms, uint64_t *launches);
@@ -227,6 +229,27 @@ int rtmb_migrate_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, cons
  *     rtmb_last_error(NULL) describes the error (per host thread). */
 int rtmb_model_shot_noalloc(const rtmb_params *params, const float *v2dt2, uint32_t sx, uint32_t sy,
                             uint32_t sz, float *rec, void *cuda_stream);
+
+/* Frequency-domain RTM of one shot (input.json "fmig": true; the reference's RTMFreqDomainKernel,
+ * src/kernel/RTMFiniteDifferencesKernel_FreqDomain.cpp:220-357, with the CPU platform's operators
+ * RTMCPUPlatform.cpp:20-102 and :397-472).  Both wavefields step forward in time together, the
+ * source one from the Ricker wavelet and the receiver one from the record read backwards, every
+ * field tapered on all faces after each step; for each of the nw frequencies
+ * w = 2 pi (fmin + iw df) dt, df = 1 / (nt dt), nw = (fmax - fmin) / df (fmig_min_freq,
+ * fmig_max_freq), a running DFT of both fields over the model interior feeds the image
+ * img += w^2 (Re S Re R - Im S Im R) at every time step.
+ *   rec:    device record in the file layout (as rtmb_migrate_shot);
+ *   nwstep: frequencies per pass over time (fmig_nwstep; 0 = all nw in one pass, the reference CPU
+ *           build's choice and its order of the image sums, so the exact form is bit-exact with it).
+ *           The pass holds 4 nwstep nx ny nz floats of frequency grids; smaller groups cost a time
+ *           loop each.  At most 256.
+ *   img:    padded FP32 image, overwritten with this shot's image.  (The reference never clears
+ *           its image between fmig shots, so its shot images accumulate; this call does not.)
+ * RTMB_FLAG_FAST_FMA selects the FMA arithmetic for the steps and the DFT.  FP32 storage only. */
+int rtmb_migrate_shot_fmig(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const float *rec, float fmin,
+                           float fmax, uint32_t nwstep, float *img);
+/* nw of a frequency-domain migration (..._FreqDomain.cpp:133-137); 0 when there is none. */
+int rtmb_fmig_nw(float dt, uint32_t nt, float fmin, float fmax);
 
 /* rtmb_migrate_shot that ADDS the shot's image to a caller-owned FP64 stack (padded, device)
  * instead of writing an FP32 image: the shot stacking of RTMAcousticController.cpp:223-242 with an

@@ -478,6 +478,7 @@ int rtmb_destroy(rtmb_ctx *ctx) {
     for (double *b : ctx->d_f64)
         if (b) cudaFree(b);
     if (ctx->d_upb64) cudaFree(ctx->d_upb64);
+    if (ctx->d_fq) cudaFree(ctx->d_fq);
     for (cudaGraphExec_t g : ctx->gexec)
         if (g) cudaGraphExecDestroy(g);
     if (ctx->d_cells) cudaFree(ctx->d_cells);
@@ -796,6 +797,119 @@ extern "C" {
 int rtmb_migrate_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const float *rec, float *img) {
     if (!ctx || !rec || !img) return fail(ctx, RTMB_EINVAL, "rtmb_migrate_shot: null pointer");
     return migrate_impl(ctx, sx, sy, sz, rec, img, false);
+}
+
+// ------------------------------------------------------------------ frequency-domain migration
+
+int rtmb_fmig_nw(float dt, uint32_t nt, float fmin, float fmax) {
+    // RTMFiniteDifferencesKernel_FreqDomain.cpp:133-137, in the reference's float / double mix
+    const float df = (float)(1. / ((nt * 1.0) * dt));
+    const float nf = ((fmax - fmin) / df);
+    return nf > 0.f ? (int)(size_t)nf : 0;
+}
+
+namespace {
+
+// The angular frequency per time step of frequency iw, w = 2 pi (iw df + fmin) dt, and the DFT
+// kernels cos(w it), sin(w it) (..._FreqDomain.cpp:17-51, the same float / double mix, so the
+// tables are the reference's bit for bit), with w2 = w^2 (wList->power2(), :151-152).
+void fmig_tables(const rtmb_params &p, float fmin, int nw, std::vector<float> &w2, std::vector<float> &kre,
+                 std::vector<float> &kim) {
+    const float df = (float)(1. / ((p.nt * 1.0) * p.dt));
+    const float pi = acosf(-1.);
+    w2.assign(nw, 0.f);
+    kre.assign((size_t)nw * p.nt, 0.f);
+    kim.assign((size_t)nw * p.nt, 0.f);
+    for (int iw = 0; iw < nw; ++iw) {
+        const float lw = (float)iw * 1.0;
+        const float w = (float)(2. * pi * ((lw * df) + fmin) * p.dt);
+        for (uint32_t it = 0; it < p.nt; ++it) {
+            kre[(size_t)iw * p.nt + it] = cosf((float)(w * (it * 1.0)));
+            kim[(size_t)iw * p.nt + it] = sinf((float)(w * (it * 1.0)));
+        }
+        w2[iw] = w * w;
+    }
+}
+
+}  // namespace
+
+// RTMFiniteDifferencesKernel_FreqDomain.cpp:220-357 (rtmFreqDomainPropagation).  Both wavefields
+// step forward in time st = nt-1-rt: the source one from the Ricker wavelet, the receiver one
+// from the record read backwards.  Per step, as the reference orders it: the two steps (:358-369,
+// rtmStepMultipleWave), the taper of the four fields, the source, the receivers, then the DFT and
+// image update of every frequency of the group.  Each group of nwstep frequencies re-runs the
+// time loop from zero fields; the image sums over the groups.
+int rtmb_migrate_shot_fmig(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const float *rec, float fmin,
+                           float fmax, uint32_t nwstep, float *img) {
+    if (!ctx || !rec || !img) return fail(ctx, RTMB_EINVAL, "rtmb_migrate_shot_fmig: null pointer");
+    int rc = check_shot(ctx, sx, sy, sz);
+    if (rc) return rc;
+    const rtmb_params &p = ctx->p;
+    if (ctx->store != rtmb::kStoreF32) return fail(ctx, RTMB_EINVAL, "frequency-domain migration runs with FP32 storage");
+    if (!(fmax > fmin)) return fail(ctx, RTMB_EINVAL, "fmig_max_freq must be above fmig_min_freq");  // RTMParam.cpp:246-251
+    if (p.receiver_depth_z + p.blen >= (uint32_t)ctx->nze - ctx->h)
+        return fail(ctx, RTMB_EINVAL, "receiver depth outside the computed region");
+    const int nw = rtmb_fmig_nw(p.dt, p.nt, fmin, fmax);
+    if (nw <= 0) return fail(ctx, RTMB_EINVAL, "no frequency in [fmig_min_freq, fmig_max_freq) at df = 1/(nt dt)");
+    int nws = (nwstep == 0 || (int)nwstep > nw) ? nw : (int)nwstep;
+    if (nws > rtmb::kFmigMaxGroup) return fail(ctx, RTMB_EINVAL, "at most %d frequencies per group (nwstep)", rtmb::kFmigMaxGroup);
+    std::vector<float> w2, kre, kim;
+    fmig_tables(p, fmin, nw, w2, kre, kim);
+    if ((rc = alloc_driver(ctx))) return rc;
+    const size_t ni = (size_t)p.nx * p.ny * p.nz, need = 4 * (size_t)nws * ni;
+    if (ctx->fq_cap < need) {
+        if (ctx->d_fq) CK(cudaFree(ctx->d_fq));
+        ctx->d_fq = nullptr;
+        ctx->fq_cap = 0;
+        CK(cudaMalloc(&ctx->d_fq, need * sizeof(float)));
+        ctx->fq_cap = need;
+    }
+    const rtmb::Geom g = geom(ctx);
+    const rtmb::RcvGeom rg = rgeom(ctx);
+    const size_t nb = wave_bytes(ctx), rchunk = (size_t)rg.rcx * rg.rcy * p.ntstep;
+    const int rmode = (p.flags & RTMB_FLAG_RCV_ADD) ? 3 : 2;
+    const int quirk = !(p.flags & RTMB_FLAG_NO_TAPER_QUIRK);
+    rtmb::StepArgs a = base_args(ctx);
+    a.V = ctx->d_v2dt2;
+    a.taper_mode = rtmb::kTaperNone;
+    a.sxe = -1;  // the source is a separate operator here (after the taper)
+    GraphScope graph(ctx, 3);
+    if ((rc = graph.begin())) return rc;
+    CK(cudaMemsetAsync(img, 0, ctx->n * sizeof(float), ctx->stream));
+    rtmb::FmigStep fs;
+    for (int gw = 0; gw < nw; gw += nws) {
+        const int m = nw - gw < nws ? nw - gw : nws;
+        float *Ps = ctx->d_w[0], *PPs = ctx->d_w[1], *Pr = ctx->d_w[2], *PPr = ctx->d_w[3];
+        for (int k = 0; k < 4; ++k) CK(cudaMemsetAsync(ctx->d_w[k], 0, nb, ctx->stream));
+        CK(cudaMemsetAsync(ctx->d_fq, 0, 4 * (size_t)nws * ni * sizeof(float), ctx->stream));
+        fs.nws = m;
+        for (uint32_t st = 0; st < p.nt; ++st) {
+            const uint32_t rt = p.nt - 1 - st;
+            for (int k = 0; k < 2; ++k) {  // rtmStepMultipleWave: both wavefields, the same v2dt2
+                a.P = k ? Pr : Ps;
+                a.PP = k ? PPr : PPs;
+                a.it = (int)st;
+                LAUNCH_CAT(RTMB_PROF_FMIG_STEP, rtmb::launch_step(a, (int)p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
+            }
+            float *tap[4] = {Ps, PPs, Pr, PPr};
+            for (float *f : tap) LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_taper(f, ctx->d_taper, g, 0, quirk, ctx->stream));
+            LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_source(PPs, ctx->d_wavelet, (int)st, (int)(sx + p.blen),
+                                                            (int)(sy + p.blen), (int)(sz + p.blen), g, ctx->stream));
+            LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_receivers(PPr, const_cast<float *>(rec) + (size_t)(rt / p.ntstep) * rchunk,
+                                                               (int)(rt % p.ntstep), rmode, rg, g, ctx->stream));
+            for (int lw = 0; lw < m; ++lw) {
+                fs.kre[lw] = kre[(size_t)(gw + lw) * p.nt + st];
+                fs.kim[lw] = kim[(size_t)(gw + lw) * p.nt + st];
+                fs.w2[lw] = w2[gw + lw];
+            }
+            LAUNCH_CAT(RTMB_PROF_FMIG_FREQ, rtmb::launch_fmig_freq(PPs, PPr, img, ctx->d_fq, fs, g, (int)p.nx, (int)p.ny,
+                                                                   (int)p.nz, exact(ctx), ctx->stream));
+            std::swap(Ps, PPs);
+            std::swap(Pr, PPr);
+        }
+    }
+    if ((rc = graph.end())) return rc;
+    return check_err_flag(ctx);
 }
 
 int rtmb_migrate_shot_acc64(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const float *rec,

@@ -37,7 +37,10 @@ struct rtmb_ctx {
     float *d_inj = nullptr;          // device scalars: [0] max |record|, [1] max forward level
     double *d_img64 = nullptr;       // FP64 image of the FP32-output migration with RTMB_FLAG_IMG_F64
     // RTMB_FLAG_USE_GRAPH: executable graph per driver kind (0 modeling, 1 migration)
-    cudaGraphExec_t gexec[3] = {};  // modeling, migration, batched migration
+    cudaGraphExec_t gexec[4] = {};  // modeling, migration, batched migration, frequency-domain migration
+    // frequency-domain migration: the four frequency grids of a group, and their capacity in floats
+    float *d_fq = nullptr;
+    size_t fq_cap = 0;
     bool capturing = false;
     // learned boundary closure (closure.cu): strip cells of the padded grid, parameters, and the
     // strip values of the next level computed before each step

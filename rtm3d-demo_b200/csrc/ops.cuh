@@ -35,6 +35,18 @@ cudaError_t launch_filter_remove(const float *img, float *out, const float *c3, 
 // acc += img over n floats.
 cudaError_t launch_stack(float *acc, const float *img, size_t n, cudaStream_t s);
 
+// Frequency-domain RTM (fmig.cu): one time step of the running DFT of both wavefields and of the
+// frequency-domain image for a group of at most kFmigMaxGroup frequencies.  The per-step table
+// values (kre = cos(w it), kim = sin(w it), w2 = w^2 for each frequency of the group) travel as
+// kernel parameters.  fq holds the four grids [4][nws][nx][ny][nz] (sRe, sIm, rRe, rIm).
+constexpr int kFmigMaxGroup = 256;
+struct FmigStep {
+    int nws;
+    float kre[kFmigMaxGroup], kim[kFmigMaxGroup], w2[kFmigMaxGroup];
+};
+cudaError_t launch_fmig_freq(const float *ps, const float *pr, float *img, float *fq, const FmigStep &f, const Geom &g,
+                             int nx, int ny, int nz, bool exact, cudaStream_t s);
+
 // FP64 overloads of the operators above, for the FP64 GPU oracle (same operator sequence and
 // multiply order, double arithmetic).
 cudaError_t launch_taper(double *P, const float *taper, const Geom &g, int upper, int quirk, cudaStream_t s);

@@ -100,6 +100,8 @@ SYMBOLS = [
     ("rtmb_migrate_shot_host", [_vp, _u32, _u32, _u32, _vp, _vp], C.c_int),
     ("rtmb_model_shot_noalloc", [C.POINTER(Params), _vp, _u32, _u32, _u32, _vp, _vp], C.c_int),
     ("rtmb_migrate_shot_acc64", [_vp, _u32, _u32, _u32, _vp, _vp], C.c_int),
+    ("rtmb_migrate_shot_fmig", [_vp, _u32, _u32, _u32, _vp, C.c_float, C.c_float, _u32, _vp], C.c_int),
+    ("rtmb_fmig_nw", [C.c_float, _u32, C.c_float, C.c_float], C.c_int),
     ("rtmb_model_shot_f64", [_vp, _u32, _u32, _u32, _vp], C.c_int),
     ("rtmb_migrate_shot_f64", [_vp, _u32, _u32, _u32, _vp, _vp], C.c_int),
     ("rtmb_closure_param_count", [], C.c_int),
@@ -204,7 +206,8 @@ class Context:
     def launches(self) -> int:
         return int(self.L.rtmb_launch_count(self.h))
 
-    PROF_NAMES = ("model", "forward", "backward_source", "backward_receiver", "other", "backward_dual")
+    PROF_NAMES = ("model", "forward", "backward_source", "backward_receiver", "other", "backward_dual",
+                  "fmig_step", "fmig_freq")
 
     def profile(self, enable: bool = True) -> None:
         """Time every driver launch with CUDA events (per category); enabling clears the totals."""
@@ -265,6 +268,10 @@ class Context:
 
     def migrate_shot(self, sx, sy, sz, rec, img):
         self._check(self.L.rtmb_migrate_shot(self.h, sx, sy, sz, _ptr(rec), _ptr(img)))
+
+    def migrate_shot_fmig(self, sx, sy, sz, rec, img, fmin, fmax, nwstep=0):
+        """Frequency-domain RTM of one shot into img (padded, device, float32, overwritten)."""
+        self._check(self.L.rtmb_migrate_shot_fmig(self.h, sx, sy, sz, _ptr(rec), fmin, fmax, nwstep, _ptr(img)))
 
     def migrate_shot_acc64(self, sx, sy, sz, rec, stack):
         """Adds this shot's image to an FP64 stack (padded, device, float64)."""
@@ -347,6 +354,11 @@ def ricker(nt, dt, fpeak):
     out = np.zeros(nt, np.float32)
     load().rtmb_ricker(nt, dt, fpeak, out.ctypes.data_as(_fp))
     return out
+
+
+def fmig_nw(dt: float, nt: int, fmin: float, fmax: float) -> int:
+    """Number of frequencies of a frequency-domain migration (0 when there is none)."""
+    return int(load().rtmb_fmig_nw(dt, nt, fmin, fmax))
 
 
 def prepare_velocity(v, blen: int, bc: str, seed: int = -1):

@@ -25,7 +25,7 @@ def test_library_exports_every_declared_symbol():
     for n in names:
         assert hasattr(lib, n), n
         assert n in bound, f"{n} missing from the Python binding"
-    assert lib.rtmb_abi_version() == 1
+    assert lib.rtmb_abi_version() == 2
 
 
 @pytest.mark.parametrize("order", [2, 4, 6, 8, 10, 12, 14, 16])
@@ -83,3 +83,11 @@ def test_storage_flag_combinations_are_checked_before_any_device_work():
     assert create(4, 16, 8, rtmb.FLAG_STORE_F16) == rtmb.RTMB_EINVAL    # order 8 only
     assert create(8, 17, 8, rtmb.FLAG_STORE_BF16) == rtmb.RTMB_EINVAL   # nz + 2 blen = 33: not a multiple of 8
     assert b"multiple of 8" in lib.rtmb_last_error(None)
+
+
+@pytest.mark.parametrize("nt,dt,fmin,fmax", [(120, 0.001, 5.0, 40.0), (90, 0.0012, 2.0, 30.0), (3000, 0.001, 0.0, 30.0),
+                                             (100, 0.001, 10.0, 10.5)])
+def test_fmig_frequency_count(oracle, nt, dt, fmin, fmax):
+    """The library's nw of a frequency-domain migration is the oracle's (the reference's float mix)."""
+    import rtmb
+    assert rtmb.fmig_nw(dt, nt, fmin, fmax) == oracle.L.orc_fmig_nw(nt, dt, fmin, fmax)
