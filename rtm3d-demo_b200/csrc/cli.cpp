@@ -20,8 +20,12 @@
 //   "b200_fast_fma" (bool)   FMA form of the stencil (not bit-exact with the reference CPU path)
 //   "b200_device"   (uint)   CUDA device ordinal
 //   "b200_rbc_seed" (uint)   seed of the random border (libc srand; the reference leaves rand() unseeded)
-// Out of scope and rejected: fmig (frequency-domain migration), distributed_grid (MPI halo
-// decomposition) and 2D models (nx == 1).
+//   fmig       frequency-domain migration instead (RTMFreqDomainKernel, selected by "fmig": true,
+//              src/process/RTMAcousticProcess.cpp:16-18), fmig_nwstep frequencies per pass over
+//              time as the reference's accelerator builds take it (0: all in one pass, the CPU
+//              build's order).
+// Out of scope and rejected: distributed_grid and fmig_distributed_imaging (MPI partitions) and
+// 2D models (nx == 1).
 #include <algorithm>
 #include <cctype>
 #include <chrono>
@@ -53,6 +57,9 @@ struct Param {
     unsigned receiver_count_x, receiver_count_y;
     float dx, dy, dz, dt, fpeak, taper_factor;
     bool modeling, migration, save_vpe_file, load_vpe_from_file, verbose, save_snapshots, distributed_grid, fmig;
+    bool fmig_distributed_imaging;
+    float fmig_min_freq, fmig_max_freq;
+    unsigned fmig_nwstep;
     bool fast_fma = false;
     int device = -1;
     long long rbc_seed = -1;
@@ -134,6 +141,8 @@ Param load_param(const std::string &path) {
     p.modeling = B("modeling"); p.migration = B("migration"); p.save_vpe_file = B("save_vpe_file");
     p.load_vpe_from_file = B("load_vpe_from_file"); p.verbose = B("verbose");
     p.save_snapshots = B("save_snapshots"); p.distributed_grid = B("distributed_grid"); p.fmig = B("fmig");
+    p.fmig_distributed_imaging = B("fmig_distributed_imaging");
+    p.fmig_min_freq = F("fmig_min_freq"); p.fmig_max_freq = F("fmig_max_freq"); p.fmig_nwstep = U("fmig_nwstep");
     if (o.count("b200_fast_fma") && o.at("b200_fast_fma").kind == Kind::Bool) p.fast_fma = o.at("b200_fast_fma").b;
     if (o.count("b200_device") && o.at("b200_device").kind == Kind::Unsigned) p.device = (int)o.at("b200_device").u;
     if (o.count("b200_rbc_seed") && o.at("b200_rbc_seed").kind == Kind::Unsigned)
@@ -141,7 +150,10 @@ Param load_param(const std::string &path) {
     // RTMParam::loadRTMParam (:241-245)
     if (p.nt < p.ntstep) throw Error("[ RTMParam Error: NT smaller than NTSTEP ]");
     if (p.ntstep == 0 || p.nt % p.ntstep) throw Error("[ nt must be a multiple of ntstep ]");
-    if (p.fmig) throw Error("[ fmig (frequency-domain migration) is not supported by this build ]");
+    if (p.fmig && p.fmig_max_freq <= p.fmig_min_freq)  // RTMParam.cpp:246-251
+        throw Error("[ RTMParam Error: fmig_max_freq must be greater than fmig_min_freq ]");
+    if (p.fmig && p.fmig_distributed_imaging)
+        throw Error("[ fmig_distributed_imaging (MPI partition of the image) is not supported: one GPU holds the volume ]");
     if (p.distributed_grid) throw Error("[ distributed_grid (MPI halo decomposition) is not supported: one GPU holds the volume ]");
     if (p.nx == 1) throw Error("[ 2D models (nx == 1) are not supported by this build ]");
     return p;
@@ -296,7 +308,12 @@ int run(const Param &p) {
             const auto t0 = std::chrono::steady_clock::now();
             if (cudaMemcpy(d_rec, rec, nrec * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
                 throw Error("record upload failed");
-            check(rtmb_migrate_shot(ctx, s.sx, s.sy, s.sz, d_rec, d_img), ctx, "migration");
+            if (p.fmig)
+                check(rtmb_migrate_shot_fmig(ctx, s.sx, s.sy, s.sz, d_rec, p.fmig_min_freq, p.fmig_max_freq,
+                                             p.fmig_nwstep, d_img),
+                      ctx, "frequency-domain migration");
+            else
+                check(rtmb_migrate_shot(ctx, s.sx, s.sy, s.sz, d_rec, d_img), ctx, "migration");
             check(rtmb_image_stack(ctx, d_stack, d_img), ctx, "image stack");
             check(rtmb_sync(ctx), ctx, "sync");
             t_total += seconds_since(t0);
@@ -316,7 +333,13 @@ int run(const Param &p) {
         write_floats(name, img.data(), img.size());
     }
     if (p.verbose) {
-        const double pts = double(n) * (p.modeling ? p.nt : (3.0 * p.nt - 2.0)) * nshots;
+        double sweeps = p.modeling ? p.nt : (3.0 * p.nt - 2.0);
+        if (p.fmig) {  // two wavefields stepped per pass over time, one pass per group of frequencies
+            const int nw = rtmb_fmig_nw(p.dt, p.nt, p.fmig_min_freq, p.fmig_max_freq);
+            const int nws = (p.fmig_nwstep == 0 || (int)p.fmig_nwstep > nw) ? nw : (int)p.fmig_nwstep;
+            sweeps = 2.0 * p.nt * (nws > 0 ? (nw + nws - 1) / nws : 0);
+        }
+        const double pts = double(n) * sweeps * nshots;
         std::printf("{\n  \"mname\": %s\n  \"nx\":%u\n  \"ny\":%u\n  \"nz\":%u\n  \"nt\":%u\n  \"%s_time\":%f\n"
                     "  \"gpoint_updates_per_s\":%f\n}\n",
                     p.mname.c_str(), p.nx, p.ny, p.nz, p.nt, p.modeling ? "modeling" : "migration", t_total,

@@ -64,7 +64,8 @@ def test_missing_key(base):
 @pytest.mark.parametrize("patch,expect", [
     (dict(nt=30, ntstep=40), "NT smaller than NTSTEP"),
     (dict(nt=100, ntstep=40), "multiple of ntstep"),
-    (dict(fmig=True), "fmig"),
+    (dict(fmig=True, fmig_min_freq=30.0, fmig_max_freq=20.0), "fmig_max_freq must be greater"),
+    (dict(fmig=True, fmig_distributed_imaging=True), "fmig_distributed_imaging"),
     (dict(distributed_grid=True), "distributed_grid"),
     (dict(nx=1), "nx == 1"),
 ])

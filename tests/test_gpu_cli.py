@@ -4,6 +4,8 @@
   own output (tests/golden/model_abc.npz).
 * HBC migration of those chunks with the reference's extended velocity (load_vpe_from_file) writes
   the reference's RTMIMG file, bit-identical to its output (tests/golden/mig_hbc.npz).
+* Frequency-domain migration ("fmig": true) writes the reference program's RTMIMG file
+  (tests/golden/mig_fmig.npz).
 * Several shots: the records are written, and read back, by a background task while the next shot
   runs; the files and the stacked image equal the library calls shot by shot."""
 import glob
@@ -57,6 +59,27 @@ def test_cli_model_and_hbc_migration_match_reference_files(cuda, golden, tmp_pat
     run_cli(d, tmp)
     files = glob.glob(os.path.join(d["outdir"], "RTMIMG_*"))
     assert len(files) == 1 and files[0].endswith(f"_NXNYNZ_{case['nx']}x{case['ny']}x{case['nz']}_NT{case['nt']}.bin.NP1")
+    img = np.fromfile(files[0], np.float32).reshape(case["nx"], case["ny"], case["nz"])
+    assert bitexact(img, g["img"])
+
+
+def test_cli_fmig_matches_reference_file(cuda, golden, tmp_path):
+    """"fmig": true runs the frequency-domain migration: the RTMIMG file equals the reference
+    program's (tests/golden/mig_fmig.npz, the same band, all frequencies in one pass)."""
+    case = CASES["golden"]
+    tmp = str(tmp_path)
+    vp = os.path.join(tmp, "vel.bin")
+    layered_model(case).tofile(vp)
+    d = input_json(case, vpfile=vp, workdir=tmp)
+    d.update(modeling=True, migration=False)
+    run_cli(d, tmp)
+    g = golden["mig_fmig"]
+    g["vpe"].astype(np.float32).tofile(d["vpefile"])
+    d.update(modeling=False, migration=True, boundary_condition="hbc", load_vpe_from_file=True, fmig=True,
+             fmig_min_freq=float(g["fmin"]), fmig_max_freq=float(g["fmax"]), fmig_nwstep=0)
+    run_cli(d, tmp)
+    files = glob.glob(os.path.join(d["outdir"], "RTMIMG_*"))
+    assert len(files) == 1
     img = np.fromfile(files[0], np.float32).reshape(case["nx"], case["ny"], case["nz"])
     assert bitexact(img, g["img"])
 
