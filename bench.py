@@ -515,6 +515,85 @@ def run_batch(args) -> dict:
             "speedup": round(ms_single / ms_batch, 3)}
 
 
+# ------------------------------------------------------------------------------------------ fmig
+def run_fmig(args) -> dict:
+    """Frequency-domain RTM of one shot (rtmb_migrate_shot_fmig): the salt model, HBC border, both
+    wavefields stepped forward in time and the running DFT of nw frequencies imaged every step.
+    Reported: s per shot, wavefield point-updates/s, and the roofline of the DFT/image kernel (HBM:
+    16 B per interior point for ps, pr and the image, plus 32 B per frequency for the four
+    frequency grids).  cpu_baseline: the oracle restatement of the same migration (OpenMP) on the
+    same grid and the same number of frequencies, for a few time steps."""
+    import torch
+    import rtmb
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    n, nt, blen, dt = args.fmig_size, args.fmig_nt, 32, 0.001
+    fmin, fmax = args.fmig_band
+    p = dict(workload(n, nt), blen=blen, boundary_condition="hbc", receiver_depth_z=2)
+    nw = rtmb.fmig_nw(dt, nt, fmin, fmax)
+    flags = form_flags(rtmb, args.form if args.form in ("fp32_exact", "fp32_fma") else "fp32_fma")
+    ctx = rtmb.Context(rtmb.Params.from_input(p, flags=flags | rtmb.FLAG_USE_GRAPH, device=0))
+    ve = rtmb.prepare_velocity(salt_model(n), blen, "hbc", seed=5)
+    ctx.load_v2dt2(rtmb.v2dt2(ve, dt), from_host=True)
+    rng = np.random.default_rng(3)
+    rec = torch.from_numpy((rng.standard_normal((1, n // 2, n // 2, nt)) * 1e-3).astype(np.float32)).to(dev)
+    img = torch.zeros(ctx.padded_shape, dtype=torch.float32, device=dev)
+    shot = (p["sx"], p["sy"], p["sz"])
+    for _ in range(max(1, args.warmup - 2)):
+        ctx.migrate_shot_fmig(*shot, rec, img, fmin, fmax, args.fmig_nwstep)
+    ctx.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ctx.migrate_shot_fmig(*shot, rec, img, fmin, fmax, args.fmig_nwstep)
+    e1.record()
+    ctx.sync()
+    ms = e0.elapsed_time(e1)
+    # per-kernel split (a separate run: events around every launch)
+    pctx = rtmb.Context(rtmb.Params.from_input(p, flags=flags, device=0))
+    pctx.load_v2dt2(rtmb.v2dt2(ve, dt), from_host=True)
+    pctx.profile(True)
+    pctx.migrate_shot_fmig(*shot, rec, img, fmin, fmax, args.fmig_nwstep)
+    prof = pctx.profile_read()
+    pctx.close()
+    nws = nw if args.fmig_nwstep in (0,) or args.fmig_nwstep > nw else args.fmig_nwstep
+    groups = -(-nw // nws)
+    npad = int(np.prod(ctx.padded_shape))
+    ni = n * n * n
+    upd = 2 * nt * groups * npad
+    fq = prof["fmig_freq"]
+    f_ms = fq["ms"] / max(fq["launches"], 1)
+    bytes_freq = ni * (16 + 32 * nws)  # the last group may be smaller; nw = nws x groups here
+    peak, peak_kind = measured_hbm_gbs()
+    achieved = bytes_freq / (f_ms * 1e-3) / 1e9
+    out = {"metric": "s per migrated shot, frequency-domain RTM", "workload": "fmig",
+           "config": {"grid": list(ctx.padded_shape), "model": f"salt {n}^3", "blen": blen, "nt": nt,
+                      "band_hz": [fmin, fmax], "nw": nw, "nwstep": nws, "form": "fp32_exact" if flags == 0 else "fp32_fma"},
+           "s_per_shot": round(ms / 1e3, 4), "gpt_s": round(upd / ms / 1e6, 2),
+           "kernels": {k: {"ms_total": round(v["ms"], 2), "launches": v["launches"]} for k, v in prof.items()
+                       if v["launches"]},
+           "roofline": {"bound": "hbm", "kernel": "fmig_freq_kernel", "achieved": round(achieved, 1),
+                        "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                        "bytes_per_launch": bytes_freq, "launch_ms": round(f_ms, 4)}}
+    if not args.no_cpu_baseline:
+        from oracle import Oracle
+        O = Oracle()
+        nts = 6
+        p_or = {k: p[k] for k in ("nx", "ny", "nz", "blen", "nt", "ntstep", "dx", "dy", "dz", "dt", "fpeak",
+                                  "taper_factor", "sx", "sy", "sz")}
+        p_or.update(order=8, nt=nts, ntstep=nts, rsx=0, rsy=0, rdz=2, rdx=2, rdy=2, rcx=n // 2, rcy=n // 2)
+        fmax_s = fmin + (nw + 0.5) / (nts * dt)  # the same number of frequencies over nts steps
+        v2 = rtmb.v2dt2(ve, dt)
+        rs = rec[..., :nts].cpu().numpy()
+        t0 = time.time()
+        O.migrate_fmig(p_or, v2, rs, fmin, fmax_s, 0)
+        cpu_s = time.time() - t0
+        cpu_upd = 2 * nts * npad
+        out["cpu_baseline"] = {"value": round(cpu_upd / cpu_s / 1e9, 4), "unit": "Gpt/s", "cores": os.cpu_count(),
+                               "kind": "port", "sample": f"oracle fmig on the same grid, nw={O.L.orc_fmig_nw(nts, dt, fmin, fmax_s)}, "
+                                                        f"{nts} time steps"}
+    return out
+
+
 # ------------------------------------------------------------------------------------------ closure
 def run_closure(args) -> dict:
     """The learned 8-cell boundary closure against the tapered borders of 8 and 32 cells: reflected
@@ -653,9 +732,14 @@ def main():
     ap.add_argument("--nt", type=int, default=3000)
     ap.add_argument("--form", choices=FORMS, default="fp32_fma", help="arithmetic/storage form of the timed shots")
     ap.add_argument("--exact", action="store_true", help="same as --form fp32_exact")
-    ap.add_argument("--workload", choices=("rtm", "batch", "closure"), default="rtm",
+    ap.add_argument("--workload", choices=("rtm", "batch", "closure", "fmig"), default="rtm",
                     help="rtm: the single-shot RTM line (default); batch: batched aperture shots against "
-                         "one-by-one; closure: the learned boundary closure against the tapered borders")
+                         "one-by-one; closure: the learned boundary closure against the tapered borders; "
+                         "fmig: frequency-domain RTM of one shot")
+    ap.add_argument("--fmig-size", type=int, default=192)
+    ap.add_argument("--fmig-nt", type=int, default=400)
+    ap.add_argument("--fmig-band", type=float, nargs=2, default=(4.0, 20.0))
+    ap.add_argument("--fmig-nwstep", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-size", type=int, default=256, help="batch workload: survey 2s x 2s x s cells")
     ap.add_argument("--batch-nt", type=int, default=500)
@@ -682,7 +766,8 @@ def main():
     if args.impl == "reference":
         out = run_reference_arm(args, rank)
     elif args.workload != "rtm":
-        out = (run_batch if args.workload == "batch" else run_closure)(args) if rank == 0 else None
+        runner = {"batch": run_batch, "closure": run_closure, "fmig": run_fmig}[args.workload]
+        out = runner(args) if rank == 0 else None
     else:
         if world > 1:
             import datetime

@@ -892,7 +892,7 @@ int rtmb_migrate_shot_fmig(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz,
                 LAUNCH_CAT(RTMB_PROF_FMIG_STEP, rtmb::launch_step(a, (int)p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
             }
             float *tap[4] = {Ps, PPs, Pr, PPr};
-            for (float *f : tap) LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_taper(f, ctx->d_taper, g, 0, quirk, ctx->stream));
+            LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_taper_fields(tap, 4, ctx->d_taper, g, 0, quirk, ctx->stream));
             LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_source(PPs, ctx->d_wavelet, (int)st, (int)(sx + p.blen),
                                                             (int)(sy + p.blen), (int)(sz + p.blen), g, ctx->stream));
             LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_receivers(PPr, const_cast<float *>(rec) + (size_t)(rt / p.ntstep) * rchunk,

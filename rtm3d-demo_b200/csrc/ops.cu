@@ -10,54 +10,71 @@ __device__ __forceinline__ float fac(const float *t, int b, int n, int i) {
     return i < b ? t[b - 1 - i] : t[i - (n - b)];
 }
 
-// One thread owns a (y, z) column and walks x, so the front-right quirk of taper3D (a cell that
-// takes its value from x = blen, RTMCPUPlatform.cpp:900-904) reads the raw value of its own column
-// before anything in the column is written.
+// Up to four fields tapered by one launch (the frequency-domain migration tapers four per step).
 template <typename R>
-__global__ void taper_kernel(R *P, const float *__restrict__ t, Geom g, int upper, int quirk) {
+struct Fields {
+    R *f[4];
+    int n;
+};
+
+// One thread per cell, z fastest (grid: z blocks, y, x), for every field of fs: the cell's loads
+// of the fields are independent, so they are in flight together.  Cells off every tapered border
+// leave at once.  The front-right quirk of taper3D (a cell (x < blen, y >= nye - blen, z off the z
+// borders) takes ((P(blen, y, z) ty) tx) ty, RTMCPUPlatform.cpp:900-904) needs the raw
+// P(blen, y, z), which its own thread overwrites: so the thread of (blen, y, z) writes the quirk
+// cells of its column and their own threads skip them.  Per cell the factors multiply in the
+// reference's loop order.
+template <typename R>
+__global__ void taper_kernel(Fields<R> fs, const float *__restrict__ t, Geom g, int upper, int quirk) {
     const int z = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y;
+    const int y = blockIdx.y, x = blockIdx.z;
     if (z >= g.nze) return;
     const int b = g.blen;
+    const bool xb = x < b || x >= g.nxe - b;
     const bool yb = y < b || y >= g.nye - b;
     const bool zb = upper ? (z < b) : (z < b || z >= g.nze - b);
-    if (upper && !zb) return;
+    if (upper ? !zb : !(xb || yb || zb)) return;
     const size_t plane = (size_t)g.nye * g.nze;
-    R *col = P + (size_t)y * g.nze + z;
+    const size_t o = ((size_t)x * g.nye + y) * g.nze + z;
+    const bool qcol = !upper && quirk && y >= g.nye - b && !zb;  // right y border, z interior
+    if (qcol && x < b) return;                                   // written by the thread of (blen, y, z)
     const R ty = yb ? (R)fac(t, b, g.nye, y) : (R)1;
     const R tz = zb ? (R)fac(t, b, g.nze, z) : (R)1;
-    // the x range that changes: the whole column if y or z is in a border, else the two x slabs
-    const bool whole = yb || zb;
-    const bool qcol = !upper && quirk && y >= g.nye - b && !zb;  // right y border, z interior
-    R face = 0;
-    if (qcol) face = col[(size_t)b * plane] * ty;  // (blen, y, z) after the right-face taper
-    for (int x = 0; x < g.nxe; ++x) {
-        const bool xb = x < b || x >= g.nxe - b;
-        if (!whole && !xb) { x = g.nxe - b - 1; continue; }
-        R v = col[(size_t)x * plane];
+    const R tx = xb ? (R)fac(t, b, g.nxe, x) : (R)1;
+    R v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (k < fs.n) v[k] = fs.f[k][o];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (k >= fs.n) break;
+        R w = v[k];
         if (xb && zb) {
-            if (yb) v = v * ty;
-            v = v * (R)fac(t, b, g.nxe, x);
-            v = v * tz;
+            if (yb) w = w * ty;
+            w = w * tx;
+            w = w * tz;
         } else if (yb && zb) {
-            v = v * ty;
-            v = v * tz;
+            w = w * ty;
+            w = w * tz;
         } else if (zb) {
-            v = v * tz;
+            w = w * tz;
         } else if (xb && yb) {
-            if (qcol && x < b) {
-                v = face * (R)fac(t, b, g.nxe, x);
-                v = v * ty;
-            } else {
-                v = v * (R)fac(t, b, g.nxe, x);
-                v = v * ty;
-            }
+            w = w * tx;
+            w = w * ty;
         } else if (yb) {
-            v = v * ty;
+            w = w * ty;
+            if (qcol && x == b) {  // the quirk cells of this column, from the raw P(blen, y, z)
+                R *c0 = fs.f[k] + (o - (size_t)b * plane);
+                for (int xq = 0; xq < b; ++xq) {
+                    R q = w * (R)fac(t, b, g.nxe, xq);
+                    q = q * ty;
+                    c0[(size_t)xq * plane] = q;
+                }
+            }
         } else {
-            v = v * (R)fac(t, b, g.nxe, x);
+            w = w * tx;
         }
-        col[(size_t)x * plane] = v;
+        fs.f[k][o] = w;
     }
 }
 
@@ -170,10 +187,15 @@ unsigned grid1d(size_t n) {
 }
 
 template <typename R>
-cudaError_t taper_t(R *P, const float *taper, const Geom &g, int upper, int quirk, cudaStream_t s) {
+cudaError_t taper_t(R *const *fields, int nf, const float *taper, const Geom &g, int upper, int quirk,
+                    cudaStream_t s) {
     if (g.blen <= 0) return cudaSuccess;
-    dim3 grid((g.nze + 127) / 128, g.nye);
-    taper_kernel<R><<<grid, 128, 0, s>>>(P, taper, g, upper, quirk);
+    if (g.nye > 65535 || g.nxe > 65535 || nf < 1 || nf > 4) return cudaErrorInvalidValue;
+    Fields<R> fs{};
+    fs.n = nf;
+    for (int k = 0; k < nf; ++k) fs.f[k] = fields[k];
+    dim3 grid((g.nze + 127) / 128, g.nye, g.nxe);
+    taper_kernel<R><<<grid, 128, 0, s>>>(fs, taper, g, upper, quirk);
     return cudaGetLastError();
 }
 
@@ -207,10 +229,14 @@ cudaError_t image_t(R *img, const R *ps, const R *pr, int z0, int z1, const Geom
 }  // namespace
 
 cudaError_t launch_taper(float *P, const float *taper, const Geom &g, int upper, int quirk, cudaStream_t s) {
-    return taper_t(P, taper, g, upper, quirk, s);
+    return taper_t(&P, 1, taper, g, upper, quirk, s);
 }
 cudaError_t launch_taper(double *P, const float *taper, const Geom &g, int upper, int quirk, cudaStream_t s) {
-    return taper_t(P, taper, g, upper, quirk, s);
+    return taper_t(&P, 1, taper, g, upper, quirk, s);
+}
+cudaError_t launch_taper_fields(float *const *fields, int nf, const float *taper, const Geom &g, int upper, int quirk,
+                                cudaStream_t s) {
+    return taper_t(fields, nf, taper, g, upper, quirk, s);
 }
 cudaError_t launch_source(float *PP, const float *wavelet, int it, int x, int y, int z, const Geom &g,
                           cudaStream_t s) {

@@ -19,6 +19,9 @@ struct RcvGeom {
 
 // taper3D / taperUpper3D in place (RTMCPUPlatform.cpp:566-920); upper != 0 for the upper form.
 cudaError_t launch_taper(float *P, const float *taper, const Geom &g, int upper, int quirk, cudaStream_t s);
+// The same on up to four fields of one geometry in one launch.
+cudaError_t launch_taper_fields(float *const *fields, int nf, const float *taper, const Geom &g, int upper, int quirk,
+                                cudaStream_t s);
 // PP[x, y, z] += wavelet[it] (padded coordinates; RTMCPUPlatform.cpp:103-113).
 cudaError_t launch_source(float *PP, const float *wavelet, int it, int x, int y, int z, const Geom &g,
                           cudaStream_t s);
