@@ -479,6 +479,8 @@ int rtmb_destroy(rtmb_ctx *ctx) {
         if (b) cudaFree(b);
     if (ctx->d_upb64) cudaFree(ctx->d_upb64);
     if (ctx->d_fq) cudaFree(ctx->d_fq);
+    for (float *b : ctx->d_fquirk)
+        if (b) cudaFree(b);
     for (cudaGraphExec_t g : ctx->gexec)
         if (g) cudaGraphExecDestroy(g);
     if (ctx->d_cells) cudaFree(ctx->d_cells);
@@ -873,6 +875,20 @@ int rtmb_migrate_shot_fmig(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz,
     a.V = ctx->d_v2dt2;
     a.taper_mode = rtmb::kTaperNone;
     a.sxe = -1;  // the source is a separate operator here (after the taper)
+    // Where the TMA step kernel runs, the fields stay tapered in HBM (StepArgs::tw): each step
+    // stores T(raw) of its new level and applies T to PP on load, which is the reference's
+    // "step, then taper P and PP in place" (the source and the receivers still come after it, as
+    // separate operators; no source or receiver lies in the quirk edge).  No taper launches.
+    const bool tw = tma_ok(ctx) && p.stencil_order <= 8 && ctx->nze % 4 == 0 && p.blen > 0 &&
+                    !(p.flags & RTMB_FLAG_NO_TAPER_STORE);
+    const size_t qn = quirk && p.blen > 0 ? (size_t)p.blen * (ctx->nze - 2 * p.blen) : 1;
+    if (tw) {
+        a.taper_mode = rtmb::kTaperAll;
+        a.tw = 1;
+        a.quirk = quirk && p.blen > 0;
+        for (float *&b : ctx->d_fquirk)
+            if ((rc = ensure(ctx, &b, qn > 0 ? qn : 1, false))) return rc;
+    }
     GraphScope graph(ctx, 3);
     if ((rc = graph.begin())) return rc;
     CK(cudaMemsetAsync(img, 0, ctx->n * sizeof(float), ctx->stream));
@@ -881,6 +897,8 @@ int rtmb_migrate_shot_fmig(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz,
         const int m = nw - gw < nws ? nw - gw : nws;
         float *Ps = ctx->d_w[0], *PPs = ctx->d_w[1], *Pr = ctx->d_w[2], *PPr = ctx->d_w[3];
         for (int k = 0; k < 4; ++k) CK(cudaMemsetAsync(ctx->d_w[k], 0, nb, ctx->stream));
+        if (tw)
+            for (float *b : ctx->d_fquirk) CK(cudaMemsetAsync(b, 0, (qn > 0 ? qn : 1) * sizeof(float), ctx->stream));
         CK(cudaMemsetAsync(ctx->d_fq, 0, 4 * (size_t)nws * ni * sizeof(float), ctx->stream));
         fs.nws = m;
         for (uint32_t st = 0; st < p.nt; ++st) {
@@ -889,10 +907,16 @@ int rtmb_migrate_shot_fmig(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz,
                 a.P = k ? Pr : Ps;
                 a.PP = k ? PPr : PPs;
                 a.it = (int)st;
+                if (tw && a.quirk) {  // side buffers of this wavefield, rotating over three levels
+                    a.quirk_in = ctx->d_fquirk[3 * k + (st + 1) % 3];
+                    a.quirk_out = ctx->d_fquirk[3 * k + st % 3];
+                }
                 LAUNCH_CAT(RTMB_PROF_FMIG_STEP, rtmb::launch_step(a, (int)p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
             }
-            float *tap[4] = {Ps, PPs, Pr, PPr};
-            LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_taper_fields(tap, 4, ctx->d_taper, g, 0, quirk, ctx->stream));
+            if (!tw) {
+                float *tap[4] = {Ps, PPs, Pr, PPr};
+                LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_taper_fields(tap, 4, ctx->d_taper, g, 0, quirk, ctx->stream));
+            }
             LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_source(PPs, ctx->d_wavelet, (int)st, (int)(sx + p.blen),
                                                             (int)(sy + p.blen), (int)(sz + p.blen), g, ctx->stream));
             LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_receivers(PPr, const_cast<float *>(rec) + (size_t)(rt / p.ntstep) * rchunk,

@@ -41,6 +41,7 @@ struct rtmb_ctx {
     // frequency-domain migration: the four frequency grids of a group, and their capacity in floats
     float *d_fq = nullptr;
     size_t fq_cap = 0;
+    float *d_fquirk[6] = {};  // taper side buffers of its two wavefields (stored-taper steps)
     bool capturing = false;
     // learned boundary closure (closure.cu): strip cells of the padded grid, parameters, and the
     // strip values of the next level computed before each step
