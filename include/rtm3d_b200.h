@@ -173,6 +173,19 @@ int rtmb_v2dt2_host(float *ve, size_t n, float dt);
 /* RTMPlatform::rtmStep (include/RTMPlatform.hpp:50-51), RTMSTEP_WRAPPER (kernel/gpu/rtmgpu.hpp:8-11):
  * PP <- 2P - PP + v2dt2 * lap(P) on [h, n-h)^3, h = order/2; PP updated in place. */
 int rtmb_step(rtmb_ctx *ctx, const float *P, float *PP, const float *v2dt2);
+/* RTMPlatform::rtmStepMultipleWave (RTMCPUPlatform.cpp:397-472): rtmb_step on two wavefields
+ * with the same v2dt2. */
+int rtmb_step_multiwave(rtmb_ctx *ctx, const float *P0, float *PP0, const float *P1, float *PP1, const float *v2dt2);
+/* RTMPlatform::rtmUpdateFreqContributions (RTMCPUPlatform.cpp:20-64): for frequency iw at time step
+ * it, slot lw of the frequency grids += kre/kim[iw][it] * PS / PR over the model interior.
+ * sre, sim, rre, rim: [nwstep][nx][ny][nz] (RTMGridCollection); kre, kim: [nw][nt] (RTMPlane);
+ * PS, PR: padded wavefields.  All device pointers. */
+int rtmb_fmig_update_freq(rtmb_ctx *ctx, uint32_t it, uint32_t iw, uint32_t lw, const float *PS, const float *PR,
+                          float *sre, float *sim, float *rre, float *rim, const float *kre, const float *kim);
+/* RTMPlatform::rtmFreqDomainImageCondition (RTMCPUPlatform.cpp:66-102): img += w2[iw] (sRe rRe -
+ * sIm rIm) over the model interior from slot lw; w2: the squared frequencies [nw] (device). */
+int rtmb_fmig_image_condition(rtmb_ctx *ctx, uint32_t iw, uint32_t lw, const float *w2, float *img, const float *sre,
+                              const float *sim, const float *rre, const float *rim);
 /* RTMPlatform::rtmTaperAllBorders / rtmTaperUpperBorders (RTMPlatform.hpp:35-42),
  * RTMTAPER_WRAPPER (rtmgpu.hpp:27-30); CPU taper semantics (RTMCPUPlatform.cpp:566-920). */
 int rtmb_taper_all_borders(rtmb_ctx *ctx, float *P);
@@ -250,6 +263,10 @@ int rtmb_migrate_shot_fmig(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz,
                            float fmax, uint32_t nwstep, float *img);
 /* nw of a frequency-domain migration (..._FreqDomain.cpp:133-137); 0 when there is none. */
 int rtmb_fmig_nw(float dt, uint32_t nt, float fmin, float fmax);
+/* Its tables, host arrays (..._FreqDomain.cpp:17-51, :151-152): w2[nw] = w^2 and kre/kim[nw][nt]
+ * = cos/sin(w it), w = 2 pi (fmin + iw df) dt; the inputs of rtmb_fmig_update_freq and
+ * rtmb_fmig_image_condition once copied to the device. */
+int rtmb_fmig_tables(float dt, uint32_t nt, float fmin, float fmax, float *w2, float *kre, float *kim);
 
 /* rtmb_migrate_shot that ADDS the shot's image to a caller-owned FP64 stack (padded, device)
  * instead of writing an FP32 image: the shot stacking of RTMAcousticController.cpp:223-242 with an

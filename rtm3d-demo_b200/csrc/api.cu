@@ -528,6 +528,31 @@ int rtmb_step(rtmb_ctx *ctx, const float *P, float *PP, const float *v2dt2) {
     return RTMB_OK;
 }
 
+int rtmb_step_multiwave(rtmb_ctx *ctx, const float *P0, float *PP0, const float *P1, float *PP1, const float *v2dt2) {
+    // RTMCPUPlatform.cpp:397-472: both wavefields, the same v2dt2, each the single-wave step's arithmetic
+    int rc = rtmb_step(ctx, P0, PP0, v2dt2);
+    return rc ? rc : rtmb_step(ctx, P1, PP1, v2dt2);
+}
+
+int rtmb_fmig_update_freq(rtmb_ctx *ctx, uint32_t it, uint32_t iw, uint32_t lw, const float *PS, const float *PR,
+                          float *sre, float *sim, float *rre, float *rim, const float *kre, const float *kim) {
+    if (!ctx || !PS || !PR || !sre || !sim || !rre || !rim || !kre || !kim)
+        return fail(ctx, RTMB_EINVAL, "rtmb_fmig_update_freq: null pointer");
+    if (it >= ctx->p.nt) return fail(ctx, RTMB_EINVAL, "rtmb_fmig_update_freq: time step out of range");
+    LAUNCH(rtmb::launch_fmig_update(PS, PR, sre, sim, rre, rim, kre, kim, (int)it, (int)iw, (int)lw, (int)ctx->p.nt,
+                                    geom(ctx), (int)ctx->p.nx, (int)ctx->p.ny, (int)ctx->p.nz, ctx->stream));
+    return RTMB_OK;
+}
+
+int rtmb_fmig_image_condition(rtmb_ctx *ctx, uint32_t iw, uint32_t lw, const float *w2, float *img, const float *sre,
+                              const float *sim, const float *rre, const float *rim) {
+    if (!ctx || !w2 || !img || !sre || !sim || !rre || !rim)
+        return fail(ctx, RTMB_EINVAL, "rtmb_fmig_image_condition: null pointer");
+    LAUNCH(rtmb::launch_fmig_image(img, sre, sim, rre, rim, w2, (int)iw, (int)lw, geom(ctx), (int)ctx->p.nx,
+                                   (int)ctx->p.ny, (int)ctx->p.nz, ctx->stream));
+    return RTMB_OK;
+}
+
 int rtmb_taper_all_borders(rtmb_ctx *ctx, float *P) {
     if (!ctx || !P) return fail(ctx, RTMB_EINVAL, "rtmb_taper_all_borders: null pointer");
     LAUNCH(rtmb::launch_taper(P, ctx->d_taper, geom(ctx), 0, !(ctx->p.flags & RTMB_FLAG_NO_TAPER_QUIRK), ctx->stream));
@@ -808,6 +833,25 @@ int rtmb_fmig_nw(float dt, uint32_t nt, float fmin, float fmax) {
     const float df = (float)(1. / ((nt * 1.0) * dt));
     const float nf = ((fmax - fmin) / df);
     return nf > 0.f ? (int)(size_t)nf : 0;
+}
+
+namespace {
+void fmig_tables(const rtmb_params &p, float fmin, int nw, std::vector<float> &w2, std::vector<float> &kre,
+                 std::vector<float> &kim);
+}  // namespace
+
+int rtmb_fmig_tables(float dt, uint32_t nt, float fmin, float fmax, float *w2, float *kre, float *kim) {
+    if (!w2 || !kre || !kim) return RTMB_EINVAL;
+    rtmb_params p{};
+    p.dt = dt;
+    p.nt = nt;
+    const int nw = rtmb_fmig_nw(dt, nt, fmin, fmax);
+    std::vector<float> a, b, c;
+    fmig_tables(p, fmin, nw, a, b, c);
+    std::memcpy(w2, a.data(), a.size() * sizeof(float));
+    std::memcpy(kre, b.data(), b.size() * sizeof(float));
+    std::memcpy(kim, c.data(), c.size() * sizeof(float));
+    return RTMB_OK;
 }
 
 namespace {

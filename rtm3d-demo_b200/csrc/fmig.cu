@@ -105,7 +105,54 @@ __global__ void __launch_bounds__(128) fmig_freq4_kernel(const float *__restrict
     *reinterpret_cast<float4 *>(img + o) = make_float4(im[0], im[1], im[2], im[3]);
 }
 
+// The reference's two per-frequency operators as they are (the per-operator entry points): one
+// frequency lw of the grids, table values read on the device at [iw][it] and [iw].
+__global__ void fmig_update_kernel(const float *__restrict__ ps, const float *__restrict__ pr, float *sre, float *sim,
+                                   float *rre, float *rim, const float *__restrict__ kre,
+                                   const float *__restrict__ kim, size_t kofs, size_t fofs, Geom g, int nx, int ny,
+                                   int nz) {
+    const int z = blockIdx.x * blockDim.x + threadIdx.x;
+    if (z >= nz) return;
+    const int y = blockIdx.y, x = blockIdx.z;
+    const size_t o = ((size_t)(x + g.blen) * g.nye + (y + g.blen)) * g.nze + (z + g.blen);
+    const size_t f = fofs + ((size_t)x * ny + y) * nz + z;
+    const float kr = kre[kofs], ki = kim[kofs], s = ps[o], r = pr[o];
+    sre[f] = sre[f] + (kr * s);
+    sim[f] = sim[f] + (ki * s);
+    rre[f] = rre[f] + (kr * r);
+    rim[f] = rim[f] + (ki * r);
+}
+
+__global__ void fmig_image_kernel(float *img, const float *__restrict__ sre, const float *__restrict__ sim,
+                                  const float *__restrict__ rre, const float *__restrict__ rim,
+                                  const float *__restrict__ w2, int iw, size_t fofs, Geom g, int nx, int ny, int nz) {
+    const int z = blockIdx.x * blockDim.x + threadIdx.x;
+    if (z >= nz) return;
+    const int y = blockIdx.y, x = blockIdx.z;
+    const size_t o = ((size_t)(x + g.blen) * g.nye + (y + g.blen)) * g.nze + (z + g.blen);
+    const size_t f = fofs + ((size_t)x * ny + y) * nz + z;
+    img[o] = img[o] + (w2[iw]) * (sre[f] * rre[f] - sim[f] * rim[f]);
+}
+
 }  // namespace
+
+cudaError_t launch_fmig_update(const float *ps, const float *pr, float *sre, float *sim, float *rre, float *rim,
+                               const float *kre, const float *kim, int it, int iw, int lw, int nt, const Geom &g,
+                               int nx, int ny, int nz, cudaStream_t s) {
+    if (nx <= 0 || ny <= 0 || nz <= 0 || ny > 65535 || nx > 65535) return cudaErrorInvalidValue;
+    dim3 grid((nz + 127) / 128, ny, nx);
+    fmig_update_kernel<<<grid, 128, 0, s>>>(ps, pr, sre, sim, rre, rim, kre, kim, (size_t)iw * nt + it,
+                                            (size_t)lw * nx * ny * nz, g, nx, ny, nz);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fmig_image(float *img, const float *sre, const float *sim, const float *rre, const float *rim,
+                              const float *w2, int iw, int lw, const Geom &g, int nx, int ny, int nz, cudaStream_t s) {
+    if (nx <= 0 || ny <= 0 || nz <= 0 || ny > 65535 || nx > 65535) return cudaErrorInvalidValue;
+    dim3 grid((nz + 127) / 128, ny, nx);
+    fmig_image_kernel<<<grid, 128, 0, s>>>(img, sre, sim, rre, rim, w2, iw, (size_t)lw * nx * ny * nz, g, nx, ny, nz);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_fmig_freq(const float *ps, const float *pr, float *img, float *fq, const FmigStep &f, const Geom &g,
                              int nx, int ny, int nz, bool exact, cudaStream_t s) {

@@ -49,6 +49,14 @@ struct FmigStep {
 };
 cudaError_t launch_fmig_freq(const float *ps, const float *pr, float *img, float *fq, const FmigStep &f, const Geom &g,
                              int nx, int ny, int nz, bool exact, cudaStream_t s);
+// The reference's per-frequency operators one by one (RTMCPUPlatform.cpp:20-64 and :66-102): the
+// DFT update of frequency iw into slot lw of the grids ([nws][nx][ny][nz]) from kre/kim[iw][it]
+// ([nw][nt]), and img += w2[iw] (sRe rRe - sIm rIm) from slot lw.
+cudaError_t launch_fmig_update(const float *ps, const float *pr, float *sre, float *sim, float *rre, float *rim,
+                               const float *kre, const float *kim, int it, int iw, int lw, int nt, const Geom &g,
+                               int nx, int ny, int nz, cudaStream_t s);
+cudaError_t launch_fmig_image(float *img, const float *sre, const float *sim, const float *rre, const float *rim,
+                              const float *w2, int iw, int lw, const Geom &g, int nx, int ny, int nz, cudaStream_t s);
 
 // FP64 overloads of the operators above, for the FP64 GPU oracle (same operator sequence and
 // multiply order, double arithmetic).

@@ -102,6 +102,10 @@ SYMBOLS = [
     ("rtmb_migrate_shot_acc64", [_vp, _u32, _u32, _u32, _vp, _vp], C.c_int),
     ("rtmb_migrate_shot_fmig", [_vp, _u32, _u32, _u32, _vp, C.c_float, C.c_float, _u32, _vp], C.c_int),
     ("rtmb_fmig_nw", [C.c_float, _u32, C.c_float, C.c_float], C.c_int),
+    ("rtmb_fmig_tables", [C.c_float, _u32, C.c_float, C.c_float, _vp, _vp, _vp], C.c_int),
+    ("rtmb_step_multiwave", [_vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
+    ("rtmb_fmig_update_freq", [_vp, _u32, _u32, _u32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
+    ("rtmb_fmig_image_condition", [_vp, _u32, _u32, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
     ("rtmb_model_shot_f64", [_vp, _u32, _u32, _u32, _vp], C.c_int),
     ("rtmb_migrate_shot_f64", [_vp, _u32, _u32, _u32, _vp, _vp], C.c_int),
     ("rtmb_closure_param_count", [], C.c_int),
@@ -269,6 +273,17 @@ class Context:
     def migrate_shot(self, sx, sy, sz, rec, img):
         self._check(self.L.rtmb_migrate_shot(self.h, sx, sy, sz, _ptr(rec), _ptr(img)))
 
+    def step_multiwave(self, P0, PP0, P1, PP1, v2dt2):
+        self._check(self.L.rtmb_step_multiwave(self.h, _ptr(P0), _ptr(PP0), _ptr(P1), _ptr(PP1), _ptr(v2dt2)))
+
+    def fmig_update_freq(self, it, iw, lw, ps, pr, sre, sim, rre, rim, kre, kim):
+        self._check(self.L.rtmb_fmig_update_freq(self.h, it, iw, lw, _ptr(ps), _ptr(pr), _ptr(sre), _ptr(sim),
+                                                  _ptr(rre), _ptr(rim), _ptr(kre), _ptr(kim)))
+
+    def fmig_image_condition(self, iw, lw, w2, img, sre, sim, rre, rim):
+        self._check(self.L.rtmb_fmig_image_condition(self.h, iw, lw, _ptr(w2), _ptr(img), _ptr(sre), _ptr(sim),
+                                                      _ptr(rre), _ptr(rim)))
+
     def migrate_shot_fmig(self, sx, sy, sz, rec, img, fmin, fmax, nwstep=0):
         """Frequency-domain RTM of one shot into img (padded, device, float32, overwritten)."""
         self._check(self.L.rtmb_migrate_shot_fmig(self.h, sx, sy, sz, _ptr(rec), fmin, fmax, nwstep, _ptr(img)))
@@ -359,6 +374,17 @@ def ricker(nt, dt, fpeak):
 def fmig_nw(dt: float, nt: int, fmin: float, fmax: float) -> int:
     """Number of frequencies of a frequency-domain migration (0 when there is none)."""
     return int(load().rtmb_fmig_nw(dt, nt, fmin, fmax))
+
+
+def fmig_tables(dt: float, nt: int, fmin: float, fmax: float):
+    """(w2[nw], kre[nw][nt], kim[nw][nt]) of a frequency-domain migration."""
+    np = _np()
+    nw = fmig_nw(dt, nt, fmin, fmax)
+    w2 = np.zeros(max(nw, 1), np.float32)
+    kre = np.zeros((max(nw, 1), nt), np.float32)
+    kim = np.zeros((max(nw, 1), nt), np.float32)
+    load().rtmb_fmig_tables(dt, nt, fmin, fmax, w2.ctypes.data, kre.ctypes.data, kim.ctypes.data)
+    return w2[:nw], kre[:nw], kim[:nw]
 
 
 def prepare_velocity(v, blen: int, bc: str, seed: int = -1):

@@ -91,3 +91,13 @@ def test_fmig_frequency_count(oracle, nt, dt, fmin, fmax):
     """The library's nw of a frequency-domain migration is the oracle's (the reference's float mix)."""
     import rtmb
     assert rtmb.fmig_nw(dt, nt, fmin, fmax) == oracle.L.orc_fmig_nw(nt, dt, fmin, fmax)
+
+
+def test_fmig_tables(oracle):
+    """The library's DFT tables of a frequency-domain migration are the oracle's bit for bit."""
+    import rtmb
+    for args in ((120, 0.001, 5.0, 40.0), (90, 0.0012, 2.0, 30.0)):
+        got = rtmb.fmig_tables(args[1], args[0], args[2], args[3])
+        ref = oracle.fmig_tables(*args)
+        for a, b in zip(got, ref):
+            assert bitexact(a, b)

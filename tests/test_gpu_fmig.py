@@ -105,3 +105,36 @@ def test_fmig_errors(cuda, oracle):
         with pytest.raises(rtmb.RtmbError) as e:
             ctx.migrate_shot_fmig(case["sx"], case["sy"], case["sz"], r, img, fmin, fmax)
         assert e.value.code == rtmb.RTMB_EINVAL
+
+
+def test_fmig_per_operator_sequence_matches_driver(cuda, oracle):
+    """The platform operators an adapter binds (rtmStepMultipleWave, the taper, the source, the
+    receivers, rtmUpdateFreqContributions, rtmFreqDomainImageCondition), called through the C ABI
+    in the reference's order, give the fused driver's image bit for bit."""
+    import torch
+    case, p, v2, rec = setup(oracle, "golden")
+    band = BANDS["golden"]
+    want, ctx = fmig_gpu(case, v2, rec, band, cuda)
+    w2, kre, kim = (dev(a, cuda) for a in rtmb.fmig_tables(case["dt"], case["nt"], *band))
+    nw = w2.numel()
+    v = dev(v2, cuda)
+    shp = ctx.padded_shape
+    Ps, PPs, Pr, PPr = (torch.zeros(shp, dtype=torch.float32, device=cuda) for _ in range(4))
+    fq = [torch.zeros((nw, case["nx"], case["ny"], case["nz"]), dtype=torch.float32, device=cuda) for _ in range(4)]
+    img = torch.zeros(shp, dtype=torch.float32, device=cuda)
+    r = dev(rec, cuda)
+    nt, ntstep = case["nt"], case["ntstep"]
+    for st in range(nt):
+        rt = nt - 1 - st
+        ctx.step_multiwave(Ps, PPs, Pr, PPr, v)
+        for f in (Ps, PPs, Pr, PPr):
+            ctx.taper_all(f)
+        ctx.apply_source(PPs, case["sx"], case["sy"], case["sz"], st)
+        ctx.restore_receivers(PPr, r[rt // ntstep], rt % ntstep)
+        for iw in range(nw):
+            ctx.fmig_update_freq(st, iw, iw, PPs, PPr, *fq, kre, kim)
+            ctx.fmig_image_condition(iw, iw, w2, img, *fq)
+        Ps, PPs = PPs, Ps
+        Pr, PPr = PPr, Pr
+    ctx.sync()
+    assert bitexact(img.cpu().numpy(), want)
