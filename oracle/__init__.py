@@ -81,6 +81,7 @@ class Oracle:
             ("orc_model_shot", [C.POINTER(OrcParams), _fp, _fp], C.c_int),
             ("orc_migrate_hbc", [C.POINTER(OrcParams), _fp, _fp, _fp], C.c_int),
             ("orc_migrate_rbc", [C.POINTER(OrcParams), _fp, _fp, _fp], C.c_int),
+            ("orc_step2d", [C.c_int] * 5 + [_fp, _fp, _fp, _fp], C.c_int),
             ("orc_fmig_nw", [C.c_int, C.c_float, C.c_float, C.c_float], C.c_int),
             ("orc_fmig_tables", [C.c_int, C.c_float, C.c_float, C.c_float, C.c_int, _fp, _fp, _fp], None),
             ("orc_migrate_fmig", [C.POINTER(OrcParams), _fp, _fp, C.c_float, C.c_float, C.c_int, _fp], C.c_int),
@@ -127,6 +128,11 @@ class Oracle:
     def step(self, order, coefs, P, PP, v2dt2):
         PP = PP.copy()
         nan = self.L.orc_step(*P.shape, order, fptr(coefs), fptr(P), fptr(PP), fptr(v2dt2))
+        return PP, nan
+
+    def step2d(self, order, coefs, P, PP, v2dt2, blen):
+        PP = PP.copy()
+        nan = self.L.orc_step2d(*P.shape, blen, order, fptr(coefs), fptr(P), fptr(PP), fptr(v2dt2))
         return PP, nan
 
     def taper(self, g, blen, taper, upper=False):

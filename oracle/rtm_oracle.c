@@ -279,6 +279,32 @@ int orc_step(int nxe, int nye, int nze, int order, const float *coefs,
     return nan;
 }
 
+/* S/src/platform/host/RTMCPUPlatform.cpp:191-256 (rtmStep2D; rtmStep picks it when nx == 1, :474-490):
+ * only the plane x = blen, the y and z terms of the Laplacian, lapl = acmy + acmz. */
+int orc_step2d(int nxe, int nye, int nze, int blen, int order, const float *coefs,
+               const float *P, float *PP, const float *v2dt2) {
+    const int h = order / 2, ix = blen;
+    const float *cy = coefs + (order + 1), *cz = coefs + 2 * (order + 1);
+    int nan = 0;
+    (void)nxe;
+#pragma omp parallel for collapse(2) reduction(| : nan)
+    for (int iy = h; iy < nye - h; iy++)
+        for (int iz = h; iz < nze - h; iz++) {
+            float acmy = 0.0f, acmz = 0.0f, lapl;
+            for (int io = 0; io <= order; io++) {
+                acmy += P[IDX(ix, iy - h + io, iz)] * cy[io];
+                acmz += P[IDX(ix, iy, iz - h + io)] * cz[io];
+            }
+            lapl = acmy + acmz;
+            size_t o = IDX(ix, iy, iz);
+            float pp = PP[o], p = P[o], v = v2dt2[o];
+            float npp = 2 * p - pp + (v)*lapl;
+            PP[o] = npp;
+            if (npp != npp || p != p || pp != pp || lapl != lapl) nan = 1;
+        }
+    return nan;
+}
+
 /* S/src/platform/host/RTMCPUPlatform.cpp:710-920 (taper3D).  The six loops run in the
  * reference's order; the "front-right" x-y edge reads its value from x = blen (:901), which
  * the left/right loop has already tapered. */
@@ -515,6 +541,12 @@ static void loop_free(loopctx *c) { free(c->taper); free(c->wavelet); }
 
 #define SWAP(a, b) do { float *t_ = a; a = b; b = t_; } while (0)
 
+/* rtmStep of the loops: the 2D form for nx == 1 (RTMCPUPlatform.cpp:474-490). */
+static int step(const orc_params *p, const loopctx *c, const float *P, float *PP, const float *v2dt2) {
+    if (p->nx == 1) return orc_step2d(c->nxe, c->nye, c->nze, p->blen, p->order, c->coefs, P, PP, v2dt2);
+    return orc_step(c->nxe, c->nye, c->nze, p->order, c->coefs, P, PP, v2dt2);
+}
+
 /* S/src/kernel/RTMFiniteDifferencesKernel.cpp:129-246 (rtmAcousticFiniteDiffModeling). */
 int orc_model_shot(const orc_params *p, const float *v2dt2, float *rec) {
     loopctx c;
@@ -530,7 +562,7 @@ int orc_model_shot(const orc_params *p, const float *v2dt2, float *rec) {
             SWAP(P, PP);
             orc_taper_all(c.nxe, c.nye, c.nze, p->blen, c.taper, P);
             orc_taper_all(c.nxe, c.nye, c.nze, p->blen, c.taper, PP);
-            nan |= orc_step(c.nxe, c.nye, c.nze, p->order, c.coefs, P, PP, v2dt2);
+            nan |= step(p, &c, P, PP, v2dt2);
             orc_apply_source(c.nxe, c.nye, c.nze, sx, sy, sz, c.wavelet[it], PP);
             orc_save_receivers(p, lt, PP, rchunk);
         }
@@ -552,7 +584,7 @@ static int forward(const orc_params *p, loopctx *c, const float *v2dt2, int hbc,
             orc_taper_upper(c->nxe, c->nye, c->nze, p->blen, c->taper, P);
             orc_taper_upper(c->nxe, c->nye, c->nze, p->blen, c->taper, PP);
         }
-        nan |= orc_step(c->nxe, c->nye, c->nze, p->order, c->coefs, P, PP, v2dt2);
+        nan |= step(p, c, P, PP, v2dt2);
         orc_apply_source(c->nxe, c->nye, c->nze, sx, sy, sz, c->wavelet[it], PP);
         if (hbc) orc_save_upb(c->nxe, c->nye, c->nze, p->blen, c->h, it, PP, upb);
     }
@@ -578,7 +610,7 @@ static int backward(const orc_params *p, loopctx *c, const float *v2dt2, int hbc
             if (it == p->nt - 1) memcpy(PP, snap1, c->n * sizeof(float));
             else if (it == p->nt - 2) memcpy(PP, snap0, c->n * sizeof(float));
             else {
-                nan |= orc_step(c->nxe, c->nye, c->nze, p->order, c->coefs, P, PP, v2dt2);
+                nan |= step(p, c, P, PP, v2dt2);
                 if (hbc) orc_restore_upb(c->nxe, c->nye, c->nze, p->blen, c->h, it, PP, upb);
             }
             SWAP(P, PP);
@@ -586,7 +618,7 @@ static int backward(const orc_params *p, loopctx *c, const float *v2dt2, int hbc
                 orc_taper_upper(c->nxe, c->nye, c->nze, p->blen, c->taper, PR);
                 orc_taper_upper(c->nxe, c->nye, c->nze, p->blen, c->taper, PPR);
             }
-            nan |= orc_step(c->nxe, c->nye, c->nze, p->order, c->coefs, PR, PPR, v2dt2);
+            nan |= step(p, c, PR, PPR, v2dt2);
             orc_restore_receivers(p, lt, PPR, rchunk);
             orc_image(c->nxe, c->nye, c->nze, p->blen, img, P, PPR);
             SWAP(PR, PPR);
@@ -686,8 +718,8 @@ int orc_migrate_fmig(const orc_params *p, const float *v2dt2, const float *rec, 
             const float *rchunk = rec + (size_t)(itstep / p->ntstep) * chunk;
             for (int lt = p->ntstep - 1; lt >= 0; --lt) {
                 const int rt = itstep + lt, st = p->nt - 1 - rt;
-                nan |= orc_step(nxe, nye, nze, p->order, c.coefs, P, PP, v2dt2);
-                nan |= orc_step(nxe, nye, nze, p->order, c.coefs, PR, PPR, v2dt2);
+                nan |= step(p, &c, P, PP, v2dt2);
+                nan |= step(p, &c, PR, PPR, v2dt2);
                 orc_taper_all(nxe, nye, nze, b, c.taper, P);
                 orc_taper_all(nxe, nye, nze, b, c.taper, PP);
                 orc_taper_all(nxe, nye, nze, b, c.taper, PR);

@@ -46,6 +46,9 @@ void orc_v2dt2(float *v, size_t n, float dt);
 /* per-step operators */
 int orc_step(int nxe, int nye, int nze, int order, const float *coefs,
              const float *P, float *PP, const float *v2dt2);
+/* the 2D step (nx == 1): plane x = blen only, no x term */
+int orc_step2d(int nxe, int nye, int nze, int blen, int order, const float *coefs,
+               const float *P, float *PP, const float *v2dt2);
 void orc_taper_all(int nxe, int nye, int nze, int blen, const float *taper, float *g);
 void orc_taper_upper(int nxe, int nye, int nze, int blen, const float *taper, float *g);
 void orc_apply_source(int nxe, int nye, int nze, int x, int y, int z, float val, float *PP);

@@ -31,7 +31,7 @@ def reference():
 def golden():
     import numpy as np
     d = os.path.join(os.path.dirname(__file__), "golden")
-    return {n: dict(np.load(os.path.join(d, n + ".npz"))) for n in ("model_abc", "mig_hbc", "mig_rbc", "mig_fmig", "ops")}
+    return {n: dict(np.load(os.path.join(d, n + ".npz"))) for n in ("model_abc", "mig_hbc", "mig_rbc", "mig_fmig", "ops", "twod")}
 
 
 @pytest.fixture(scope="session")

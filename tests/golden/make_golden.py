@@ -7,10 +7,11 @@ The reference CPU program (oracle/_ref/RTM3D.bin, built from the reference's sou
   * mig_hbc.npz    -- HBC migration image (RTMIMG file) with the extended velocity it used (vpe)
   * mig_rbc.npz    -- RBC migration image with its extended velocity
   * mig_fmig.npz   -- frequency-domain RTM image (fmig = true) with its extended velocity
+  * twod.npz       -- 2D model (nx = 1): record, HBC / RBC / fmig images and a 2D step vector
   * ops.npz        -- per-operator vectors from the reference CPU platform (oracle/_ref/librtmref.so)
 
 Run:  python tests/golden/make_golden.py [names...]   (needs oracle/_ref, i.e. the reference sources;
-      names: model mig ops fmig, default all)
+      names: model mig ops fmig twod, default all)
 """
 from __future__ import annotations
 
@@ -77,7 +78,38 @@ def fmig_fixture(case: dict, rec: np.ndarray, wd: str):
                         fmin=FMIG["fmig_min_freq"], fmax=FMIG["fmig_max_freq"])
 
 
-def main(names=("model", "mig", "ops", "fmig")):
+def twod_fixture(wd_root: str):
+    """2D models (nx = 1; the reference's rtmStep2D): modeling record, HBC / RBC / fmig images with
+    the extended velocities they used, and a per-operator 2D step vector."""
+    case = dict(CASES["golden"], nx=1, sx=0, rsx=0, rcx=1, rdx=1)
+    out = {}
+    with tempfile.TemporaryDirectory(dir=wd_root) as wd:
+        rec = read_record(run_reference(case, "model", wd))
+        out["rec"] = rec
+        for name, bc, extra in (("hbc", "hbc", None), ("rbc", "rbc", None),
+                                ("fmig", "hbc", dict(fmig=True, **FMIG))):
+            for f in glob.glob(os.path.join(wd, "out", "RTMIMG_*")):
+                os.remove(f)
+            dm = run_reference(case, bc, wd, vpe_path=os.path.join(wd, f"vpe2d_{name}.bin"), extra=extra)
+            out[f"img_{name}"] = np.fromfile(glob.glob(os.path.join(wd, "out", "RTMIMG_*"))[0], np.float32).reshape(
+                1, case["ny"], case["nz"])
+            out[f"vpe_{name}"] = np.fromfile(dm["vpefile"], np.float32).reshape(
+                1 + 2 * case["blen"], case["ny"] + 2 * case["blen"], case["nz"] + 2 * case["blen"])
+    R = Reference()
+    rng = np.random.default_rng(17)
+    ny, nz, b = 12, 9, 6
+    shp = (1 + 2 * b, ny + 2 * b, nz + 2 * b)
+    P = rng.standard_normal(shp).astype(np.float32)
+    PP = rng.standard_normal(shp).astype(np.float32)
+    V = (rng.random(shp) * 0.1).astype(np.float32)
+    out.update(P=P, PP=PP, V=V)
+    for order in (4, 8):
+        out[f"step{order}"], _ = R.step(1, ny, nz, b, order, 10.0, 12.5, 7.5, P, PP, V)
+    out.update(fmin=FMIG["fmig_min_freq"], fmax=FMIG["fmig_max_freq"])
+    np.savez_compressed(os.path.join(HERE, "twod.npz"), **out)
+
+
+def main(names=("model", "mig", "ops", "fmig", "twod")):
     if not os.path.exists(REF_BIN):
         raise SystemExit("oracle/_ref/RTM3D.bin missing: run `make -C oracle ref` first")
     rng = np.random.default_rng(7)
@@ -89,6 +121,8 @@ def main(names=("model", "mig", "ops", "fmig")):
             np.savez_compressed(os.path.join(HERE, "model_abc.npz"), rec=rec)
         if "fmig" in names:
             fmig_fixture(case, rec, wd)
+        if "twod" in names:
+            twod_fixture(wd)
         for bc in ("hbc", "rbc") if "mig" in names else ():
             for f in glob.glob(os.path.join(wd, "out", "RTMIMG_*")):
                 os.remove(f)
@@ -128,4 +162,4 @@ def main(names=("model", "mig", "ops", "fmig")):
 
 
 if __name__ == "__main__":
-    main(tuple(sys.argv[1:]) or ("model", "mig", "ops", "fmig"))
+    main(tuple(sys.argv[1:]) or ("model", "mig", "ops", "fmig", "twod"))

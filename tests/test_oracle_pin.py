@@ -106,6 +106,49 @@ def test_fmig_vs_reference_program(oracle):
     assert bitexact(fin, want.reshape(fin.shape))
 
 
+def twod_case():
+    """The golden case as a 2D model (nx = 1): the reference runs rtmStep2D on the plane x = blen."""
+    return dict(CASES["golden"], nx=1, sx=0, rsx=0, rcx=1, rdx=1)
+
+
+def test_twod_vs_golden(oracle, golden):
+    g = golden["twod"]
+    for order in (4, 8):
+        c = oracle.stencil_coefs(order, 10.0, 12.5, 7.5)
+        out, nan = oracle.step2d(order, c, g["P"], g["PP"], g["V"], 6)
+        assert nan == 0
+        assert bitexact(out, g[f"step{order}"]), order
+    case = twod_case()
+    p = oracle_params(case)
+    ve = oracle.extend_init_borders(layered_model(case), case["blen"], "abc")
+    rec, rc = oracle.model_shot(p, oracle.v2dt2(ve, case["dt"]))
+    assert rc == 0 and bitexact(rec, g["rec"])
+    for name in ("hbc", "rbc", "fmig"):
+        v2 = oracle.v2dt2(g[f"vpe_{name}"], case["dt"])
+        if name == "fmig":
+            img, rc = oracle.migrate_fmig(p, v2, g["rec"], float(g["fmin"]), float(g["fmax"]))
+        else:
+            img, rc = oracle.migrate(p, v2, g["rec"], name)
+        assert rc == 0
+        fin = oracle.filter_remove(img, case["blen"], case["dx"], case["dy"], case["dz"])
+        assert np.abs(fin).max() > 0
+        assert bitexact(fin, g[f"img_{name}"]), name
+
+
+def test_step2d_vs_reference_build(oracle, reference):
+    rng = np.random.default_rng(5)
+    for (ny, nz, b, order) in ((11, 17, 5, 6), (16, 10, 8, 12)):
+        shp = (1 + 2 * b, ny + 2 * b, nz + 2 * b)
+        P = rng.standard_normal(shp).astype(np.float32)
+        PP = rng.standard_normal(shp).astype(np.float32)
+        V = (rng.random(shp) * 0.1).astype(np.float32)
+        c = oracle.stencil_coefs(order, 9.0, 11.0, 13.0)
+        ref, rc = reference.step(1, ny, nz, b, order, 9.0, 11.0, 13.0, P, PP, V)
+        got, nan = oracle.step2d(order, c, P, PP, V, b)
+        assert rc == 0 and nan == 0
+        assert bitexact(got, ref)
+
+
 def test_ops_vs_reference_build(oracle, reference):
     rng = np.random.default_rng(123)
     for (nx, ny, nz, b, order) in ((13, 11, 17, 5, 6), (9, 16, 10, 8, 16)):
