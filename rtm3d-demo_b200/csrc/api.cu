@@ -114,6 +114,12 @@ rtmb::StepArgs base_args(const rtmb_ctx *c) {
         a.cz[i] = c->coefs[2 * (o + 1) + i];
         a.iso &= a.cx[i] == a.cy[i] && a.cx[i] == a.cz[i] && c->coefs[i] == c->coefs[o - i];
     }
+    if (c->p.nx == 1) {  // RTMCPUPlatform.cpp:191-256 (rtmStep2D): the plane x = blen, no x term
+        for (int i = 0; i <= o; ++i) a.cx[i] = 0.f;
+        a.iso = 0;
+        a.x_lo = (int)c->p.blen;
+        a.x_hi = (int)c->p.blen + 1;
+    }
     a.taper = c->d_taper;
     a.wavelet = c->d_wavelet;
     a.sxe = a.sye = a.sze = -1;
@@ -759,7 +765,8 @@ int migrate_impl(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const flo
     rcv.inj_dev = st ? ctx->d_inj : nullptr;
     const int rmode = (p.flags & RTMB_FLAG_RCV_ADD) ? rtmb::kRecAdd : rtmb::kRecOverwrite;
     // FP32 FMA form: the source and receiver steps of one time step in one launch
-    const bool dual = !st && !exact(ctx) && p.stencil_order == 8 && tma_ok(ctx) && !(p.flags & RTMB_FLAG_NO_DUAL);
+    const bool dual = !st && !exact(ctx) && p.stencil_order == 8 && tma_ok(ctx) && !(p.flags & RTMB_FLAG_NO_DUAL) &&
+                      p.nx > 1;
     for (int it = (int)p.nt - 1; it >= 0; --it) {
         if (dual && it < (int)p.nt - 2) {
             src.P = s_cur; src.PP = s_prev; src.it = it;
@@ -1063,8 +1070,8 @@ int rtmb_migrate_batch(rtmb_ctx *ctx, uint32_t nshots, const rtmb_shot *shots, d
     if (!ctx || !shots || !stack) return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: null pointer");
     const rtmb_params &p = ctx->p;
     if (nshots == 0 || nshots > 12) return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: 1 to 12 shots per batch");
-    if (p.boundary != RTMB_BC_RBC || p.stencil_order != 8 || (int)p.blen < ctx->h)
-        return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: boundary RBC, stencil_order 8 and blen >= 4");
+    if (p.boundary != RTMB_BC_RBC || p.stencil_order != 8 || (int)p.blen < ctx->h || p.nx == 1)
+        return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: boundary RBC, stencil_order 8, blen >= 4, 3D (nx > 1)");
     const bool st = ctx->store != rtmb::kStoreF32;
     const size_t es = st ? 2 : 4;
     const bool img64 = st;  // the 16-bit forms stack through an FP64 shot image, FP32 through FP32

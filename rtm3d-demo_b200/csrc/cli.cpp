@@ -24,8 +24,8 @@
 //              src/process/RTMAcousticProcess.cpp:16-18), fmig_nwstep frequencies per pass over
 //              time as the reference's accelerator builds take it (0: all in one pass, the CPU
 //              build's order).
-// Out of scope and rejected: distributed_grid and fmig_distributed_imaging (MPI partitions) and
-// 2D models (nx == 1).
+// 2D models (nx == 1) run the reference's 2D step (the plane x = blen, no x term).
+// Out of scope and rejected: distributed_grid and fmig_distributed_imaging (MPI partitions).
 #include <algorithm>
 #include <cctype>
 #include <chrono>
@@ -155,7 +155,6 @@ Param load_param(const std::string &path) {
     if (p.fmig && p.fmig_distributed_imaging)
         throw Error("[ fmig_distributed_imaging (MPI partition of the image) is not supported: one GPU holds the volume ]");
     if (p.distributed_grid) throw Error("[ distributed_grid (MPI halo decomposition) is not supported: one GPU holds the volume ]");
-    if (p.nx == 1) throw Error("[ 2D models (nx == 1) are not supported by this build ]");
     return p;
 }
 

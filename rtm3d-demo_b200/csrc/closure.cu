@@ -761,8 +761,8 @@ int rtmb_closure_set(rtmb_ctx *ctx, const float *params, float min_scale, float 
     if (!ctx || !params || !(min_scale >= 0.f) || !(damp >= 0.f && damp < 1.f)) return RTMB_EINVAL;
     ctx->closure_min_scale = min_scale;
     ctx->closure_damp = damp;
-    if (ctx->p.boundary != RTMB_BC_LEARNED || ctx->p.blen != (uint32_t)kStrip) {
-        ctx->err = "rtmb_closure_set: the context needs boundary RTMB_BC_LEARNED and blen 8";
+    if (ctx->p.boundary != RTMB_BC_LEARNED || ctx->p.blen != (uint32_t)kStrip || ctx->p.nx == 1) {
+        ctx->err = "rtmb_closure_set: the context needs boundary RTMB_BC_LEARNED, blen 8 and a 3D model";
         return RTMB_EINVAL;
     }
     if (cudaSetDevice(ctx->device) != cudaSuccess) return RTMB_ECUDA;
@@ -799,8 +799,8 @@ int rtmb_closure_collect(rtmb_ctx *wide, uint32_t sx, uint32_t sy, uint32_t sz, 
     if (!wide || !X || !R || !count || !tstride || !per_step) return RTMB_EINVAL;
     rtmb_ctx *ctx = wide;
     const rtmb_params &p = ctx->p;
-    if (p.blen < (uint32_t)kStrip + 8) {
-        ctx->err = "rtmb_closure_collect: the wide context's border must be wider than the 8-cell strip";
+    if (p.blen < (uint32_t)kStrip + 8 || p.nx == 1) {
+        ctx->err = "rtmb_closure_collect: a 3D wide context whose border is wider than the 8-cell strip";
         return RTMB_EINVAL;
     }
     int rc = rtmb::driver::check_model_shot(ctx, sx, sy, sz);

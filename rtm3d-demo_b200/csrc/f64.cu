@@ -112,6 +112,7 @@ int check64(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz) {
         return fail64(ctx, RTMB_EINVAL, "Invalid Source Position: (%u,%u,%u)", sx, sy, sz);
     if (!ctx->d_v2dt2) return fail64(ctx, RTMB_EINVAL, "no velocity loaded (rtmb_load_v2dt2)");
     if ((int)p.blen < ctx->h) return fail64(ctx, RTMB_EINVAL, "the per-shot drivers need blen >= stencil_order/2");
+    if (p.nx == 1) return fail64(ctx, RTMB_EINVAL, "the FP64 oracle runs 3D models only (nx > 1)");
     if (p.receiver_count_x > p.nx || p.receiver_count_y > p.ny)
         return fail64(ctx, RTMB_EINVAL, "Invalid Receiver Grid Size");
     if (p.receiver_depth_z + p.blen >= (uint32_t)ctx->nze - ctx->h)

@@ -93,6 +93,9 @@ struct StepArgs {
     float inj;                  // bound on |values| written by injection (source, receivers, border)
     const float *inj_dev;       // optional device scalar added to inj
     int iso;                    // cx == cy == cz, symmetric: the FMA form may use the packed symmetric sum
+    // 2D models (nx == 1, the reference's rtmStep2D): computed planes restricted to [x_lo, x_hi)
+    // when x_hi > 0, with the x coefficients zero (so lap = acmy + acmz exactly)
+    int x_lo, x_hi;
 };
 
 // Exponent of a produced level: the smallest e with bound * 2^-e < 2^15.  bound is

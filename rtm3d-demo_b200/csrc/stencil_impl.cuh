@@ -30,8 +30,12 @@ __global__ void __launch_bounds__(kThreads, 2) step_kernel(const __grid_constant
     const int yt0 = H + blockIdx.y * kTY;
     const int z0 = zt0 + tz * kVZ;
     const int y = yt0 + ty;
-    const int xc0 = H + blockIdx.z * a.chunk;
-    const int xc1 = min(xc0 + a.chunk, a.nxe - H);
+    int xc0 = H + blockIdx.z * a.chunk;
+    int xc1 = min(xc0 + a.chunk, a.nxe - H);
+    if (a.x_hi > 0) {  // 2D models: the plane x = blen only
+        xc0 = max(xc0, a.x_lo);
+        xc1 = min(xc1, a.x_hi);
+    }
     if (xc0 >= xc1) return;
     const size_t plane = (size_t)a.nye * a.nze;
     const bool row_ok = y < a.nye;

@@ -295,8 +295,12 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
     const int yt0 = H + by * kTY;
     const int z0 = zt0 + tz * kVZ;
     const int y = yt0 + ty;
-    const int xc0 = H + bz * a.chunk;
-    const int xc1 = min(xc0 + a.chunk, a.nxe - H);
+    int xc0 = H + bz * a.chunk;
+    int xc1 = min(xc0 + a.chunk, a.nxe - H);
+    if (a.x_hi > 0) {  // 2D models: the plane x = blen only
+        xc0 = max(xc0, a.x_lo);
+        xc1 = min(xc1, a.x_hi);
+    }
     if (xc0 >= xc1) return;
     const int n = xc1 - xc0;        // output planes, local index i <-> x = xc0 + i
     const int nplanes = n + 2 * H;  // P planes, local index k <-> x = xc0 - H + k

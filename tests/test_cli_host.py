@@ -67,7 +67,6 @@ def test_missing_key(base):
     (dict(fmig=True, fmig_min_freq=30.0, fmig_max_freq=20.0), "fmig_max_freq must be greater"),
     (dict(fmig=True, fmig_distributed_imaging=True), "fmig_distributed_imaging"),
     (dict(distributed_grid=True), "distributed_grid"),
-    (dict(nx=1), "nx == 1"),
 ])
 def test_rejected_modes(base, patch, expect):
     d, tmp = base

@@ -84,6 +84,25 @@ def test_cli_fmig_matches_reference_file(cuda, golden, tmp_path):
     assert bitexact(img, g["img"])
 
 
+def test_cli_twod_matches_reference_files(cuda, golden, tmp_path):
+    """A 2D model (nx = 1) through the CLI: the .seism chunks and the HBC RTMIMG file equal the
+    reference program's (tests/golden/twod.npz)."""
+    case = dict(CASES["golden"], nx=1, sx=0, rsx=0, rcx=1, rdx=1)
+    tmp = str(tmp_path)
+    vp = os.path.join(tmp, "vel.bin")
+    layered_model(case).tofile(vp)
+    d = input_json(case, vpfile=vp, workdir=tmp)
+    d.update(modeling=True, migration=False)
+    run_cli(d, tmp)
+    g = golden["twod"]
+    assert bitexact(read_record(d, case["sx"], case["sy"], case["sz"]), g["rec"])
+    g["vpe_hbc"].astype(np.float32).tofile(d["vpefile"])
+    d.update(modeling=False, migration=True, boundary_condition="hbc", load_vpe_from_file=True)
+    run_cli(d, tmp)
+    img = np.fromfile(glob.glob(os.path.join(d["outdir"], "RTMIMG_*"))[0], np.float32).reshape(1, case["ny"], case["nz"])
+    assert bitexact(img, g["img_hbc"])
+
+
 def test_cli_several_shots_overlapped_io_matches_library(cuda, oracle, tmp_path):
     import torch
     case = CASES["golden"]
