@@ -610,30 +610,47 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                 const bool yb = signbit(tyv);
                 const float4 tz4 = *reinterpret_cast<const float4 *>(tab + S::SROWS + ZH + tz * kVZ);
                 const bool qx = ALL && a.quirk && x < a.blen && y >= a.nye - a.blen;
+                // the cases are uniform per thread, so each runs its own unrolled loop; cells
+                // outside the computed region are tapered too (harmless: they keep their stored
+                // value on output)
+                if (qx) {  // rare: planes x < blen, rows on the right y border
 #pragma unroll
-                for (int e = 0; e < kVZ; ++e) {
-                    if (!((vmask >> e) & 1u)) continue;
-                    const int z = z0 + e;
-                    float pp = ppv[e];
-                    if (qx && z >= a.blen && z < a.nze - a.blen) {
-                        // the x = blen redirect, twice: from the raw u(blen, y, z) of PP's level
-                        pp = a.quirk_in[(size_t)(y - (a.nye - a.blen)) * (a.nze - 2 * a.blen) + (z - a.blen)];
-                        if (SC) pp = pp * sPPinv;  // the side buffer holds values, not stored units
-                        pp = pp * fy;
-                        pp = pp * fy;
-                        pp = pp * fx;
-                        pp = pp * fy;
-                    } else if (ALL && !xb) {  // fx = 1: T(v) = (v fy) fz
+                    for (int e = 0; e < kVZ; ++e) {
+                        const int z = z0 + e;
+                        float pp = ppv[e];
+                        if (((vmask >> e) & 1u) && z >= a.blen && z < a.nze - a.blen) {
+                            // the x = blen redirect, twice: from the raw u(blen, y, z) of PP's level
+                            pp = a.quirk_in[(size_t)(y - (a.nye - a.blen)) * (a.nze - 2 * a.blen) + (z - a.blen)];
+                            if (SC) pp = pp * sPPinv;  // the side buffer holds values, not stored units
+                            pp = pp * fy;
+                            pp = pp * fy;
+                            pp = pp * fx;
+                            pp = pp * fy;
+                        } else {
+                            float f1, f2, f3;
+                            taper_factors3<ALL>(fx, fy, fabsf(get(tz4, e)), xb, yb, signbit(get(tz4, e)), f1, f2, f3);
+                            pp = ((pp * f1) * f2) * f3;
+                            if (!TWS) pp = ((pp * f1) * f2) * f3;
+                        }
+                        ppv[e] = pp;
+                    }
+                } else if (ALL && !xb) {  // fx = 1: T(v) = (v fy) fz
+#pragma unroll
+                    for (int e = 0; e < kVZ; ++e) {
                         const float fz = fabsf(get(tz4, e));
-                        pp = (pp * fy) * fz;
+                        float pp = (ppv[e] * fy) * fz;
                         if (!TWS) pp = (pp * fy) * fz;
-                    } else {
+                        ppv[e] = pp;
+                    }
+                } else {
+#pragma unroll
+                    for (int e = 0; e < kVZ; ++e) {
                         float f1, f2, f3;
                         taper_factors3<ALL>(fx, fy, fabsf(get(tz4, e)), xb, yb, signbit(get(tz4, e)), f1, f2, f3);
-                        pp = ((pp * f1) * f2) * f3;
+                        float pp = ((ppv[e] * f1) * f2) * f3;
                         if (!TWS) pp = ((pp * f1) * f2) * f3;
+                        ppv[e] = pp;
                     }
-                    ppv[e] = pp;
                 }
             }
             float npp[kVZ];
