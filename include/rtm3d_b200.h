@@ -86,11 +86,12 @@ typedef enum rtmb_boundary {
 /* With a storage flag: accumulate the image over the time steps in FP64 (the caller's FP32 image
  * is written from it at the end of the shot). */
 #define RTMB_FLAG_IMG_F64       0x100u
-/* FP32 migration in the FMA form runs the backward source and receiver steps of each time step as
- * ONE launch (both wavefields and the image in one pass over the grid: 36 instead of 44 bytes per
+/* FP32 RBC migration in the FMA form runs the backward source and receiver steps of each time step
+ * as ONE launch (both wavefields and the image in one pass over the grid: 36 instead of 44 bytes per
  * point) when stencil_order is 8 and rows are 16-byte aligned; same results as two launches (no
  * reference counterpart: the reference runs them as separate operators).  This flag keeps the two
- * launches.  The exact form keeps two launches: in one it is issue-bound and gains nothing. */
+ * launches.  The exact form and HBC migration (whose receiver steps taper the upper border) keep
+ * two launches: there one launch gained nothing or lost. */
 #define RTMB_FLAG_NO_DUAL       0x200u
 /* Modeling (every face tapered) keeps the wavefields tapered in HBM between time steps: each step
  * stores T(u) of its new level instead of u, so the next step reads its input without a taper pass

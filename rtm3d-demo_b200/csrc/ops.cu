@@ -17,7 +17,7 @@ struct Fields {
     int n;
 };
 
-// One thread per cell, z fastest (grid: z blocks, y, x), for every field of fs: the cell's loads
+// One thread per cell, z fastest (grid: z blocks, y blocks, x), for every field of fs: the cell's loads
 // of the fields are independent, so they are in flight together.  Cells off every tapered border
 // leave at once.  The front-right quirk of taper3D (a cell (x < blen, y >= nye - blen, z off the z
 // borders) takes ((P(blen, y, z) ty) tx) ty, RTMCPUPlatform.cpp:900-904) needs the raw
@@ -27,8 +27,8 @@ struct Fields {
 template <typename R>
 __global__ void taper_kernel(Fields<R> fs, const float *__restrict__ t, Geom g, int upper, int quirk) {
     const int z = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y, x = blockIdx.z;
-    if (z >= g.nze) return;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y, x = blockIdx.z;
+    if (z >= g.nze || y >= g.nye) return;
     const int b = g.blen;
     const bool xb = x < b || x >= g.nxe - b;
     const bool yb = y < b || y >= g.nye - b;
@@ -194,8 +194,13 @@ cudaError_t taper_t(R *const *fields, int nf, const float *taper, const Geom &g,
     Fields<R> fs{};
     fs.n = nf;
     for (int k = 0; k < nf; ++k) fs.f[k] = fields[k];
-    dim3 grid((g.nze + 127) / 128, g.nye, g.nxe);
-    taper_kernel<R><<<grid, 128, 0, s>>>(fs, taper, g, upper, quirk);
+    // threads over the z range that can change (the whole row, or z < blen for the upper form),
+    // several y rows per block when that range is short
+    const int zr = upper ? (g.blen < g.nze ? g.blen : g.nze) : g.nze;
+    const int bx = zr >= 128 ? 128 : ((zr + 31) / 32) * 32;
+    const int by = 256 / bx;
+    dim3 block(bx, by), grid((zr + bx - 1) / bx, (g.nye + by - 1) / by, g.nxe);
+    taper_kernel<R><<<grid, block, 0, s>>>(fs, taper, g, upper, quirk);
     return cudaGetLastError();
 }
 

@@ -119,9 +119,9 @@ cudaError_t launch_step(const StepArgs &a, int order, bool exact, cudaStream_t s
 // (args[0]'s are used).  At most 12 shots.
 cudaError_t launch_step_batch(const StepArgs *args, int nshots, int order, bool exact, cudaStream_t s);
 
-// The dual-wavefield backward step: src advances the reconstructed source wavefield (no taper,
-// optional upper-border restore), rcv the receiver wavefield with its taper, receiver injection and
-// the image of the new source values (rcv.ps is not read).  One launch instead of two; FP32, order 8,
+// The dual-wavefield backward step of RBC migration: src advances the reconstructed source
+// wavefield, rcv the receiver wavefield with its receiver injection and the image of the new source
+// values (rcv.ps is not read); neither is tapered.  One launch instead of two; FP32, order 8,
 // TMA-aligned volumes, rcv.chunk x planes per CTA (64 x 8 tiles).
 bool dual_step_supported(const StepArgs &src, const StepArgs &rcv, int order);
 cudaError_t launch_dual_step(const StepArgs &src, const StepArgs &rcv, int order, bool exact, cudaStream_t s);

@@ -40,7 +40,7 @@ bool dual_step_supported(const StepArgs &src, const StepArgs &rcv, int order) {
                          reinterpret_cast<uintptr_t>(rcv.V) | reinterpret_cast<uintptr_t>(rcv.img);
     return order == 8 && rcv.nze % 4 == 0 && al % 16 == 0 && src.store == kStoreF32 && rcv.store == kStoreF32 &&
            !rcv.img64 && rcv.img && src.taper_mode == kTaperNone &&
-           (rcv.taper_mode == kTaperNone || rcv.taper_mode == kTaperUpper) && src.V == rcv.V &&
+           rcv.taper_mode == kTaperNone && src.upb_mode == kUpbNone && src.V == rcv.V &&
            (rcv.rec_mode == kRecOverwrite || rcv.rec_mode == kRecAdd || rcv.rec_mode == kRecNone) &&
            dual_encoder() != nullptr;
 }

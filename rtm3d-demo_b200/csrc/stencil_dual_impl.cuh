@@ -28,8 +28,8 @@ struct DualMaps {
 };
 
 struct DualArgs {
-    StepArgs s;  // the source step (no taper; upper-border restore for HBC)
-    StepArgs r;  // the receiver step (taper, receiver injection, image)
+    StepArgs s;  // the source step (no taper)
+    StepArgs r;  // the receiver step (receiver injection, image; no taper)
 };
 
 template <int H>
@@ -56,28 +56,17 @@ __device__ __forceinline__ void dual_consumer(const StepArgs &a, const StepArgs 
                                               uint64_t *pempty, uint64_t *cfull, uint64_t *cempty, uint64_t *xfull,
                                               uint64_t *xempty, int tid, int zt0, int yt0, int xc0, int n) {
     using S = DualShape<H>;
-    constexpr int ZH = S::ZH, SPITCH = S::SPITCH, STAGE = S::STAGE, STRIDE = S::STRIDE, D = S::D, R = S::R,
+    constexpr int ZH = S::ZH, SPITCH = S::SPITCH, STRIDE = S::STRIDE, D = S::D, R = S::R,
                   E = S::E, CSLOT = S::CSLOT, CORE = S::CORE;
     constexpr int NQ = 2 * H + 1;
     constexpr int ZQ = kTZ / kVZ;
     constexpr bool RCV = ROLE == 1;
-    constexpr int TP = RCV ? TAPER : kTaperNone;
-    constexpr bool CB = TP != kTaperNone;  // named barrier 2 among the receiver warps
+    static_assert(TAPER == kTaperNone, "the dual step has no taper form (HBC runs two launches)");
     const int lane = tid & 31;
     const int tz = tid % ZQ, ty = tid / ZQ;
     const int z0 = zt0 + tz * kVZ;
     const int y = yt0 + ty;
     const size_t plane = (size_t)a.nye * a.nze;
-
-    auto group_sync = [&]() { asm volatile("bar.sync 2, %0;" ::"n"(kGThreads) : "memory"); };
-    auto group_sync_or = [&](bool v) {
-        uint32_t out;
-        asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, 2, %2, p;\n selp.u32 %0, 1, 0, q;\n}\n"
-                     : "=r"(out)
-                     : "r"((uint32_t)v), "n"(kGThreads)
-                     : "memory");
-        return out != 0;
-    };
 
     const bool row_ok = y < a.nye && z0 < a.nze;
     const bool y_ok = y < a.nye - H;
@@ -99,9 +88,6 @@ __device__ __forceinline__ void dual_consumer(const StepArgs &a, const StepArgs 
         }
     }
     const bool special = rec_e >= 0 || umask != 0;
-    bool tile_taper_yz = false;
-    if (TP == kTaperUpper) tile_taper_yz = (zt0 - ZH < a.blen);
-    const bool pp_taper_yz = TP == kTaperUpper && z0 < a.blen;
     const size_t row_off = (size_t)y * a.nze + z0;
     float *PPp = a.PP + row_off;
     const int col = ZH + tz * kVZ;
@@ -115,19 +101,6 @@ __device__ __forceinline__ void dual_consumer(const StepArgs &a, const StepArgs 
         __syncwarp();
         if (lane == 0) mbar_arrive(bar);
     };
-    auto taper_stage = [&](int k, int slot) {  // receiver form with the upper taper only
-        if (!tile_taper_yz) return;
-        const int x = xc0 - H + k;
-        float *st = const_cast<float *>(pring) + slot * STRIDE;
-        for (int c = tid; c < STAGE; c += kGThreads) {
-            const int r = c / SPITCH, cc = c % SPITCH;
-            const int yy = yt0 - H + r, zz = zt0 - ZH + cc;
-            if (yy >= a.nye || zz < 0 || zz >= a.nze) continue;
-            st[c] = taper_once(st[c], x, yy, zz, a);
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        group_sync();
-    };
 
     float4 q[NQ];
     float nanacc = 0.f;
@@ -140,9 +113,8 @@ __device__ __forceinline__ void dual_consumer(const StepArgs &a, const StepArgs 
     int s_in = (2 * H) % D, ph_in = ((2 * H) / D) & 1, s_mid = H % D, s_core = 0, ph_core = 0, s_x = 0, ph_x = 0;
     for (int k = 0; k < 2 * H; ++k) {
         wait_p(k, 0);
-        if (CB) taper_stage(k, k);
     }
-    if (CB ? group_sync_or(bad_wait) : bad_wait) goto drain;
+    if (bad_wait) goto drain;
 #pragma unroll
     for (int k = 0; k < 2 * H; ++k) q[k + 1] = ld_f4(pring + k * STRIDE + (ty + H) * SPITCH + col);
 #pragma unroll
@@ -153,7 +125,6 @@ __device__ __forceinline__ void dual_consumer(const StepArgs &a, const StepArgs 
                            s_core = s_core + 1 == R ? (ph_core ^= 1, 0) : s_core + 1,
                            s_x = s_x + 1 == E ? (ph_x ^= 1, 0) : s_x + 1) {
         const int x = xc0 + i;
-        const int kin = i + 2 * H;
         // the record value this plane injects, loaded now so that its latency overlaps the stencil
         const float *rec_p = nullptr;
         float rec_v = 0.f;
@@ -166,12 +137,7 @@ __device__ __forceinline__ void dual_consumer(const StepArgs &a, const StepArgs 
         }
         wait_p(s_in, ph_in);
         const float *s = pring + s_mid * STRIDE;
-        if constexpr (CB) {
-            if (group_sync_or(bad_wait)) goto drain;
-            taper_stage(kin, s_in);
-        } else if (bad_wait) {
-            goto drain;
-        }
+        if (bad_wait) goto drain;
 #pragma unroll
         for (int k = 0; k < NQ - 1; ++k) q[k] = q[k + 1];
         q[NQ - 1] = ld_f4(pring + s_in * STRIDE + (ty + H) * SPITCH + col);
@@ -241,7 +207,6 @@ __device__ __forceinline__ void dual_consumer(const StepArgs &a, const StepArgs 
         // core tiles of plane x
         if (!__all_sync(0xffffffffu, mbar_wait(&cfull[s_core], ph_core))) {
             bad_wait = true;
-            if (CB) continue;
             goto drain;
         }
         const unsigned char *ct = cring + s_core * CSLOT;
@@ -253,7 +218,6 @@ __device__ __forceinline__ void dual_consumer(const StepArgs &a, const StepArgs 
         // the exchange slot of plane x: the source warps fill it, the receiver warps read it
         if (!__all_sync(0xffffffffu, mbar_wait(RCV ? &xfull[s_x] : &xempty[s_x], RCV ? ph_x : (ph_x ^ 1)))) {
             bad_wait = true;
-            if (CB) continue;
             goto drain;
         }
         float4 ps4 = pp_raw;
@@ -263,14 +227,6 @@ __device__ __forceinline__ void dual_consumer(const StepArgs &a, const StepArgs 
         if (row_ok) {
             const float4 qc = q[H];
             float ppv[kVZ] = {pp_raw.x, pp_raw.y, pp_raw.z, pp_raw.w};
-            if (TP == kTaperUpper && pp_taper_yz) {
-#pragma unroll
-                for (int e = 0; e < kVZ; ++e) {
-                    if (!((vmask >> e) & 1u)) continue;
-                    const int z = z0 + e;
-                    ppv[e] = taper_once(taper_once(ppv[e], x, y, z, a), x, y, z, a);
-                }
-            }
             float npp[kVZ];
 #pragma unroll
             for (int e = 0; e < kVZ; ++e) {
@@ -410,7 +366,7 @@ cudaError_t launch_dual_h(const DualMaps &maps, const DualArgs &d, bool exact, i
     static unsigned long long attr_done[4] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    const int variant = (exact ? 2 : 0) + (taper == kTaperUpper ? 1 : 0);
+    const int variant = exact ? 1 : 0;
     auto run = [&](void (*kern)(DualMaps, DualArgs)) -> cudaError_t {
         const unsigned long long bit = 1ull << (dev & 63);
         if (!(attr_done[variant] & bit)) {
@@ -421,9 +377,8 @@ cudaError_t launch_dual_h(const DualMaps &maps, const DualArgs &d, bool exact, i
         kern<<<grid, kDualThreads, DualShape<H>::SMEM, s>>>(maps, d);
         return cudaGetLastError();
     };
-    if (taper != kTaperNone && taper != kTaperUpper) return cudaErrorInvalidValue;
-    if (exact) return taper ? run(dual_step_kernel<H, true, kTaperUpper>) : run(dual_step_kernel<H, true, kTaperNone>);
-    return taper ? run(dual_step_kernel<H, false, kTaperUpper>) : run(dual_step_kernel<H, false, kTaperNone>);
+    if (taper != kTaperNone) return cudaErrorInvalidValue;
+    return exact ? run(dual_step_kernel<H, true, kTaperNone>) : run(dual_step_kernel<H, false, kTaperNone>);
 }
 
 }  // namespace detail
