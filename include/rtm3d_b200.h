@@ -93,12 +93,13 @@ typedef enum rtmb_boundary {
  * launches.  The exact form and HBC migration (whose receiver steps taper the upper border) keep
  * two launches: there one launch gained nothing or lost. */
 #define RTMB_FLAG_NO_DUAL       0x200u
-/* Modeling (every face tapered) keeps the wavefields tapered in HBM between time steps: each step
- * stores T(u) of its new level instead of u, so the next step reads its input without a taper pass
- * (T: the reference's taper3D, RTMCPUPlatform.cpp:710-920; the same products of per-axis factors in
- * the same order, so the record is bit-identical).  Taken when the TMA step kernel runs
- * (stencil_order <= 8, rows 16-byte aligned, no RTMB_FLAG_NO_TMA); this flag keeps the raw fields
- * and tapers on load (no reference counterpart). */
+/* Modeling (every face tapered) and HBC migration (the upper border tapered) keep the wavefields
+ * tapered in HBM between time steps: each step stores T(u) of its new level instead of u, so the
+ * next step reads its input without a taper pass (T: the reference's taper3D / taperUpper3D,
+ * RTMCPUPlatform.cpp:566-920; the same products of per-axis factors in the same order, so records
+ * and images are bit-identical).  Taken when the TMA step kernel runs (stencil_order <= 8, rows
+ * 16-byte aligned, no RTMB_FLAG_NO_TMA); this flag keeps the raw fields and tapers on load (no
+ * reference counterpart). */
 #define RTMB_FLAG_NO_TAPER_STORE 0x400u
 
 /* The input.json parameters on the path (include/RTMParam.hpp:188-249). */

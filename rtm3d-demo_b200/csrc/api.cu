@@ -325,10 +325,13 @@ int rtmb::driver::run_forward(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t 
     // taper-all runs keep the fields tapered in HBM (StepArgs::tw) when the TMA kernel runs; a hook
     // reads the fields between steps, so it gets the raw form, and so does a gathered record with a
     // receiver in the taper region (where the stored T(u) is not u)
-    const bool tw = taper_mode == rtmb::kTaperAll && !hook && tma_ok(ctx) && p.stencil_order <= 8 &&
-                    ctx->nze % 4 == 0 && !(p.flags & RTMB_FLAG_NO_TAPER_STORE) &&
-                    (!gather || receivers_untapered(ctx));
-    a.tw = tw ? 1 : 0;
+    const bool tw_ok = !hook && tma_ok(ctx) && p.stencil_order <= 8 && ctx->nze % 4 == 0 &&
+                       !(p.flags & RTMB_FLAG_NO_TAPER_STORE);
+    const bool tw = taper_mode == rtmb::kTaperAll && tw_ok && (!gather || receivers_untapered(ctx));
+    a.tw = tw ? rtmb::kTwStored : 0;
+    // HBC migration's forward pass (upper taper): the same, except that the last two levels, the
+    // snapshots the backward pass starts from, are stored raw (the last step tapers its P on load)
+    const bool tw_up = taper_mode == rtmb::kTaperUpper && tw_ok && !st;
     for (uint32_t it = 0; it < p.nt; ++it) {
         std::swap(P, PP);
         std::swap(scP, scPP);
@@ -341,6 +344,8 @@ int rtmb::driver::run_forward(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t 
         if (rec && !gather) set_receivers(a, ctx, rtmb::kRecSample, rec, (int)it);
         if (upb) { a.upb_mode = rtmb::kUpbSave; a.upb = upb + (size_t)it * upb_step; }
         if (quirk) { a.quirk_in = ctx->d_quirk[(it + 1) % 3]; a.quirk_out = ctx->d_quirk[it % 3]; }
+        if (tw_up)
+            a.tw = it + 1 < p.nt ? (rtmb::kTwStored | (it + 2 == p.nt ? rtmb::kTwRawOut : 0)) : rtmb::kTwPPOnce;
         int rc;
         if (hook && (rc = hook->before((int)it, P, PP))) return rc;
         LAUNCH_CAT(cat, rtmb::launch_step(a, (int)p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
@@ -757,6 +762,11 @@ int migrate_impl(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const flo
     rtmb::StepArgs rcv = base_args(ctx);
     rcv.V = ctx->d_v2dt2;
     rcv.taper_mode = hbc ? rtmb::kTaperUpper : rtmb::kTaperNone;
+    // HBC: the receiver wavefield stays tapered in HBM (the image takes the raw new level in the
+    // step; nothing reads the receiver fields afterwards)
+    if (hbc && !st && tma_ok(ctx) && p.stencil_order <= 8 && ctx->nze % 4 == 0 &&
+        !(p.flags & RTMB_FLAG_NO_TAPER_STORE) && reinterpret_cast<uintptr_t>(img) % 16 == 0)
+        rcv.tw = rtmb::kTwStored;
     rcv.img = static_cast<float *>(img);
     rcv.img64 = img64;
     rcv.img_z0 = full ? 0 : (int)p.blen;

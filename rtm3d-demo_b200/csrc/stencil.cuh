@@ -28,8 +28,15 @@ constexpr int kVZ = 4;       // z-points per thread
 constexpr int kThreads = (kTZ / kVZ) * kTY;  // 256
 constexpr int kMaxOrder = 16;
 
-// kTaperAllStored: kTaperAll with the fields stored tapered (StepArgs::tw), a kernel form only.
-enum TaperMode : int { kTaperNone = 0, kTaperUpper = 1, kTaperAll = 2, kTaperAllStored = 3 };
+// kTaperAllStored / kTaperUpperStored: kTaperAll / kTaperUpper with the fields stored tapered
+// (StepArgs::tw), kernel forms only.
+enum TaperMode : int { kTaperNone = 0, kTaperUpper = 1, kTaperAll = 2, kTaperAllStored = 3, kTaperUpperStored = 4 };
+// StepArgs::tw bits.  kTwStored: P and PP hold T(u) (the taper of the raw level u) instead of u,
+// the launch applies T once more to PP and stores T(u_new); kTwRawOut: with kTwStored, store u_new
+// raw (a driver's last levels); kTwPPOnce: without kTwStored (P raw, tapered on load), PP holds
+// T(u) and takes T once.  The same products of the same factors in the same order as the taper
+// on load, so the results are bit-identical.
+enum TwBits : int { kTwStored = 1, kTwRawOut = 2, kTwPPOnce = 4 };
 // How P, PP and ps are stored in HBM.  The 16-bit forms hold value * 2^-e in the 16-bit type, with
 // one power-of-two exponent e per stored time level (ScaleRec); all arithmetic stays FP32.
 enum StoreType : int { kStoreF32 = 0, kStoreF16 = 1, kStoreBF16 = 2 };
@@ -59,10 +66,8 @@ struct StepArgs {
     int taper_mode;             // TaperMode
     int quirk;                  // front-right x-y edge reads x = blen (taper3D, :901)
     const float *quirk_in;      // [blen][nze-2blen]: raw PP(blen, nye-blen+j, blen+k) of this PP
-    // taper-all launches of the TMA kernel: P and PP hold T(u) (the taper of the raw level u)
-    // instead of u, and the launch stores T(u_new); the quirk cells of the new level are written
-    // by the CTA of plane blen.  The same products of the same factors in the same order as the
-    // taper on load, so the results are bit-identical.
+    // TwBits (taper launches of the TMA kernel only; 0 elsewhere).  Taper-all: the quirk cells of
+    // a stored level are written by the CTA of plane blen.
     int tw;
     float *quirk_out;           // same, receives PP_new(blen, ...)
     // source: PP[sxe,sye,sze] += wavelet[it]

@@ -255,8 +255,8 @@ __device__ __forceinline__ void taper_tile(T *st, const float *tab, const StepAr
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-// TAPER: kTaperNone / kTaperUpper / kTaperAll (raw fields, tapered on load) / kTaperAllStored
-// (every face tapered, the fields stored tapered: no pass over the P tile, no consumer barrier).
+// TAPER: kTaperNone / kTaperUpper / kTaperAll (raw P, tapered on load) / kTaperUpperStored /
+// kTaperAllStored (the fields stored tapered: no pass over the P tile, no consumer barrier).
 // IMG: the epilogue accumulates the image.
 // T: storage type of P, PP and ps (float: the FP32 form, bit-identical to the plain-load kernel;
 // __half / __nv_bfloat16: scaled 16-bit storage).  IT: image type (float or double).
@@ -269,9 +269,10 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
     using S = TmaShape<H, IMG, T, IT>;
     using ST = Stor<T>;
     constexpr bool SC = ST::kScaled;
-    // ALL: every face tapered (kTaperAll, kTaperAllStored); TWS: the fields are stored tapered
+    // ALL: every face tapered; UPPER: the upper border only; TWS: the fields are stored tapered
     constexpr bool ALL = TAPER == kTaperAll || TAPER == kTaperAllStored;
-    constexpr bool TWS = TAPER == kTaperAllStored;
+    constexpr bool UPPER = TAPER == kTaperUpper || TAPER == kTaperUpperStored;
+    constexpr bool TWS = TAPER == kTaperAllStored || TAPER == kTaperUpperStored;
     // CB: the consumers meet at named barriers (taper passes), so a timed-out wait must be seen by
     // all of them at the next barrier instead of one warp leaving alone
     constexpr bool CB = TAPER == kTaperUpper || TAPER == kTaperAll;
@@ -315,7 +316,7 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
         if (i >= 0 && i < n_ax) {
             bool in;
             f = taper_factor(a.taper, a.blen, n_ax, i, in);
-            if (TAPER == kTaperUpper && !row) in = i < a.blen;
+            if (UPPER && !row) in = i < a.blen;
             if (in) f = -f;
         }
         tab[tid] = f;
@@ -404,11 +405,11 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
     if (ALL)
         tile_taper_yz = (yt0 - H < a.blen) || (yt0 + kTY + H > a.nye - a.blen) || (zt0 - ZH < a.blen) ||
                         (zt0 + kTZ + ZH > a.nze - a.blen);
-    if (TAPER == kTaperUpper) tile_taper_yz = (zt0 - ZH < a.blen);
+    if (UPPER) tile_taper_yz = (zt0 - ZH < a.blen);
     bool pp_taper_yz = false;    // are this thread's own cells in the y or z taper region?
     if (ALL)
         pp_taper_yz = (y < a.blen) || (y >= a.nye - a.blen) || (z0 < a.blen) || (z0 + kVZ > a.nze - a.blen);
-    if (TAPER == kTaperUpper) pp_taper_yz = z0 < a.blen;
+    if (UPPER) pp_taper_yz = z0 < a.blen;
     const size_t row_off = (size_t)y * a.nze + z0;
     T *PPp = reinterpret_cast<T *>(a.PP) + row_off;
     const int col = ZH + tz * kVZ;
@@ -610,6 +611,7 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                 const bool yb = signbit(tyv);
                 const float4 tz4 = *reinterpret_cast<const float4 *>(tab + S::SROWS + ZH + tz * kVZ);
                 const bool qx = ALL && a.quirk && x < a.blen && y >= a.nye - a.blen;
+                const bool once = TWS || (a.tw & kTwPPOnce);  // PP holds T(u): one more T
                 // the cases are uniform per thread, so each runs its own unrolled loop; cells
                 // outside the computed region are tapered too (harmless: they keep their stored
                 // value on output)
@@ -630,7 +632,7 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                             float f1, f2, f3;
                             taper_factors3<ALL>(fx, fy, fabsf(get(tz4, e)), xb, yb, signbit(get(tz4, e)), f1, f2, f3);
                             pp = ((pp * f1) * f2) * f3;
-                            if (!TWS) pp = ((pp * f1) * f2) * f3;
+                            if (!once) pp = ((pp * f1) * f2) * f3;
                         }
                         ppv[e] = pp;
                     }
@@ -639,7 +641,7 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                     for (int e = 0; e < kVZ; ++e) {
                         const float fz = fabsf(get(tz4, e));
                         float pp = (ppv[e] * fy) * fz;
-                        if (!TWS) pp = (pp * fy) * fz;
+                        if (!once) pp = (pp * fy) * fz;
                         ppv[e] = pp;
                     }
                 } else {
@@ -648,7 +650,7 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                         float f1, f2, f3;
                         taper_factors3<ALL>(fx, fy, fabsf(get(tz4, e)), xb, yb, signbit(get(tz4, e)), f1, f2, f3);
                         float pp = ((ppv[e] * f1) * f2) * f3;
-                        if (!TWS) pp = ((pp * f1) * f2) * f3;
+                        if (!once) pp = ((pp * f1) * f2) * f3;
                         ppv[e] = pp;
                     }
                 }
@@ -718,20 +720,25 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                     }
                 }
             }
-            if (TWS && tap) {  // store T(u_new): the receivers and the side buffer saw u_new
+            // the stored level: T(u_new) in the stored-taper forms; the receivers, the side buffer and
+            // the image take u_new itself
+            float nst[kVZ];
+#pragma unroll
+            for (int e = 0; e < kVZ; ++e) nst[e] = npp[e];
+            if (TWS && tap && !(a.tw & kTwRawOut)) {
                 const float tyv = tab[H + ty];
                 const float4 tz4 = *reinterpret_cast<const float4 *>(tab + S::SROWS + ZH + tz * kVZ);
-                if (!xb) {  // fx = 1: T(v) = (v fy) fz
+                if (ALL && !xb) {  // fx = 1: T(v) = (v fy) fz
 #pragma unroll
-                    for (int e = 0; e < kVZ; ++e) npp[e] = (npp[e] * fabsf(tyv)) * fabsf(get(tz4, e));
+                    for (int e = 0; e < kVZ; ++e) nst[e] = (npp[e] * fabsf(tyv)) * fabsf(get(tz4, e));
                 } else {
-                    const float fx = taper_factor_in(a.taper, a.blen, a.nxe, x);
+                    const float fx = xb ? taper_factor_in(a.taper, a.blen, a.nxe, x) : 1.f;
 #pragma unroll
                     for (int e = 0; e < kVZ; ++e) {
                         float f1, f2, f3;
-                        taper_factors3<true>(fx, fabsf(tyv), fabsf(get(tz4, e)), xb, signbit(tyv), signbit(get(tz4, e)),
-                                             f1, f2, f3);
-                        npp[e] = ((npp[e] * f1) * f2) * f3;
+                        taper_factors3<ALL>(fx, fabsf(tyv), fabsf(get(tz4, e)), xb, signbit(tyv), signbit(get(tz4, e)),
+                                            f1, f2, f3);
+                        nst[e] = ((npp[e] * f1) * f2) * f3;
                     }
                 }
             }
@@ -741,11 +748,11 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                 const bool v = (vmask >> e) & 1u;
                 float o;
                 if (SC) {
-                    o = v ? npp[e] * sOutInv : get(pp_raw, e) * sKeep;
-                    if (v) amax = fmaxf(amax, fabsf(npp[e]));
-                    nanacc = fmaf(0.f, npp[e], nanacc);
+                    o = v ? nst[e] * sOutInv : get(pp_raw, e) * sKeep;
+                    if (v) amax = fmaxf(amax, fabsf(nst[e]));
+                    nanacc = fmaf(0.f, nst[e], nanacc);
                 } else {
-                    o = v ? npp[e] : get(pp_raw, e);
+                    o = v ? nst[e] : get(pp_raw, e);
                     nanacc = fmaf(0.f, o, nanacc);  // stays 0 unless a NaN or an infinity appears
                 }
                 put(out, e, o);
@@ -767,7 +774,7 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                 for (int e = 0; e < kVZ; ++e) {
                     IT acc;
                     if (SC) acc = im[e] + (IT)(get(ps4, e) * sPS) * (IT)npp[e];
-                    else acc = im[e] + (IT)get(ps4, e) * (IT)get(out, e);
+                    else acc = im[e] + (IT)get(ps4, e) * (IT)npp[e];  // valid cells: the new level
                     res[e] = ((imask >> e) & 1u) ? acc : im[e];
                 }
                 if constexpr (sizeof(IT) == 4) {
@@ -838,11 +845,12 @@ template <int H>
 cudaError_t launch_tma_h(const TmaMaps &maps, const StepArgs &a, bool exact, int taper, bool img, dim3 grid,
                          cudaStream_t s) {
     // the dynamic shared-memory opt-in, once per (variant, device)
-    static unsigned long long attr_done[16] = {};
+    static unsigned long long attr_done[20] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    if (taper == kTaperAll && a.tw) taper = kTaperAllStored;
-    const int variant = (exact ? 8 : 0) + (img ? 4 : 0) + taper;
+    if (a.tw & kTwStored) taper = taper == kTaperAll ? kTaperAllStored : (taper == kTaperUpper ? kTaperUpperStored : -1);
+    if (taper < 0) return cudaErrorInvalidValue;
+    const int variant = (exact ? 10 : 0) + (img ? 5 : 0) + taper;
     auto run = [&](void (*kern)(TmaMaps, StepArgs), size_t smem) -> cudaError_t {
         const unsigned long long bit = 1ull << (dev & 63);
         if (!(attr_done[variant] & bit)) {
@@ -859,14 +867,18 @@ cudaError_t launch_tma_h(const TmaMaps &maps, const StepArgs &a, bool exact, int
     RTMB_TMA_CASE(true, kTaperUpper, false)
     RTMB_TMA_CASE(true, kTaperAll, false)
     RTMB_TMA_CASE(true, kTaperAllStored, false)
+    RTMB_TMA_CASE(true, kTaperUpperStored, false)
     RTMB_TMA_CASE(true, kTaperNone, true)
     RTMB_TMA_CASE(true, kTaperUpper, true)
+    RTMB_TMA_CASE(true, kTaperUpperStored, true)
     RTMB_TMA_CASE(false, kTaperNone, false)
     RTMB_TMA_CASE(false, kTaperUpper, false)
     RTMB_TMA_CASE(false, kTaperAll, false)
     RTMB_TMA_CASE(false, kTaperAllStored, false)
+    RTMB_TMA_CASE(false, kTaperUpperStored, false)
     RTMB_TMA_CASE(false, kTaperNone, true)
     RTMB_TMA_CASE(false, kTaperUpper, true)
+    RTMB_TMA_CASE(false, kTaperUpperStored, true)
 #undef RTMB_TMA_CASE
     return cudaErrorInvalidValue;
 }
@@ -879,7 +891,8 @@ cudaError_t launch_tma_store(const TmaMaps &maps, const StepArgs &a, int taper, 
     static unsigned long long attr_done[12] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    if (taper == kTaperAll && a.tw) taper = kTaperAllStored;
+    if (a.tw & kTwStored) taper = taper == kTaperAll ? kTaperAllStored : -1;  // 16-bit forms: modeling only
+    if (taper < 0) return cudaErrorInvalidValue;
     const int variant = (img ? (img64 ? 8 : 4) : 0) + taper;
     auto run = [&](void (*kern)(TmaMaps, StepArgs), size_t smem) -> cudaError_t {
         const unsigned long long bit = 1ull << (dev & 63);

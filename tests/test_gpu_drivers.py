@@ -87,6 +87,24 @@ def test_tapered_storage_matches_raw_fields(cuda, oracle, form, nt):
         assert rc == 0 and bitexact(out[0], ref)
 
 
+@pytest.mark.parametrize("extra", [0, rtmb.FLAG_IMG_FULL_Z], ids=["img", "img_full_z"])
+@pytest.mark.parametrize("form", ["exact", "fma"])
+def test_hbc_tapered_storage_matches_raw_fields(cuda, oracle, form, extra):
+    """HBC migration keeps the source wavefield tapered in HBM except its last two levels (the
+    snapshots of the backward pass) and the receiver wavefield tapered throughout: the image equals
+    the taper-on-load form's bit for bit, also over the tapered top slab (RTMB_FLAG_IMG_FULL_Z)."""
+    case = CASES["mid"]
+    p = oracle_params(case)
+    rec, _ = oracle.model_shot(p, oracle.v2dt2(oracle.extend_init_borders(layered_model(case), case["blen"], "abc"),
+                                               case["dt"]))
+    v2 = oracle.v2dt2(oracle.extend_init_borders(layered_model(case), case["blen"], "hbc", seed=4), case["dt"])
+    base = (rtmb.FLAG_FAST_FMA if form == "fma" else 0) | extra
+    a, _ = migrate_gpu(case, v2, rec, "hbc", cuda, flags=base)
+    b, _ = migrate_gpu(case, v2, rec, "hbc", cuda, flags=base | rtmb.FLAG_NO_TAPER_STORE)
+    assert np.abs(a).max() > 0
+    assert np.array_equal(a, b)
+
+
 def test_model_matches_reference_golden(cuda, golden):
     """GPU record vs the reference program's own .seism output."""
     import rtmb as R
