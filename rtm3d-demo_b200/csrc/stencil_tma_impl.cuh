@@ -3,9 +3,9 @@
 // Same contract and arithmetic as stencil_impl.cuh (bit-identical results); used when rows are
 // 16-byte aligned (nze % 4 == 0, 16-byte aligned base pointers).
 //
-// Pipeline.  A CTA owns a TZ x TY tile of the (y, z) plane and a chunk of x planes; its eight warps
-// compute, and thread 0 is also the producer of two rings of shared-memory slots filled by
-// cp.async.bulk.tensor (TMA) loads that complete on "full" mbarriers:
+// Pipeline.  A CTA owns a TZ x TY tile of the (y, z) plane and a chunk of x planes; eight consumer
+// warps compute, and lane 0 of a ninth warp is the producer of two rings of shared-memory slots
+// filled by cp.async.bulk.tensor (TMA) loads that complete on "full" mbarriers:
 //   * the P ring (D slots): the P tile of one plane with a y halo of H rows and a z halo of ZH
 //     columns.  A slot is needed from the plane's arrival (its centre values enter each thread's
 //     register queue of x taps) until the plane is computed H planes later (y and z taps);
@@ -14,9 +14,13 @@
 // The CTA has eight consumer warps and one producer warp.  Lane 0 of the producer warp issues the
 // loads in order; each slot is refilled once its "empty" mbarrier shows that all eight consumer warps
 // have released it, so loads run up to D-H-1 planes (P) and R-1 planes (core) ahead and no consumer
-// ever waits at a block barrier (the taper forms add a consumer-only named barrier per tapered
-// plane).  Each thread keeps the 2H+1 x taps of its four points in a register queue that shifts by
-// one plane per iteration.
+// ever waits at a block barrier (the taper-on-load forms add a consumer-only named barrier per
+// tapered plane; the stored-taper forms taper on store and need none).  Each thread keeps the 2H+1
+// x taps of its four points in a register queue that shifts by one plane per iteration.
+//
+// The rare per-cell work (source, receivers, upper border, taper side buffer) is found per plane by
+// CTA-uniform tests: the kernel runs at the 96-register cap of two CTAs per SM, and per-thread
+// state kept live through the plane loop costs instructions everywhere.
 //
 // Every wait is bounded (about two seconds): a wait that runs out sets error bit 2 and the warp
 // stops; the producer waits, again bounded, for the copies it issued before it exits.
