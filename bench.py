@@ -515,6 +515,99 @@ def run_batch(args) -> dict:
             "speedup": round(ms_single / ms_batch, 3)}
 
 
+# ------------------------------------------------------------------------------------------ model
+def run_model(args) -> dict:
+    """The CPU-runnable modeling configuration in full: a 128^3 three-layer model (1500, 2500 and
+    3500 m/s from depths 0, 40 and 80 cells), a 32-cell border tapered on every face but the free
+    surface's velocity, 1000 steps of 1 ms, a 15 Hz Ricker at (64, 64, 4), 64 x 64 receivers every
+    2 cells at depth 4.  GPU: s per modeled shot in the exact and FMA forms.  With the reference
+    program built: its own modeling of the same shot truncated to a bounded number of steps (the
+    cpu_baseline), and the GPU's exact-form record of that run compared with the reference's .seism
+    file bit for bit."""
+    import tempfile
+    import torch
+    import rtmb
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    n, blen, nt = 128, 32, args.model_nt
+    v = np.full((n, n, n), 3500.0, np.float32)
+    v[:, :, :40] = 1500.0
+    v[:, :, 40:80] = 2500.0
+    p = dict(nx=n, ny=n, nz=n, blen=blen, nt=nt, ntstep=nt, stencil_order=8, dx=10.0, dy=10.0, dz=10.0, dt=0.001,
+             fpeak=15.0, taper_factor=0.2, receiver_start_x=0, receiver_start_y=0, receiver_depth_z=4,
+             receiver_distance_x=2, receiver_distance_y=2, receiver_count_x=64, receiver_count_y=64,
+             boundary_condition="hbc", sx=64, sy=64, sz=4)
+    v2 = rtmb.v2dt2(rtmb.prepare_velocity(v, blen, "abc"), p["dt"])
+    out = {"metric": "s per modeled shot (128^3, 32-cell border, nt=1000)", "workload": "model",
+           "config": {"grid": [n + 2 * blen] * 3, "model": "3-layer 1500/2500/3500 m/s", "nt": nt, "fpeak_hz": 15.0,
+                      "receivers": [64, 64]}, "forms": {}}
+    npad = (n + 2 * blen) ** 3
+
+    def shot(flags, ntr):
+        q = dict(p, nt=ntr, ntstep=ntr)
+        ctx = rtmb.Context(rtmb.Params.from_input(q, flags=flags | rtmb.FLAG_USE_GRAPH, device=0))
+        ctx.load_v2dt2(v2, from_host=True)
+        rec = torch.zeros((1, 64, 64, ntr), device=dev)
+        ctx.model_shot(p["sx"], p["sy"], p["sz"], rec)  # warm-up: graph capture
+        ctx.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ctx.model_shot(p["sx"], p["sy"], p["sz"], rec)
+        e1.record()
+        ctx.sync()
+        ms = e0.elapsed_time(e1)
+        ctx.close()
+        return ms, rec.cpu().numpy()
+
+    for form, flags in (("fp32_exact", 0), ("fp32_fma", rtmb.FLAG_FAST_FMA)):
+        ms, _ = shot(flags, nt)
+        out["forms"][form] = {"s_per_shot": round(ms / 1e3, 4), "gpt_s": round(npad * nt / ms / 1e6, 2)}
+    out["value"] = out["forms"]["fp32_fma"]["gpt_s"]
+    out["unit"] = "Gpt/s"
+    if not args.no_cpu_baseline:
+        from oracle import REF_BIN
+        if os.path.exists(REF_BIN):
+            nts = args.model_ref_nt
+            with tempfile.TemporaryDirectory() as wd:
+                for sub in ("out", "tmp", "dat"):
+                    os.makedirs(os.path.join(wd, sub), exist_ok=True)
+                vp = os.path.join(wd, "vel.bin")
+                v.tofile(vp)
+                threads = os.cpu_count() or 1
+                d = dict(mname="bench", vpfile=vp, vpefile=os.path.join(wd, "vpe.bin"), save_vpe_file=False,
+                         outdir=os.path.join(wd, "out"), tmpdir=os.path.join(wd, "tmp"), datdir=os.path.join(wd, "dat"),
+                         nx=n, ny=n, nz=n, blen=blen, width_m=0, height_m=0, depth_m=0, nt=nts, dz=10.0, dy=10.0,
+                         dx=10.0, dt=p["dt"], fpeak=p["fpeak"], fmax=30.0, taper_factor=p["taper_factor"],
+                         stencil_order=8, modeling=True, migration=False, rtm_type="rtm", boundary_condition="hbc",
+                         source_total=1, source_start_x=64, source_start_y=64, source_depth_z=4, source_distance_x=1,
+                         source_distance_y=1, source_count_x=1, source_count_y=1, receiver_total=64 * 64,
+                         receiver_start_x=0, receiver_start_y=0, receiver_depth_z=4, receiver_distance_x=2,
+                         receiver_distance_y=2, receiver_count_x=64, receiver_count_y=64, ntstep=nts,
+                         nthreads=threads, load_vpe_from_file=False, save_snapshots=False, distributed_grid=False,
+                         snapshot_step=10, fmig=False, fmig_max_freq=30.0, fmig_min_freq=1.0, fmig_nwstep=1,
+                         fmig_distributed_imaging=False, fpga_xclbin="", fpga_fwd_kernel="", fpga_bwd_kernel="",
+                         verbose=True)
+                jp = os.path.join(wd, "model.json")
+                with open(jp, "w") as f:
+                    json.dump(d, f)
+                r = subprocess.run([REF_BIN, jp], capture_output=True, text=True, cwd=wd, timeout=900)
+                t = None
+                for line in r.stdout.splitlines():
+                    if '"modeling_time"' in line:
+                        t = float(line.split(":")[1].strip().rstrip(","))
+                seism = os.path.join(wd, "dat", f"RTMSEISMOGRAM_S64x64x4_NXNY_64x64_NTSTART0_NTSTEP{nts}.seism")
+                ref_rec = np.fromfile(seism, np.float32) if os.path.exists(seism) else None
+            if t:
+                out["cpu_baseline"] = {"value": round(npad * nts / t / 1e9, 4), "unit": "Gpt/s", "cores": threads,
+                                       "kind": "reference",
+                                       "sample": f"RTM3D.bin modeling of the same shot, nt={nts}, its own modeling timer"}
+            if ref_rec is not None:
+                _, got = shot(0, nts)
+                out["record_vs_reference"] = {"nt": nts, "bitexact": bool(np.array_equal(
+                    got.reshape(-1).view(np.uint32), ref_rec.view(np.uint32)))}
+    return out
+
+
 # ------------------------------------------------------------------------------------------ fmig
 def run_fmig(args) -> dict:
     """Frequency-domain RTM of one shot (rtmb_migrate_shot_fmig): the salt model, HBC border, both
@@ -732,10 +825,12 @@ def main():
     ap.add_argument("--nt", type=int, default=3000)
     ap.add_argument("--form", choices=FORMS, default="fp32_fma", help="arithmetic/storage form of the timed shots")
     ap.add_argument("--exact", action="store_true", help="same as --form fp32_exact")
-    ap.add_argument("--workload", choices=("rtm", "batch", "closure", "fmig"), default="rtm",
+    ap.add_argument("--workload", choices=("rtm", "batch", "closure", "fmig", "model"), default="rtm",
                     help="rtm: the single-shot RTM line (default); batch: batched aperture shots against "
                          "one-by-one; closure: the learned boundary closure against the tapered borders; "
-                         "fmig: frequency-domain RTM of one shot")
+                         "fmig: frequency-domain RTM of one shot; model: the 128^3 modeling configuration")
+    ap.add_argument("--model-nt", type=int, default=1000)
+    ap.add_argument("--model-ref-nt", type=int, default=200, help="steps of the reference program's timed sample")
     ap.add_argument("--fmig-size", type=int, default=192)
     ap.add_argument("--fmig-nt", type=int, default=400)
     ap.add_argument("--fmig-band", type=float, nargs=2, default=(4.0, 20.0))
@@ -766,7 +861,7 @@ def main():
     if args.impl == "reference":
         out = run_reference_arm(args, rank)
     elif args.workload != "rtm":
-        runner = {"batch": run_batch, "closure": run_closure, "fmig": run_fmig}[args.workload]
+        runner = {"batch": run_batch, "closure": run_closure, "fmig": run_fmig, "model": run_model}[args.workload]
         out = runner(args) if rank == 0 else None
     else:
         if world > 1:
