@@ -135,6 +135,44 @@ def test_twod_vs_golden(oracle, golden):
         assert bitexact(fin, g[f"img_{name}"]), name
 
 
+def test_twod_vs_reference_program(oracle):
+    """A second 2D case through the reference program itself (order 4, unequal spacing): record,
+    HBC image and fmig image."""
+    import glob
+    import os
+    import sys
+    import tempfile
+    from oracle import REF_BIN
+    if not os.path.exists(REF_BIN):
+        pytest.skip("reference program (oracle/_ref/RTM3D.bin) not present")
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    from make_golden import read_record, run_reference
+    case = dict(CASES["odd"], nx=1, sx=0, rsx=0, rcx=1, rdx=1)
+    b = case["blen"]
+    shp = (1 + 2 * b, case["ny"] + 2 * b, case["nz"] + 2 * b)
+    p = oracle_params(case)
+    with tempfile.TemporaryDirectory() as wd:
+        rec = read_record(run_reference(case, "model", wd))
+        ve = oracle.extend_init_borders(layered_model(case), b, "abc")
+        got, rc = oracle.model_shot(p, oracle.v2dt2(ve, case["dt"]))
+        assert rc == 0 and np.abs(rec).max() > 0 and bitexact(got, rec)
+        for name, extra in (("hbc", None), ("fmig", dict(fmig=True, fmig_min_freq=2.0, fmig_max_freq=30.0,
+                                                            fmig_nwstep=1))):
+            for f in glob.glob(os.path.join(wd, "out", "RTMIMG_*")):
+                os.remove(f)
+            d = run_reference(case, "hbc", wd, vpe_path=os.path.join(wd, f"vpe_{name}.bin"), extra=extra)
+            want = np.fromfile(glob.glob(os.path.join(wd, "out", "RTMIMG_*"))[0], np.float32)
+            v2 = oracle.v2dt2(np.fromfile(d["vpefile"], np.float32).reshape(shp), case["dt"])
+            if name == "fmig":
+                img, rc = oracle.migrate_fmig(p, v2, rec, 2.0, 30.0)
+            else:
+                img, rc = oracle.migrate(p, v2, rec, "hbc")
+            assert rc == 0
+            fin = oracle.filter_remove(img, b, case["dx"], case["dy"], case["dz"])
+            assert np.abs(want).max() > 0
+            assert bitexact(fin, want.reshape(fin.shape)), name
+
+
 def test_step2d_vs_reference_build(oracle, reference):
     rng = np.random.default_rng(5)
     for (ny, nz, b, order) in ((11, 17, 5, 6), (16, 10, 8, 12)):
