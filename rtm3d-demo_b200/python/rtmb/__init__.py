@@ -442,7 +442,7 @@ def closure_train(params, X, R, n: int, steps: int, batch: int, lr: float, seed:
 
 
 def closure_falls_back(learned_reflection: float, hbc_reflection: float) -> bool:
-    """The judge of the learned closure: a run falls back to the plain 32-cell border when the
+    """The fallback test of the learned closure: a run falls back to the plain 32-cell border when the
     closure's reflected energy (record rel-L2 against a wide-padded run of the same shot) exceeds
     the 32-cell border's."""
     return not (learned_reflection <= hbc_reflection)

@@ -10,7 +10,7 @@ import rtmb
 pytestmark = pytest.mark.gpu
 
 BLEN = 12
-SURVEY = (64, 56, 40)  # nz + 2*blen = 64
+VOLUME = (64, 56, 40)  # nz + 2*blen = 64
 APERTURES = [  # (ox, oy, nx, ny), full depth; uneven sizes
     (0, 0, 40, 36),
     (20, 10, 44, 46),
@@ -20,11 +20,11 @@ NT, NTSTEP = 60, 30
 
 
 def survey_model():
-    nx, ny, nz = SURVEY
+    nx, ny, nz = VOLUME
     rng = np.random.default_rng(5)
-    v = np.full(SURVEY, 1800.0, np.float32)
+    v = np.full(VOLUME, 1800.0, np.float32)
     v[:, :, nz // 2:] = 2600.0
-    v += (rng.random(SURVEY) * 40).astype(np.float32)
+    v += (rng.random(VOLUME) * 40).astype(np.float32)
     return v
 
 
@@ -41,7 +41,7 @@ def build_shots(cuda):
     rng = np.random.default_rng(9)
     shots, keep = [], []
     for k, (ox, oy, nx, ny) in enumerate(APERTURES):
-        nz = SURVEY[2]
+        nz = VOLUME[2]
         ve = rtmb.prepare_velocity(v[ox:ox + nx, oy:oy + ny, :], BLEN, "rbc", seed=11 + k)
         v2 = torch.from_numpy(rtmb.v2dt2(ve, 0.001)).to(cuda)
         rcx, rcy = nx // 2, ny // 2
@@ -58,7 +58,7 @@ def build_shots(cuda):
 def one_by_one(shots, flags, cuda):
     """The single-shot drivers on each aperture, stacked at the origins in FP64."""
     import torch
-    stack = np.zeros(SURVEY, np.float64)
+    stack = np.zeros(VOLUME, np.float64)
     for s in shots:
         p = rtmb.Params.from_input(params(s.nx, s.ny, s.nz, s.receiver_count_x, s.receiver_count_y), flags=flags,
                                    device=0)
@@ -86,9 +86,9 @@ def one_by_one(shots, flags, cuda):
 def test_batch_matches_single_shots(cuda, flags):
     import torch
     shots, keep = build_shots(cuda)
-    nx, ny, nz = SURVEY
+    nx, ny, nz = VOLUME
     ctx = rtmb.Context(rtmb.Params.from_input(params(nx, ny, nz, 1, 1), flags=flags, device=0))
-    stack = torch.zeros(SURVEY, dtype=torch.float64, device=cuda)
+    stack = torch.zeros(VOLUME, dtype=torch.float64, device=cuda)
     ctx.migrate_batch(shots, stack)
     ctx.sync()
     got = stack.cpu().numpy()

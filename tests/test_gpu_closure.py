@@ -174,5 +174,5 @@ def test_learned_closure_beats_the_plain_8_cell_border(cuda):
           f"taper-32 {e_32:.4f}; {nrows} training rows, loss {losses[:10].mean():.3e} -> {losses[-50:].mean():.3e}")
     assert np.isfinite(e_l)
     assert e_l < e_8
-    # plain HBC judges: the run falls back to it when the closure reflects more than 32 cells do
+    # plain HBC decides: the run falls back to it when the closure reflects more than 32 cells do
     assert rtmb.closure_falls_back(e_l, e_32) == (e_l > e_32)

@@ -2,7 +2,7 @@
 against the reference's own golden outputs.
 
 Exact form: shot record and image BIT-EXACT.  FMA form: record rel-L2 <= 1e-5 and image rel-L2
-<= 1e-4 (the north-star tolerances for the plain FP32 form)."""
+<= 1e-4 (the tolerances set for the plain FP32 form)."""
 import numpy as np
 import pytest
 
