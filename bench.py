@@ -48,33 +48,43 @@ L2_BYTES = 126 * 2**20
 
 
 # ------------------------------------------------------------------------------------------ workload
-def workload(n: int, nt: int) -> dict:
-    """input.json parameters of the benchmark shot (configs scale with n, reference value 512)."""
-    return dict(nx=n, ny=n, nz=n, blen=40, nt=nt, ntstep=nt, stencil_order=8, dx=10.0, dy=10.0, dz=10.0,
+METRIC = "G point-updates/s per migrated RTM shot (512^3 RBC, nt=3000)"
+
+
+def workload(n: int, nt: int, ny: int | None = None, nz: int | None = None) -> dict:
+    """input.json parameters of the benchmark shot on an n x ny x nz model (default cubic; the
+    workload is 512^3): 40-cell RBC border, 12 Hz Ricker at the surface centre, receivers every 2
+    cells over the whole surface."""
+    ny = n if ny is None else ny
+    nz = n if nz is None else nz
+    return dict(nx=n, ny=ny, nz=nz, blen=40, nt=nt, ntstep=nt, stencil_order=8, dx=10.0, dy=10.0, dz=10.0,
                 dt=0.001, fpeak=12.0, taper_factor=0.2, receiver_start_x=0, receiver_start_y=0,
                 receiver_depth_z=0, receiver_distance_x=2, receiver_distance_y=2,
-                receiver_count_x=n // 2, receiver_count_y=n // 2, boundary_condition="rbc",
-                sx=n // 2, sy=n // 2, sz=0)
+                receiver_count_x=n // 2, receiver_count_y=ny // 2, boundary_condition="rbc",
+                sx=n // 2, sy=ny // 2, sz=0)
 
 
-def salt_model(n: int, seed: int = 1234) -> np.ndarray:
-    """Seeded synthetic velocity (x slowest, z fastest), float32 m/s."""
+def salt_model(nx: int, ny: int | None = None, nz: int | None = None, seed: int = 1234) -> np.ndarray:
+    """Seeded synthetic velocity (x slowest, z fastest), float32 m/s, on an nx x ny x nz grid at 10 m:
+    the 512^3 salt model scaled per axis to the grid (ellipsoid semi-axes 120 x 100 x 60 cells and
+    centre (256, 256, 300) at 512^3; the background depends on depth in metres only)."""
     from scipy import ndimage
-    f = n / 512.0
-    z = np.arange(n, dtype=np.float32) * 10.0
-    v = np.broadcast_to(np.minimum(1500.0 + 0.6 * z, 4500.0), (n, n, n)).astype(np.float32)
-    c = np.arange(n, dtype=np.float32)
-    ex = ((c - 256 * f) / (120 * f)) ** 2
-    ey = ((c - 256 * f) / (100 * f)) ** 2
-    ez = ((c - 300 * f) / (60 * f)) ** 2
+    ny = nx if ny is None else ny
+    nz = nx if nz is None else nz
+    fx, fy, fz = nx / 512.0, ny / 512.0, nz / 512.0
+    z = np.arange(nz, dtype=np.float32) * 10.0
+    v = np.broadcast_to(np.minimum(1500.0 + 0.6 * z, 4500.0), (nx, ny, nz)).astype(np.float32)
+    ex = ((np.arange(nx, dtype=np.float32) - 256 * fx) / (120 * fx)) ** 2
+    ey = ((np.arange(ny, dtype=np.float32) - 256 * fy) / (100 * fy)) ** 2
+    ez = ((np.arange(nz, dtype=np.float32) - 300 * fz) / (60 * fz)) ** 2
     salt = (ex[:, None, None] + ey[None, :, None] + ez[None, None, :]) <= 1.0
     v[salt] = 4500.0
     # +-3% perturbation: white noise on a grid 8x coarser, Gaussian-smoothed (sigma 1 coarse cell
     # = 8 cells) and interpolated trilinearly to the model grid
     rng = np.random.default_rng(seed)
-    nc = max(4, n // 8)
-    pert = ndimage.gaussian_filter(rng.standard_normal((nc, nc, nc)).astype(np.float32), 1.0, mode="wrap")
-    pert = ndimage.zoom(pert, n / nc, order=1, mode="nearest")[:n, :n, :n]
+    nc = [max(4, k // 8) for k in (nx, ny, nz)]
+    pert = ndimage.gaussian_filter(rng.standard_normal(nc).astype(np.float32), 1.0, mode="wrap")
+    pert = ndimage.zoom(pert, (nx / nc[0], ny / nc[1], nz / nc[2]), order=1, mode="nearest")[:nx, :ny, :nz]
     pert *= 0.03 / max(float(np.abs(pert).max()), 1e-12)
     v = v * (1.0 + pert)
     # keep the order-8 leapfrog inside its CFL bound (v dt / dx <= 0.453 at 10 m, 1 ms)
@@ -164,64 +174,80 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------------------ reference CPU
-def run_reference_sample(p: dict, v: np.ndarray, vpe: np.ndarray, rec: np.ndarray, nts: int, workdir: str):
-    """Run the reference's own CPU program (RTM3D.bin) for an RBC migration of the same shot with
-    nt truncated to nts.  Returns (seconds of its migration timer, point updates, threads)."""
-    from oracle import REF_BIN
-    if not os.path.exists(REF_BIN):
-        raise FileNotFoundError("oracle/_ref/RTM3D.bin is not built")
+def ref_input(p: dict, workdir: str, vp: str, nts: int, threads: int, migration: bool) -> dict:
+    """input.json of the reference program for the workload p with nt cut to nts."""
+    sx, sy, sz = p["sx"], p["sy"], p["sz"]
+    return dict(mname="bench", vpfile=vp, vpefile=os.path.join(workdir, "vpe.bin"), save_vpe_file=False,
+                outdir=os.path.join(workdir, "out"), tmpdir=os.path.join(workdir, "tmp"),
+                datdir=os.path.join(workdir, "dat"), nx=p["nx"], ny=p["ny"], nz=p["nz"], blen=p["blen"],
+                width_m=0, height_m=0, depth_m=0, nt=nts, dz=p["dz"], dy=p["dy"], dx=p["dx"], dt=p["dt"],
+                fpeak=p["fpeak"], fmax=30.0, taper_factor=p["taper_factor"], stencil_order=p["stencil_order"],
+                modeling=not migration, migration=migration, rtm_type="rtm",
+                boundary_condition=p["boundary_condition"], source_total=1, source_start_x=sx, source_start_y=sy,
+                source_depth_z=sz, source_distance_x=1, source_distance_y=1, source_count_x=1, source_count_y=1,
+                receiver_total=p["receiver_count_x"] * p["receiver_count_y"],
+                receiver_start_x=p["receiver_start_x"], receiver_start_y=p["receiver_start_y"],
+                receiver_depth_z=p["receiver_depth_z"], receiver_distance_x=p["receiver_distance_x"],
+                receiver_distance_y=p["receiver_distance_y"], receiver_count_x=p["receiver_count_x"],
+                receiver_count_y=p["receiver_count_y"], ntstep=nts, nthreads=threads, load_vpe_from_file=False,
+                save_snapshots=False, distributed_grid=False, snapshot_step=10, fmig=False, fmig_max_freq=30.0,
+                fmig_min_freq=1.0, fmig_nwstep=1, fmig_distributed_imaging=False, fpga_xclbin="",
+                fpga_fwd_kernel="", fpga_bwd_kernel="", verbose=True)
+
+
+def run_reference_program(binary: str, p: dict, v: np.ndarray, rec: np.ndarray | None, nts: int, workdir: str,
+                          migration: bool = True):
+    """Run one of the reference's own programs (RTM3D.bin, or its GPU build RTM3D_GPU.bin) on the
+    workload p with nt cut to nts: an RBC migration of the given record (the program builds its own
+    random border), or a modeling shot.  Returns (seconds of the program's own migration or modeling
+    timer, point updates, threads, the record it wrote when modeling)."""
+    if not os.path.exists(binary):
+        raise FileNotFoundError(f"{os.path.relpath(binary, ROOT)} is not built")
     for sub in ("out", "tmp", "dat"):
         os.makedirs(os.path.join(workdir, sub), exist_ok=True)
     vp = os.path.join(workdir, "vel.bin")
-    vpe_path = os.path.join(workdir, "vpe.bin")
     if not os.path.exists(vp):
         v.tofile(vp)
-        vpe.tofile(vpe_path)
-    # the record chunk [rcx][rcy][nts] under the reference's file name (RTMBase.hpp:131-138)
     sx, sy, sz = p["sx"], p["sy"], p["sz"]
     seism = os.path.join(workdir, "dat", f"RTMSEISMOGRAM_S{sx}x{sy}x{sz}_NXNY_{p['receiver_count_x']}x"
                                          f"{p['receiver_count_y']}_NTSTART0_NTSTEP{nts}.seism")
-    np.ascontiguousarray(rec[..., :nts]).tofile(seism)
+    if migration:  # the record chunk [rcx][rcy][nts] under the reference's file name (RTMBase.hpp:131-138)
+        np.ascontiguousarray(rec[..., :nts]).tofile(seism)
+    elif os.path.exists(seism):
+        os.remove(seism)
     threads = os.cpu_count() or 1
-    d = dict(mname="bench", vpfile=vp, vpefile=vpe_path, save_vpe_file=False, outdir=os.path.join(workdir, "out"),
-             tmpdir=os.path.join(workdir, "tmp"), datdir=os.path.join(workdir, "dat"), nx=p["nx"], ny=p["ny"],
-             nz=p["nz"], blen=p["blen"], width_m=0, height_m=0, depth_m=0, nt=nts, dz=p["dz"], dy=p["dy"],
-             dx=p["dx"], dt=p["dt"], fpeak=p["fpeak"], fmax=30.0, taper_factor=p["taper_factor"],
-             stencil_order=p["stencil_order"], modeling=False, migration=True, rtm_type="rtm",
-             boundary_condition="rbc", source_total=1, source_start_x=sx, source_start_y=sy, source_depth_z=sz,
-             source_distance_x=1, source_distance_y=1, source_count_x=1, source_count_y=1,
-             receiver_total=p["receiver_count_x"] * p["receiver_count_y"],
-             receiver_start_x=p["receiver_start_x"], receiver_start_y=p["receiver_start_y"],
-             receiver_depth_z=p["receiver_depth_z"], receiver_distance_x=p["receiver_distance_x"],
-             receiver_distance_y=p["receiver_distance_y"], receiver_count_x=p["receiver_count_x"],
-             receiver_count_y=p["receiver_count_y"], ntstep=nts, nthreads=threads, load_vpe_from_file=True,
-             save_snapshots=False, distributed_grid=False, snapshot_step=10, fmig=False, fmig_max_freq=30.0,
-             fmig_min_freq=1.0, fmig_nwstep=1, fmig_distributed_imaging=False, fpga_xclbin="",
-             fpga_fwd_kernel="", fpga_bwd_kernel="", verbose=True)
-    jp = os.path.join(workdir, "mig.json")
+    d = ref_input(p, workdir, vp, nts, threads, migration)
+    jp = os.path.join(workdir, "run.json")
     with open(jp, "w") as f:
         json.dump(d, f)
-    r = subprocess.run([REF_BIN, jp], capture_output=True, text=True, cwd=workdir, timeout=900)
+    r = subprocess.run([binary, jp], capture_output=True, text=True, cwd=workdir, timeout=1200)
     if r.returncode != 0:
-        raise RuntimeError(f"RTM3D.bin failed: {r.stdout[-500:]} {r.stderr[-500:]}")
-    mig = None
+        raise RuntimeError(f"{os.path.basename(binary)} failed: {r.stdout[-400:]} {r.stderr[-400:]}")
+    key = '"migration_time"' if migration else '"modeling_time"'
+    t = None
     for line in r.stdout.splitlines():
-        if '"migration_time"' in line:
-            mig = float(line.split(":")[1].strip().rstrip(","))
-    if not mig:
-        raise RuntimeError("no migration_time in the reference report")
+        if key in line:
+            t = float(line.split(":")[1].strip().rstrip(","))
+    if not t:
+        raise RuntimeError(f"no {key} in the report of {os.path.basename(binary)}")
     pts = n_points(p)
-    return mig, pts * (3 * nts - 2), threads
+    upd = pts * (3 * nts - 2) if migration else pts * nts
+    out_rec = None if migration else np.fromfile(seism, np.float32)
+    return t, upd, threads, out_rec
 
 
-def reference_sample_steps(p: dict) -> int:
-    return 8
+def ref_gpu_bin() -> str:
+    return os.path.join(ROOT, "oracle", "_ref", "RTM3D_GPU.bin")
+
+
+def ref_cpu_bin() -> str:
+    return os.path.join(ROOT, "oracle", "_ref", "RTM3D.bin")
 
 
 # ------------------------------------------------------------------------------------------ arms
 def build_inputs(p: dict, with_abc: bool):
     import rtmb
-    v = salt_model(p["nx"])
+    v = salt_model(p["nx"], p["ny"], p["nz"])
     vpe = rtmb.prepare_velocity(v, p["blen"], "rbc", seed=1234)
     v2 = rtmb.v2dt2(vpe, p["dt"])
     v2m = rtmb.v2dt2(rtmb.prepare_velocity(v, p["blen"], "abc"), p["dt"]) if with_abc else None
@@ -229,6 +255,7 @@ def build_inputs(p: dict, with_abc: bool):
 
 
 FORMS = ("fp32_exact", "fp32_fma", "fp16", "bf16", "fp16_img64", "bf16_img64")
+C3_FORMS = ("fp32_exact", "fp32_fma", "fp16", "bf16")
 
 
 def form_flags(rtmb, form: str) -> int:
@@ -237,14 +264,23 @@ def form_flags(rtmb, form: str) -> int:
             "bf16_img64": rtmb.FLAG_STORE_BF16 | rtmb.FLAG_IMG_F64}[form]
 
 
-def compare_forms(p: dict, v2: np.ndarray, rec_full, dev, nt_cmp: int) -> dict:
-    """Per-form timing and image error against the FP64 GPU oracle on the first nt_cmp steps."""
+def rel_l2_dev(a, ref, ref_norm: float) -> float:
+    import torch
+    return float(torch.linalg.vector_norm(a.double() - ref)) / (ref_norm if ref_norm > 0 else 1.0)
+
+
+def compare_forms(p: dict, v2: np.ndarray, v2m: np.ndarray | None, rec_full, dev, nt_cmp: int,
+                  forms=FORMS) -> dict:
+    """Per-form device time and error against the FP64 GPU oracle on the same grid, over nt_cmp
+    steps (the full nt by default): the migrated image of the given record (image rel-L2) and, when
+    v2m (the modeling velocity) is given, the modeled shot record (record rel-L2)."""
     import torch
     import rtmb
     q = dict(p, nt=nt_cmp, ntstep=nt_cmp)
     rec = rec_full[..., :nt_cmp].contiguous()
     sx, sy, sz = q["sx"], q["sy"], q["sz"]
-    ctx = rtmb.Context(rtmb.Params.from_input(q, device=dev.index or 0))
+    d = dev.index or 0
+    ctx = rtmb.Context(rtmb.Params.from_input(q, device=d))
     ctx.load_v2dt2(v2, from_host=True)
     shape = ctx.padded_shape
     ref = torch.zeros(shape, dtype=torch.float64, device=dev)
@@ -254,33 +290,132 @@ def compare_forms(p: dict, v2: np.ndarray, rec_full, dev, nt_cmp: int) -> dict:
     f64_s = time.time() - t0
     ctx.close()
     ref_norm = float(torch.linalg.vector_norm(ref))
-    forms = {f: form_flags(rtmb, f) for f in FORMS}
+    rec_ref = None
+    if v2m is not None:
+        mc = rtmb.Context(rtmb.Params.from_input(dict(q, boundary_condition="hbc"), device=d))
+        mc.load_v2dt2(v2m, from_host=True)
+        rec_ref = torch.zeros(rec.shape, dtype=torch.float64, device=dev)
+        mc.model_shot_f64(sx, sy, sz, rec_ref)
+        mc.sync()
+        mc.close()
+        rec_ref_norm = float(torch.linalg.vector_norm(rec_ref))
     sweeps_cmp = 3 * nt_cmp - 2
     sweeps_full = 3 * p["nt"] - 2
     out = {}
     img = torch.zeros(shape, dtype=torch.float32, device=dev)
-    for name, fl in forms.items():
-        c = rtmb.Context(rtmb.Params.from_input(q, flags=fl, device=dev.index or 0))
+    for name in forms:
+        fl = form_flags(rtmb, name)
+        c = rtmb.Context(rtmb.Params.from_input(q, flags=fl, device=d))
         c.load_v2dt2(v2, from_host=True)
-        c.migrate_shot(sx, sy, sz, rec, img)  # allocation and warm-up
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        c.migrate_shot(sx, sy, sz, rec, img)
+        c.migrate_shot(sx, sy, sz, rec, img)  # one full shot, timed (buffers are allocated on first use)
         e1.record()
         c.sync()
         ms = e0.elapsed_time(e1)
-        err = float(torch.linalg.vector_norm(img.double() - ref)) / (ref_norm if ref_norm > 0 else 1.0)
-        per_sweep = ms / sweeps_cmp
-        out[name] = {"ms_per_sweep": round(per_sweep, 4), "s_per_shot": round(per_sweep * sweeps_full / 1e3, 3),
-                     "gpt_s": round(n_points(p) / (per_sweep * 1e-3) / 1e9, 2),
-                     "image_rel_l2_vs_fp64": float("%.3e" % err)}
         c.close()
+        per_sweep = ms / sweeps_cmp
+        r = {"ms_per_sweep": round(per_sweep, 4), "s_per_shot": round(per_sweep * sweeps_full / 1e3, 3),
+             "gpt_s": round(n_points(p) / (per_sweep * 1e-3) / 1e9, 2),
+             "image_rel_l2_vs_fp64": float("%.3e" % rel_l2_dev(img, ref, ref_norm))}
+        if rec_ref is not None:
+            mc = rtmb.Context(rtmb.Params.from_input(dict(q, boundary_condition="hbc"), flags=fl, device=d))
+            mc.load_v2dt2(v2m, from_host=True)
+            got = torch.zeros(rec.shape, dtype=torch.float32, device=dev)
+            mc.model_shot(sx, sy, sz, got)
+            mc.sync()
+            mc.close()
+            r["record_rel_l2_vs_fp64"] = float("%.3e" % rel_l2_dev(got, rec_ref, rec_ref_norm))
+        out[name] = r
     ok = {k: v for k, v in out.items() if v["image_rel_l2_vs_fp64"] <= 1e-3}
     chosen = min(ok, key=lambda k: ok[k]["ms_per_sweep"]) if ok else "fp32_exact"
-    return {"nt": nt_cmp, "note": f"s_per_shot scaled to nt={p['nt']} from the nt={nt_cmp} run; FP64 oracle "
-                                  f"run took {f64_s:.1f} s", "forms": out, "chosen": chosen,
-            "chosen_vs_plain": round(out["fp32_exact"]["ms_per_sweep"] / out[chosen]["ms_per_sweep"], 3)}
+    note = (f"every form run over the full nt={nt_cmp}" if nt_cmp == p["nt"] else
+            f"s_per_shot scaled to nt={p['nt']} from the nt={nt_cmp} run")
+    res = {"nt": nt_cmp, "grid": list(shape), "note": f"{note}; FP64 oracle migration took {f64_s:.1f} s",
+           "forms": out, "chosen": chosen}
+    if "fp32_exact" in out:
+        res["chosen_vs_plain"] = round(out["fp32_exact"]["ms_per_sweep"] / out[chosen]["ms_per_sweep"], 3)
+    return res
+
+
+def run_precision(args, forms=FORMS) -> dict:
+    """The precision configuration: 896 x 896 x 512 at 10 m (the salt model scaled to the grid),
+    40-cell RBC border (976 x 976 x 592 padded), 12 Hz, receivers every 2 cells over the surface,
+    the full nt; each storage form's shot record and image against the FP64 GPU oracle on the same
+    grid, and its device time.  The record comes from this library's FP32 modeling pass."""
+    import torch
+    import rtmb
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    nx, ny, nz = args.c3_grid
+    p = workload(nx, args.nt, ny=ny, nz=nz)
+    v = salt_model(nx, ny, nz)
+    v2 = rtmb.v2dt2(rtmb.prepare_velocity(v, p["blen"], "rbc", seed=1234), p["dt"])
+    v2m = rtmb.v2dt2(rtmb.prepare_velocity(v, p["blen"], "abc"), p["dt"])
+    mctx = rtmb.Context(rtmb.Params.from_input(dict(p, boundary_condition="hbc"), flags=rtmb.FLAG_FAST_FMA,
+                                               device=0))
+    rec = torch.zeros((1, p["receiver_count_x"], p["receiver_count_y"], p["nt"]), dtype=torch.float32, device=dev)
+    mctx.load_v2dt2(v2m, from_host=True)
+    mctx.model_shot(p["sx"], p["sy"], p["sz"], rec)
+    mctx.sync()
+    mctx.close()
+    res = compare_forms(p, v2, v2m, rec, dev, p["nt"], forms)
+    res["workload"] = f"precision_{nx}x{ny}x{nz}_nt{p['nt']}"
+    return res
+
+
+def reference_gpu_bar(args, p: dict, v: np.ndarray, rec, value: float) -> dict:
+    """The reference's own GPU program (oracle/_ref/RTM3D_GPU.bin: its CUDA back-end built for
+    sm_100a from its sources) on this GPU: the modeling configuration in full (128^3 + 32-cell
+    border, 1000 steps), and the RBC migration of the benchmark shot with nt cut to --ref-gpu-nt,
+    each timed by the program's own timer; beside them this library on the same work."""
+    import torch
+    import rtmb
+    out = {"program": "oracle/_ref/RTM3D_GPU.bin (the reference's kernel/gpu/rtmgpu_finitediff.cu, sm_100a)"}
+    binary = ref_gpu_bin()
+    with tempfile.TemporaryDirectory() as wd:
+        nts = args.ref_gpu_nt
+        sec, upd, _, _ = run_reference_program(binary, p, v, rec.cpu().numpy(), nts, wd)
+        out["rtm_rbc"] = {"nt_sample": nts, "gpt_s": round(upd / sec / 1e9, 3),
+                          "s_per_shot_extrapolated": round(sec * (3 * p["nt"] - 2) / (3 * nts - 2), 2),
+                          "this_library_gpt_s": round(value, 3), "speedup": round(value / (upd / sec / 1e9), 2)}
+    mp, vm = c1_workload()
+    with tempfile.TemporaryDirectory() as wd:
+        sec, upd, _, ref_rec = run_reference_program(binary, mp, vm, None, mp["nt"], wd, migration=False)
+    dev = torch.device("cuda", 0)
+    v2 = rtmb.v2dt2(rtmb.prepare_velocity(vm, mp["blen"], "abc"), mp["dt"])
+    ctx = rtmb.Context(rtmb.Params.from_input(mp, flags=rtmb.FLAG_FAST_FMA | rtmb.FLAG_USE_GRAPH, device=0))
+    ctx.load_v2dt2(v2, from_host=True)
+    got = torch.zeros((1, 64, 64, mp["nt"]), device=dev)
+    ctx.model_shot(mp["sx"], mp["sy"], mp["sz"], got)  # warm-up: graph capture
+    ctx.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ctx.model_shot(mp["sx"], mp["sy"], mp["sz"], got)
+    e1.record()
+    ctx.sync()
+    ms = e0.elapsed_time(e1)
+    ctx.close()
+    g = got.cpu().numpy().reshape(-1).astype(np.float64)
+    r = ref_rec.astype(np.float64)
+    out["model_c1"] = {"nt": mp["nt"], "s_per_shot": round(sec, 4), "gpt_s": round(upd / sec / 1e9, 3),
+                       "this_library_s_per_shot": round(ms / 1e3, 4), "speedup": round(sec / (ms / 1e3), 2),
+                       "record_rel_l2_vs_this_library": float("%.3e" % (np.linalg.norm(g - r) / np.linalg.norm(g)))}
+    return out
+
+
+def c1_workload():
+    """The CPU-runnable modeling configuration (128^3 three-layer model, 32-cell border, 1000 steps)."""
+    n, blen = 128, 32
+    v = np.full((n, n, n), 3500.0, np.float32)
+    v[:, :, :40] = 1500.0
+    v[:, :, 40:80] = 2500.0
+    p = dict(nx=n, ny=n, nz=n, blen=blen, nt=1000, ntstep=1000, stencil_order=8, dx=10.0, dy=10.0, dz=10.0,
+             dt=0.001, fpeak=15.0, taper_factor=0.2, receiver_start_x=0, receiver_start_y=0, receiver_depth_z=4,
+             receiver_distance_x=2, receiver_distance_y=2, receiver_count_x=64, receiver_count_y=64,
+             boundary_condition="hbc", sx=64, sy=64, sz=4)
+    return p, v
 
 
 def run_b200(args, rank: int, world: int, local_rank: int) -> dict | None:
@@ -304,7 +439,7 @@ def run_b200(args, rank: int, world: int, local_rank: int) -> dict | None:
     mctx.load_v2dt2(v2m, from_host=True)
     mctx.model_shot(sx, sy, sz, rec)
     mctx.close()
-    del v2m
+    v2m_keep = v2m  # the modeling velocity, for the per-form record errors
 
     ctx = rtmb.Context(params)
     ctx.set_stream(stream.cuda_stream)
@@ -375,7 +510,7 @@ def run_b200(args, rank: int, world: int, local_rank: int) -> dict | None:
     if rank != 0:
         return None
     out = {
-        "metric": "G point-updates/s per migrated RTM shot (512^3 RBC, nt=3000)",
+        "metric": METRIC,
         "value": round(value, 3),
         "unit": "Gpt/s",
         "n_gpus": world,
@@ -405,16 +540,17 @@ def run_b200(args, rank: int, world: int, local_rank: int) -> dict | None:
                     if v_["launches"]},
         "clocks": clk,
     }
-    if world == 1 and args.forms_nt > 0:
+    if world == 1 and args.forms_nt >= 0:
         try:
-            out["forms"] = compare_forms(p, v2, rec, dev, min(args.forms_nt, p["nt"]))
+            nt_cmp = p["nt"] if args.forms_nt == 0 else min(args.forms_nt, p["nt"])
+            out["forms"] = compare_forms(p, v2, v2m_keep, rec, dev, nt_cmp)
         except Exception as exc:  # report, do not fail the headline measurement
             out["forms"] = {"failed": f"{exc}"[:300]}
     if world == 1 and not args.no_cpu_baseline:
         try:
             with tempfile.TemporaryDirectory() as wd:
-                nts = reference_sample_steps(p)
-                sec, upd_s, thr = run_reference_sample(p, v, vpe, rec.cpu().numpy(), nts, wd)
+                nts = args.ref_nt
+                sec, upd_s, thr, _ = run_reference_program(ref_cpu_bin(), p, v, rec.cpu().numpy(), nts, wd)
             out["cpu_baseline"] = {"value": round(upd_s / sec / 1e9, 4), "unit": "Gpt/s", "cores": thr,
                                    "kind": "reference",
                                    "sample": f"reference RTM3D.bin RBC migration of the same shot, nt={nts} "
@@ -423,6 +559,16 @@ def run_b200(args, rank: int, world: int, local_rank: int) -> dict | None:
         except Exception as exc:  # report, do not fail the GPU measurement
             out["cpu_baseline"] = {"value": None, "unit": "Gpt/s", "cores": os.cpu_count(), "kind": "reference",
                                    "sample": f"failed: {exc}"[:300]}
+    if world == 1 and not args.no_reference_gpu:
+        try:
+            out["reference_gpu"] = reference_gpu_bar(args, p, v, rec, value)
+        except Exception as exc:  # report, do not fail the GPU measurement
+            out["reference_gpu"] = {"failed": f"{exc}"[:300]}
+    if world == 1 and args.c3:
+        try:
+            out["precision_c3"] = run_precision(args, forms=C3_FORMS)
+        except Exception as exc:  # report, do not fail the headline measurement
+            out["precision_c3"] = {"failed": f"{exc}"[:300]}
     return out
 
 
@@ -564,47 +710,17 @@ def run_model(args) -> dict:
         out["forms"][form] = {"s_per_shot": round(ms / 1e3, 4), "gpt_s": round(npad * nt / ms / 1e6, 2)}
     out["value"] = out["forms"]["fp32_fma"]["gpt_s"]
     out["unit"] = "Gpt/s"
-    if not args.no_cpu_baseline:
-        from oracle import REF_BIN
-        if os.path.exists(REF_BIN):
-            nts = args.model_ref_nt
-            with tempfile.TemporaryDirectory() as wd:
-                for sub in ("out", "tmp", "dat"):
-                    os.makedirs(os.path.join(wd, sub), exist_ok=True)
-                vp = os.path.join(wd, "vel.bin")
-                v.tofile(vp)
-                threads = os.cpu_count() or 1
-                d = dict(mname="bench", vpfile=vp, vpefile=os.path.join(wd, "vpe.bin"), save_vpe_file=False,
-                         outdir=os.path.join(wd, "out"), tmpdir=os.path.join(wd, "tmp"), datdir=os.path.join(wd, "dat"),
-                         nx=n, ny=n, nz=n, blen=blen, width_m=0, height_m=0, depth_m=0, nt=nts, dz=10.0, dy=10.0,
-                         dx=10.0, dt=p["dt"], fpeak=p["fpeak"], fmax=30.0, taper_factor=p["taper_factor"],
-                         stencil_order=8, modeling=True, migration=False, rtm_type="rtm", boundary_condition="hbc",
-                         source_total=1, source_start_x=64, source_start_y=64, source_depth_z=4, source_distance_x=1,
-                         source_distance_y=1, source_count_x=1, source_count_y=1, receiver_total=64 * 64,
-                         receiver_start_x=0, receiver_start_y=0, receiver_depth_z=4, receiver_distance_x=2,
-                         receiver_distance_y=2, receiver_count_x=64, receiver_count_y=64, ntstep=nts,
-                         nthreads=threads, load_vpe_from_file=False, save_snapshots=False, distributed_grid=False,
-                         snapshot_step=10, fmig=False, fmig_max_freq=30.0, fmig_min_freq=1.0, fmig_nwstep=1,
-                         fmig_distributed_imaging=False, fpga_xclbin="", fpga_fwd_kernel="", fpga_bwd_kernel="",
-                         verbose=True)
-                jp = os.path.join(wd, "model.json")
-                with open(jp, "w") as f:
-                    json.dump(d, f)
-                r = subprocess.run([REF_BIN, jp], capture_output=True, text=True, cwd=wd, timeout=900)
-                t = None
-                for line in r.stdout.splitlines():
-                    if '"modeling_time"' in line:
-                        t = float(line.split(":")[1].strip().rstrip(","))
-                seism = os.path.join(wd, "dat", f"RTMSEISMOGRAM_S64x64x4_NXNY_64x64_NTSTART0_NTSTEP{nts}.seism")
-                ref_rec = np.fromfile(seism, np.float32) if os.path.exists(seism) else None
-            if t:
-                out["cpu_baseline"] = {"value": round(npad * nts / t / 1e9, 4), "unit": "Gpt/s", "cores": threads,
-                                       "kind": "reference",
-                                       "sample": f"RTM3D.bin modeling of the same shot, nt={nts}, its own modeling timer"}
-            if ref_rec is not None:
-                _, got = shot(0, nts)
-                out["record_vs_reference"] = {"nt": nts, "bitexact": bool(np.array_equal(
-                    got.reshape(-1).view(np.uint32), ref_rec.view(np.uint32)))}
+    if not args.no_cpu_baseline and os.path.exists(ref_cpu_bin()):
+        nts = args.model_ref_nt
+        with tempfile.TemporaryDirectory() as wd:
+            t, upd_r, threads, ref_rec = run_reference_program(ref_cpu_bin(), dict(p, ntstep=nts), v, None, nts, wd,
+                                                               migration=False)
+        out["cpu_baseline"] = {"value": round(upd_r / t / 1e9, 4), "unit": "Gpt/s", "cores": threads,
+                               "kind": "reference",
+                               "sample": f"RTM3D.bin modeling of the same shot, nt={nts}, its own modeling timer"}
+        _, got = shot(0, nts)
+        out["record_vs_reference"] = {"nt": nts, "bitexact": bool(np.array_equal(
+            got.reshape(-1).view(np.uint32), ref_rec.view(np.uint32)))}
     return out
 
 
@@ -779,38 +895,41 @@ def run_closure(args) -> dict:
 
 
 def run_reference_arm(args, rank: int) -> dict | None:
+    """The reference's own CPU program (oracle/_ref/RTM3D.bin, built from its sources) on the same
+    workload: an RBC migration of the same shot geometry with nt cut to --ref-nt steps per bench
+    step, every host thread, timed by the program's own migration timer.  Nothing of this
+    repository's library is loaded: the program builds its own random border, and the record is a
+    seeded random array of the record's shape (the CPU program's cost does not depend on its values)."""
     if rank != 0:
         return None
-    from oracle import REF_BIN
     p = workload(args.size, args.nt)
-    if not os.path.exists(REF_BIN):
+    binary = ref_cpu_bin()
+    if not os.path.exists(binary):
         return {"impl": "reference", "unavailable": "oracle/_ref/RTM3D.bin was not built from the reference sources"}
-    import rtmb
-    v = salt_model(p["nx"])
-    vpe = rtmb.prepare_velocity(v, p["blen"], "rbc", seed=1234)
-    nts = reference_sample_steps(p)
-    # a record of the right shape; the reference's cost does not depend on its values
+    v = salt_model(p["nx"], p["ny"], p["nz"])
+    nts = args.ref_nt
     rng = np.random.default_rng(5)
     rec = (rng.standard_normal((1, p["receiver_count_x"], p["receiver_count_y"], nts)) * 1e-3).astype(np.float32)
     secs, upds, thr = [], 0, 1
     with tempfile.TemporaryDirectory() as wd:
         for _ in range(args.warmup):
-            run_reference_sample(p, v, vpe, rec, nts, wd)
+            run_reference_program(binary, p, v, rec, nts, wd)
         for _ in range(args.steps):
-            s_, u_, thr = run_reference_sample(p, v, vpe, rec, nts, wd)
+            s_, u_, thr, _ = run_reference_program(binary, p, v, rec, nts, wd)
             secs.append(s_)
             upds += u_
     value = upds / sum(secs) / 1e9
     return {
         "impl": "reference",
-        "metric": "G point-updates/s per migrated RTM shot (512^3 RBC, nt=3000)",
+        "metric": METRIC,
         "value": round(value, 4), "unit": "Gpt/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(1e3 * sum(secs) / len(secs), 1), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded salt model)",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded salt model, seeded random record)",
         "config": {"workload": f"rtm_rbc_{args.size}^3_nt{args.nt}", "nt_sample": nts, "boundary": "rbc",
                    "stencil_order": 8},
         "cpu_baseline": {"value": round(value, 4), "unit": "Gpt/s", "cores": thr, "kind": "reference",
-                         "sample": f"RTM3D.bin RBC migration, nt={nts} per step, its own migration timer"},
+                         "sample": f"RTM3D.bin RBC migration, nt={nts} ({3 * nts - 2} sweeps of {n_points(p)} "
+                                   f"points) per step, its own migration timer"},
         "e2e": {"value": round(value, 4), "unit": "Gpt/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -825,10 +944,11 @@ def main():
     ap.add_argument("--nt", type=int, default=3000)
     ap.add_argument("--form", choices=FORMS, default="fp32_fma", help="arithmetic/storage form of the timed shots")
     ap.add_argument("--exact", action="store_true", help="same as --form fp32_exact")
-    ap.add_argument("--workload", choices=("rtm", "batch", "closure", "fmig", "model"), default="rtm",
+    ap.add_argument("--workload", choices=("rtm", "batch", "closure", "fmig", "model", "precision"), default="rtm",
                     help="rtm: the single-shot RTM line (default); batch: batched aperture shots against "
                          "one-by-one; closure: the learned boundary closure against the tapered borders; "
-                         "fmig: frequency-domain RTM of one shot; model: the 128^3 modeling configuration")
+                         "fmig: frequency-domain RTM of one shot; model: the 128^3 modeling configuration; "
+                         "precision: the 896 x 896 x 512 storage-form comparison against the FP64 oracle")
     ap.add_argument("--model-nt", type=int, default=1000)
     ap.add_argument("--model-ref-nt", type=int, default=200, help="steps of the reference program's timed sample")
     ap.add_argument("--fmig-size", type=int, default=192)
@@ -846,8 +966,17 @@ def main():
     ap.add_argument("--closure-steps", type=int, default=8000)
     ap.add_argument("--closure-candidates", type=int, default=3,
                     help="networks trained with different seeds; the one reflecting least on a validation shot is kept")
-    ap.add_argument("--forms-nt", type=int, default=300,
-                    help="nt of the storage-form comparison against the FP64 oracle (0: skip)")
+    ap.add_argument("--forms-nt", type=int, default=0,
+                    help="nt of the storage-form comparison against the FP64 oracle (0: the full nt; -1: skip)")
+    ap.add_argument("--ref-nt", type=int, default=8,
+                    help="steps of the reference CPU program's RBC migration sample (reference arm, cpu_baseline)")
+    ap.add_argument("--ref-gpu-nt", type=int, default=100,
+                    help="steps of the reference GPU program's RBC migration sample")
+    ap.add_argument("--no-reference-gpu", action="store_true", help="skip the reference GPU program bar")
+    ap.add_argument("--c3", dest="c3", action="store_true", default=True,
+                    help="add the precision configuration (896 x 896 x 512) to the default line (default)")
+    ap.add_argument("--no-c3", dest="c3", action="store_false")
+    ap.add_argument("--c3-grid", type=int, nargs=3, default=(896, 896, 512))
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.exact:
@@ -861,7 +990,8 @@ def main():
     if args.impl == "reference":
         out = run_reference_arm(args, rank)
     elif args.workload != "rtm":
-        runner = {"batch": run_batch, "closure": run_closure, "fmig": run_fmig, "model": run_model}[args.workload]
+        runner = {"batch": run_batch, "closure": run_closure, "fmig": run_fmig, "model": run_model,
+                  "precision": run_precision}[args.workload]
         out = runner(args) if rank == 0 else None
     else:
         if world > 1:

@@ -234,7 +234,10 @@ int rtmb_migrate_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, cons
  * v2dt2 (padded, device) and rec (device, file layout) and the stream (NULL: the legacy default
  * stream), and every other buffer lives in one 64 MiB device array inside the library that each GPU
  * loading the library holds until the process exits.  Grids up to about 8.3 million padded points
- * fit (two wavefields plus small tables); larger ones are rejected with RTMB_EINVAL.
+ * fit (two wavefields plus small tables); larger ones are rejected with RTMB_EINVAL, and so are
+ * blen above 1024 (the taper table goes up through a stack buffer of 1024 floats), the 16-bit
+ * storage flags and boundary RTMB_BC_LEARNED (both need a context), and v2dt2 or rec that are not
+ * device (or managed) memory of the call's device (checked with cudaPointerGetAttributes).
  *   - The first call on a device looks up that array's address (once per device, with the device
  *     current); make that first call before any stream capture on the device.
  *   - All calls on a device share the array and it keeps the previous call's contents; the entry

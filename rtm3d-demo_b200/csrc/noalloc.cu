@@ -45,6 +45,22 @@ int scratch_on(int dev, float **out) {
 
 size_t align_floats(size_t n) { return (n + 63) & ~size_t(63); }  // 256-byte sections
 
+// Longest taper table (blen) the entry point takes: the tables go up through a stack buffer of
+// this many floats.
+constexpr uint32_t kMaxBlen = 1024;
+
+// Is p memory that kernels on device dev may read and write: device memory of dev, or managed
+// memory?  cudaPointerGetAttributes allocates nothing.
+bool device_buffer(const void *p, int dev) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    if (at.type == cudaMemoryTypeManaged) return true;
+    return at.type == cudaMemoryTypeDevice && at.device == dev;
+}
+
 }  // namespace
 
 extern "C" int rtmb_model_shot_noalloc(const rtmb_params *params, const float *v2dt2, uint32_t sx, uint32_t sy,
@@ -57,6 +73,12 @@ extern "C" int rtmb_model_shot_noalloc(const rtmb_params *params, const float *v
         return fail_noctx(RTMB_EINVAL, "rtmb_model_shot_noalloc: invalid parameters");
     if (p.flags & (RTMB_FLAG_STORE_F16 | RTMB_FLAG_STORE_BF16 | RTMB_FLAG_IMG_F64))
         return fail_noctx(RTMB_EINVAL, "rtmb_model_shot_noalloc: the 16-bit storage forms need a context");
+    // the learned closure needs its parameters and strip tables, which only a context holds
+    if (p.boundary == RTMB_BC_LEARNED)
+        return fail_noctx(RTMB_EINVAL, "rtmb_model_shot_noalloc: boundary RTMB_BC_LEARNED needs a context");
+    // the taper table is uploaded through a 1024-float stack buffer
+    if (p.blen > kMaxBlen)
+        return fail_noctx(RTMB_EINVAL, "rtmb_model_shot_noalloc: blen above 1024");
 
     // a context on the stack: it owns nothing, every device pointer below points into g_scratch or
     // at the caller's buffers
@@ -80,6 +102,11 @@ extern "C" int rtmb_model_shot_noalloc(const rtmb_params *params, const float *v
     } else if (cudaSetDevice(dev) != cudaSuccess) {
         return fail_noctx(RTMB_ECUDA, "cudaSetDevice failed");
     }
+    // v2dt2 and rec go straight to the kernels: accept only device (or managed) memory of this
+    // device, so a host or stale pointer is an error here and not a fault on the GPU
+    if (!device_buffer(v2dt2, dev) || !device_buffer(rec, dev))
+        return fail_noctx(RTMB_EINVAL,
+                          "rtmb_model_shot_noalloc: v2dt2 and rec must be device memory of the call's device");
     float *scr = nullptr;
     int rc = scratch_on(dev, &scr);
     if (rc) return rc;
@@ -97,16 +124,15 @@ extern "C" int rtmb_model_shot_noalloc(const rtmb_params *params, const float *v
 
     // tables computed on the host (bit-identical to the reference) and copied into the scratch in
     // chunks through a stack buffer; each copy is complete before the buffer is refilled
-    if (p.blen > 1024) return fail_noctx(RTMB_EINVAL, "rtmb_model_shot_noalloc: blen above 1024");
-    float buf[1024];
+    float buf[kMaxBlen];
     bool ok = true;
     if (p.blen) {
         ok = rtmb_taper_vector(p.blen, p.taper_factor, buf) == RTMB_OK &&
              cudaMemcpyAsync(c.d_taper, buf, p.blen * sizeof(float), cudaMemcpyHostToDevice, c.stream) == cudaSuccess &&
              cudaStreamSynchronize(c.stream) == cudaSuccess;
     }
-    for (uint32_t i = 0; ok && i < p.nt; i += 1024) {
-        const uint32_t m = p.nt - i < 1024 ? p.nt - i : 1024;
+    for (uint32_t i = 0; ok && i < p.nt; i += kMaxBlen) {
+        const uint32_t m = p.nt - i < kMaxBlen ? p.nt - i : kMaxBlen;
         for (uint32_t k = 0; k < m; ++k) buf[k] = rtmb::ricker_sample(i + k, p.dt, p.fpeak);
         ok = cudaMemcpyAsync(c.d_wavelet + i, buf, m * sizeof(float), cudaMemcpyHostToDevice, c.stream) == cudaSuccess &&
              cudaStreamSynchronize(c.stream) == cudaSuccess;

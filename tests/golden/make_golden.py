@@ -9,9 +9,11 @@ The reference CPU program (oracle/_ref/RTM3D.bin, built from the reference's sou
   * mig_fmig.npz   -- frequency-domain RTM image (fmig = true) with its extended velocity
   * twod.npz       -- 2D model (nx = 1): record, HBC / RBC / fmig images and a 2D step vector
   * ops.npz        -- per-operator vectors from the reference CPU platform (oracle/_ref/librtmref.so)
+  * c1_model.npz   -- the full-size modeling configuration (128^3 + 32-cell border, 1000 steps): the
+                      SHA-256 of the reference's whole record and every 8th receiver's traces
 
 Run:  python tests/golden/make_golden.py [names...]   (needs oracle/_ref, i.e. the reference sources;
-      names: model mig ops fmig twod, default all)
+      names: model mig ops fmig twod c1, default all)
 """
 from __future__ import annotations
 
@@ -30,15 +32,16 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 from oracle import REF_BIN, Reference  # noqa: E402
-from rtm_cases import input_json, layered_model, CASES  # noqa: E402
+from rtm_cases import C1, c1_model, input_json, layered_model, record_digest, CASES  # noqa: E402
 
 
 FMIG = dict(fmig_min_freq=5.0, fmig_max_freq=40.0, fmig_nwstep=2)
 
 
-def run_reference(case: dict, mode: str, workdir: str, vpe_path: str | None = None, extra: dict | None = None):
+def run_reference(case: dict, mode: str, workdir: str, vpe_path: str | None = None, extra: dict | None = None,
+                  v: np.ndarray | None = None):
     """Run RTM3D.bin for one case. mode: 'model' | 'hbc' | 'rbc'. Returns output arrays."""
-    v = layered_model(case)
+    v = layered_model(case) if v is None else v
     vp = os.path.join(workdir, "vel.bin")
     v.tofile(vp)
     d = input_json(case, vpfile=vp, workdir=workdir)
@@ -109,9 +112,25 @@ def twod_fixture(wd_root: str):
     np.savez_compressed(os.path.join(HERE, "twod.npz"), **out)
 
 
-def main(names=("model", "mig", "ops", "fmig", "twod")):
+def c1_fixture():
+    """The full-size modeling configuration: the reference's record (64 x 64 receivers x 1000
+    steps, 16 MB) is kept as its SHA-256 and the traces of every 8th receiver in x and y."""
+    with tempfile.TemporaryDirectory() as wd:
+        d = run_reference(C1, "model", wd, v=c1_model())
+        rec = read_record(d)
+    np.savez_compressed(os.path.join(HERE, "c1_model.npz"), sha256=np.array(record_digest(rec)),
+                        shape=np.array(rec.shape), traces=rec[:, ::8, ::8, :].copy(),
+                        rms=np.array(float(np.sqrt(np.mean(rec.astype(np.float64) ** 2)))))
+
+
+def main(names=("model", "mig", "ops", "fmig", "twod", "c1")):
     if not os.path.exists(REF_BIN):
         raise SystemExit("oracle/_ref/RTM3D.bin missing: run `make -C oracle ref` first")
+    if "c1" in names:
+        c1_fixture()
+        if set(names) == {"c1"}:
+            print("golden fixtures written to", HERE)
+            return
     rng = np.random.default_rng(7)
     case = CASES["golden"]
     with tempfile.TemporaryDirectory() as wd:
@@ -162,4 +181,4 @@ def main(names=("model", "mig", "ops", "fmig", "twod")):
 
 
 if __name__ == "__main__":
-    main(tuple(sys.argv[1:]) or ("model", "mig", "ops", "fmig", "twod"))
+    main(tuple(sys.argv[1:]) or ("model", "mig", "ops", "fmig", "twod", "c1"))

@@ -21,6 +21,27 @@ CASES = {
                 rsx=0, rsy=0, rdz=4, rdx=2, rdy=2, rcx=40, rcy=36, seed=11),
 }
 
+# The CPU-runnable modeling configuration at full size: 128^3 at 10 m, three layers (1500, 2500 and
+# 3500 m/s from depths 0, 40 and 80 cells), 32-cell border, 1000 steps of 1 ms, 15 Hz Ricker at
+# (64, 64, 4), 64 x 64 receivers every 2 cells at depth 4, order 8; the record in four 250-step chunks.
+C1 = dict(nx=128, ny=128, nz=128, blen=32, nt=1000, ntstep=250, order=8, dx=10.0, dy=10.0, dz=10.0,
+          dt=0.001, fpeak=15.0, taper_factor=0.2, sx=64, sy=64, sz=4,
+          rsx=0, rsy=0, rdz=4, rdx=2, rdy=2, rcx=64, rcy=64)
+
+
+def c1_model() -> np.ndarray:
+    """The three-layer velocity of C1 (x slowest, z fastest)."""
+    v = np.full((C1["nx"], C1["ny"], C1["nz"]), 3500.0, np.float32)
+    v[:, :, :40] = 1500.0
+    v[:, :, 40:80] = 2500.0
+    return v
+
+
+def record_digest(rec) -> str:
+    """SHA-256 of a record's float32 bytes in file layout (chunk, rcx, rcy, ntstep)."""
+    import hashlib
+    return hashlib.sha256(np.ascontiguousarray(rec, np.float32).tobytes()).hexdigest()
+
 
 def layered_model(case: dict) -> np.ndarray:
     """Three layers plus a little seeded roughness, x slowest, z fastest."""
