@@ -254,14 +254,23 @@ def build_inputs(p: dict, with_abc: bool):
     return v, vpe, v2, v2m
 
 
-FORMS = ("fp32_exact", "fp32_fma", "fp16", "bf16", "fp16_img64", "bf16_img64")
-C3_FORMS = ("fp32_exact", "fp32_fma", "fp16", "bf16")
+FORMS = ("fp32_exact", "fp32_fma", "fp16", "bf16", "fp16_img64", "bf16_img64", "fp16_diff", "bf16_diff",
+         "fp16_diff_img64")
+C3_FORMS = ("fp32_exact", "fp32_fma", "fp16", "bf16", "fp16_diff", "bf16_diff")
 
 
 def form_flags(rtmb, form: str) -> int:
-    return {"fp32_exact": 0, "fp32_fma": rtmb.FLAG_FAST_FMA, "fp16": rtmb.FLAG_STORE_F16,
-            "bf16": rtmb.FLAG_STORE_BF16, "fp16_img64": rtmb.FLAG_STORE_F16 | rtmb.FLAG_IMG_F64,
-            "bf16_img64": rtmb.FLAG_STORE_BF16 | rtmb.FLAG_IMG_F64}[form]
+    """Flags of a form: fp32_exact (bit-exact with the reference CPU path), fp32_fma, 16-bit storage
+    of the two levels (fp16, bf16), of the level and its increment (*_diff), FP64 image (*_img64)."""
+    f = {"fp32_exact": 0, "fp32_fma": rtmb.FLAG_FAST_FMA}.get(form)
+    if f is not None:
+        return f
+    f = rtmb.FLAG_STORE_F16 if form.startswith("fp16") else rtmb.FLAG_STORE_BF16
+    if "_diff" in form:
+        f |= rtmb.FLAG_STORE_DIFF
+    if form.endswith("_img64"):
+        f |= rtmb.FLAG_IMG_F64
+    return f
 
 
 def rel_l2_dev(a, ref, ref_norm: float) -> float:
@@ -319,7 +328,9 @@ def compare_forms(p: dict, v2: np.ndarray, v2m: np.ndarray | None, rec_full, dev
         r = {"ms_per_sweep": round(per_sweep, 4), "s_per_shot": round(per_sweep * sweeps_full / 1e3, 3),
              "gpt_s": round(n_points(p) / (per_sweep * 1e-3) / 1e9, 2),
              "image_rel_l2_vs_fp64": float("%.3e" % rel_l2_dev(img, ref, ref_norm))}
-        if rec_ref is not None:
+        if rec_ref is not None and "_diff" in name:
+            r["record_rel_l2_vs_fp64"] = None  # the increment form runs RBC migration only, no modeling
+        elif rec_ref is not None:
             mc = rtmb.Context(rtmb.Params.from_input(dict(q, boundary_condition="hbc"), flags=fl, device=d))
             mc.load_v2dt2(v2m, from_host=True)
             got = torch.zeros(rec.shape, dtype=torch.float32, device=dev)

@@ -101,6 +101,16 @@ typedef enum rtmb_boundary {
  * 16-byte aligned, no RTMB_FLAG_NO_TMA); this flag keeps the raw fields and tapers on load (no
  * reference counterpart). */
 #define RTMB_FLAG_NO_TAPER_STORE 0x400u
+/* With a 16-bit storage flag: store each wavefield as its current level p(t) and its increment
+ * d(t) = p(t) - p(t-1) instead of the two levels p(t) and p(t-1), and step as
+ * d(t+1) = d(t) + v2dt2 lap p(t), p(t+1) = p(t) + d(t+1): algebraically the same leapfrog.
+ * In the two-level form 2p - p(t-1) cancels most of its digits, so the rounding of the stored
+ * p(t-1) lands in full on the small difference that carries the wave's time derivative; stored as
+ * its own 16-bit value with its own exponent, the increment keeps its relative precision.  Each
+ * level and each increment has its own power-of-two exponent.  12 bytes per point and step instead
+ * of 10 (both levels' increments are written), against 16 for FP32.  RBC migration only (no taper
+ * in the steps); no reference counterpart. */
+#define RTMB_FLAG_STORE_DIFF    0x800u
 
 /* The input.json parameters on the path (include/RTMParam.hpp:188-249). */
 typedef struct rtmb_params {

@@ -167,7 +167,7 @@ size_t wave_bytes(const rtmb_ctx *c) { return c->n * (c->store == rtmb::kStoreF3
 // Scale records of the storage forms: a pool of 3 nt + 8 records per shot (forward levels, rebuilt
 // source levels, receiver levels), cleared at the start of each shot.
 int reset_scales(rtmb_ctx *ctx) {
-    const int need = 3 * (int)ctx->p.nt + 8;
+    const int need = (ctx->diff ? 6 : 3) * (int)ctx->p.nt + 16;  // increment storage: two records per step
     if (ctx->sc_cap < need) {
         if (ctx->d_scale) CK(cudaFree(ctx->d_scale));
         ctx->d_scale = nullptr;
@@ -375,6 +375,10 @@ int alloc_driver(rtmb_ctx *ctx) {
         int rc = ensure(ctx, &ctx->d_inj, 2, true);
         if (rc) return rc;
     }
+    for (int k = 0; ctx->diff && k < 2; ++k) {
+        int rc = ensure_bytes(ctx, &ctx->d_inc[k], wave_bytes(ctx), false);
+        if (rc) return rc;
+    }
     return RTMB_OK;
 }
 
@@ -432,6 +436,8 @@ int rtmb_create(const rtmb_params *params, rtmb_ctx **out) {
         return rtmb::driver::fail_noctx(RTMB_EINVAL, "rtmb_create: choose one of RTMB_FLAG_STORE_F16 and _BF16");
     if ((p.flags & RTMB_FLAG_IMG_F64) && !sf)
         return rtmb::driver::fail_noctx(RTMB_EINVAL, "rtmb_create: RTMB_FLAG_IMG_F64 needs a 16-bit storage flag");
+    if ((p.flags & RTMB_FLAG_STORE_DIFF) && !sf)
+        return rtmb::driver::fail_noctx(RTMB_EINVAL, "rtmb_create: RTMB_FLAG_STORE_DIFF needs a 16-bit storage flag");
     if (sf && !rtmb::storage_form_supported((int)p.stencil_order, (int)(p.nz + 2 * p.blen)))
         return rtmb::driver::fail_noctx(RTMB_EINVAL,
                                         "rtmb_create: the 16-bit storage forms need stencil_order 8 and nz + 2*blen "
@@ -440,6 +446,7 @@ int rtmb_create(const rtmb_params *params, rtmb_ctx **out) {
     ctx->p = p;
     ctx->store = sf == RTMB_FLAG_STORE_F16 ? rtmb::kStoreF16 : (sf ? rtmb::kStoreBF16 : rtmb::kStoreF32);
     ctx->img64 = (p.flags & RTMB_FLAG_IMG_F64) != 0;
+    ctx->diff = (p.flags & RTMB_FLAG_STORE_DIFF) != 0;
     rtmb::driver::init_geometry(ctx);
     auto bail = [&](int code) {
         rtmb_destroy(ctx);
@@ -486,6 +493,8 @@ int rtmb_destroy(rtmb_ctx *ctx) {
     if (ctx->d_scale) cudaFree(ctx->d_scale);
     if (ctx->d_inj) cudaFree(ctx->d_inj);
     if (ctx->d_img64) cudaFree(ctx->d_img64);
+    for (void *b : ctx->d_inc)
+        if (b) cudaFree(b);
     for (double *b : ctx->d_f64)
         if (b) cudaFree(b);
     if (ctx->d_upb64) cudaFree(ctx->d_upb64);
@@ -661,6 +670,7 @@ int rtmb_model_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, float 
     if (learned && !ctx->d_cparams) return fail(ctx, RTMB_EINVAL, "boundary RTMB_BC_LEARNED needs rtmb_closure_set");
     if (learned && ctx->store != rtmb::kStoreF32)
         return fail(ctx, RTMB_EINVAL, "the learned closure runs with FP32 storage");
+    if (ctx->diff) return fail(ctx, RTMB_EINVAL, "the increment storage form (RTMB_FLAG_STORE_DIFF) runs RBC migration only");
     // the learned closure: the strip's next level before each step, scattered after it
     struct Closure : rtmb::driver::StepHook {
         rtmb_ctx *c;
@@ -688,6 +698,121 @@ int rtmb_model_shot(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, float 
 
 namespace {
 
+// RBC migration in the increment storage form (RTMB_FLAG_STORE_DIFF): each wavefield is a 16-bit
+// level p and a 16-bit increment d = p - p_prev, each with its own exponent; the steps write
+// d' = d + v2dt2 lap p in place and p' = p + d' into the other level buffer.  The same time loop
+// as the two-level drivers (RBC.cpp:54-274): forward from zero, the backward pass rebuilds the
+// source wavefield from the forward pass's last two levels and images it against the receiver
+// wavefield.  img: the FP32 image (overwritten), the FP64 image of RTMB_FLAG_IMG_F64, or with acc64
+// the caller's FP64 stack (added to).
+int migrate_diff(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const float *rec, void *img_out, bool acc64) {
+    const rtmb_params &p = ctx->p;
+    if (p.boundary != RTMB_BC_RBC)
+        return fail(ctx, RTMB_EINVAL, "the increment storage form (RTMB_FLAG_STORE_DIFF) migrates with boundary RBC");
+    int rc;
+    if ((rc = alloc_driver(ctx))) return rc;
+    if ((rc = reset_scales(ctx))) return rc;
+    if (ctx->img64 && !acc64 &&
+        (rc = ensure_bytes(ctx, reinterpret_cast<void **>(&ctx->d_img64), ctx->n * sizeof(double), false)))
+        return rc;
+    const size_t nb = wave_bytes(ctx);
+    for (int k = 0; k < 4; ++k) CK(cudaMemsetAsync(ctx->d_w[k], 0, nb, ctx->stream));
+    for (int k = 0; k < 2; ++k) CK(cudaMemsetAsync(ctx->d_inc[k], 0, nb, ctx->stream));
+    GraphScope graph(ctx, 1);
+    if ((rc = graph.begin())) return rc;
+
+    // one wavefield: level buffers cur / next, increment d, and their scale records
+    struct Wave {
+        float *cur, *next;
+        void *d;
+        rtmb::ScaleRec *sc_cur, *sc_d;
+    };
+    auto fresh = [&](Wave &w, float *a, float *b, void *d) -> int {
+        w.cur = a; w.next = b; w.d = d;
+        if (!(w.sc_cur = new_scale(ctx)) || !(w.sc_d = new_scale(ctx)))
+            return fail(ctx, RTMB_EINVAL, "scale record pool exhausted");
+        return RTMB_OK;
+    };
+    // one step of w: (cur, d) -> (next, d in place), the records of the new level and increment
+    auto step = [&](Wave &w, rtmb::StepArgs &a, int cat) -> int {
+        rtmb::ScaleRec *lp = new_scale(ctx), *ld = new_scale(ctx);
+        if (!lp || !ld) return fail(ctx, RTMB_EINVAL, "scale record pool exhausted");
+        a.P = w.cur; a.PP = static_cast<float *>(w.d); a.Pout = w.next;
+        a.sc_p = w.sc_cur; a.sc_pp = w.sc_d; a.sc_out = lp; a.sc_out2 = ld;
+        LAUNCH_CAT(cat, rtmb::launch_step(a, (int)p.stencil_order, false, ctx->stream, true));
+        std::swap(w.cur, w.next);
+        w.sc_cur = lp;
+        w.sc_d = ld;
+        return RTMB_OK;
+    };
+    Wave S, R;
+    if ((rc = fresh(S, ctx->d_w[0], ctx->d_w[1], ctx->d_inc[0])) || (rc = fresh(R, ctx->d_w[2], ctx->d_w[3], ctx->d_inc[1])))
+        return rc;
+
+    // forward pass (RBC.cpp:54-144): source injection, no taper, no record
+    rtmb::StepArgs a = base_args(ctx);
+    a.V = ctx->d_v2dt2;
+    a.store = ctx->store;
+    a.diff = 1;
+    a.inj = ctx->wmax;
+    a.sxe = (int)(sx + p.blen); a.sye = (int)(sy + p.blen); a.sze = (int)(sz + p.blen);
+    for (uint32_t it = 0; it < p.nt; ++it) {
+        a.it = (int)it;
+        if ((rc = step(S, a, RTMB_PROF_FORWARD))) return rc;
+    }
+
+    void *img = img_out;
+    bool img64 = acc64;
+    if (!acc64 && ctx->img64) {
+        img = ctx->d_img64;
+        img64 = true;
+    }
+    if (!acc64) CK(cudaMemsetAsync(img, 0, ctx->n * (img64 ? sizeof(double) : sizeof(float)), ctx->stream));
+    const size_t nrec = (size_t)p.nt * p.receiver_count_x * p.receiver_count_y;
+    LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_absmax(rec, nrec, ctx->d_inj, ctx->stream));
+
+    // backward pass (RBC.cpp:146-274): it = nt-1 images p(nt); it = nt-2 images p(nt-1), rebuilt
+    // from the last level and increment; below, each source step rebuilds p(it+1)
+    rtmb::StepArgs src = base_args(ctx);
+    src.V = ctx->d_v2dt2;
+    src.store = ctx->store;
+    src.diff = 1;
+    rtmb::StepArgs rcv = base_args(ctx);
+    rcv.V = ctx->d_v2dt2;
+    rcv.store = ctx->store;
+    rcv.diff = 1;
+    const bool full = p.flags & RTMB_FLAG_IMG_FULL_Z;
+    rcv.img = static_cast<float *>(img);
+    rcv.img64 = img64;
+    rcv.img_z0 = full ? 0 : (int)p.blen;
+    rcv.img_z1 = full ? ctx->nze : ctx->nze - (int)p.blen;
+    rcv.inj_dev = ctx->d_inj;
+    const int rmode = (p.flags & RTMB_FLAG_RCV_ADD) ? rtmb::kRecAdd : rtmb::kRecOverwrite;
+    for (int it = (int)p.nt - 1; it >= 0; --it) {
+        if (it == (int)p.nt - 2) {
+            rtmb::ScaleRec *lp = new_scale(ctx);
+            if (!lp) return fail(ctx, RTMB_EINVAL, "scale record pool exhausted");
+            LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_diff_rewind(ctx->store, S.cur, S.d, S.next, S.sc_cur, S.sc_d, lp,
+                                                                 ctx->n, ctx->stream));
+            std::swap(S.cur, S.next);
+            S.sc_cur = lp;
+        } else if (it < (int)p.nt - 2) {
+            src.it = it;
+            if ((rc = step(S, src, RTMB_PROF_BACKWARD_SOURCE))) return rc;
+        }
+        rcv.it = it;
+        rcv.ps = S.cur;
+        rcv.sc_ps = S.sc_cur;
+        set_receivers(rcv, ctx, rmode, const_cast<float *>(rec), it);
+        if ((rc = step(R, rcv, RTMB_PROF_BACKWARD_RECEIVER))) return rc;
+    }
+    if (img != img_out)
+        LAUNCH_CAT(RTMB_PROF_OTHER, rtmb::launch_to_float(ctx->d_img64, static_cast<float *>(img_out), ctx->n,
+                                                          ctx->stream));
+    if ((rc = graph.end())) return rc;
+    return check_err_flag(ctx);
+}
+
 // The migration of one shot.  img_out: the caller's FP32 image (overwritten) or, with acc64, the
 // caller's FP64 stack (added to).
 int migrate_impl(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const float *rec, void *img_out,
@@ -700,6 +825,7 @@ int migrate_impl(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const flo
     if (p.receiver_depth_z + p.blen >= (uint32_t)ctx->nze - ctx->h)
         return fail(ctx, RTMB_EINVAL, "receiver depth outside the computed region");
     const bool st = ctx->store != rtmb::kStoreF32;
+    if (ctx->diff) return migrate_diff(ctx, sx, sy, sz, rec, img_out, acc64);
     if (!st && acc64) {
         // FP32 storage: the FP32 shot image, then added to the FP64 stack
         if ((rc = ensure(ctx, &ctx->d_img, ctx->n, false))) return rc;
@@ -1081,6 +1207,7 @@ int rtmb_migrate_batch(rtmb_ctx *ctx, uint32_t nshots, const rtmb_shot *shots, d
     if (!ctx || !shots || !stack) return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: null pointer");
     const rtmb_params &p = ctx->p;
     if (nshots == 0 || nshots > 12) return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: 1 to 12 shots per batch");
+    if (ctx->diff) return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: the increment storage form runs single shots");
     if (p.boundary != RTMB_BC_RBC || p.stencil_order != 8 || (int)p.blen < ctx->h || p.nx == 1)
         return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: boundary RBC, stencil_order 8, blen >= 4, 3D (nx > 1)");
     const bool st = ctx->store != rtmb::kStoreF32;

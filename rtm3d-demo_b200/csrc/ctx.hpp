@@ -31,6 +31,8 @@ struct rtmb_ctx {
     // storage forms (RTMB_FLAG_STORE_*): element type of d_w, one scale record per stored level
     int store = rtmb::kStoreF32;
     bool img64 = false;              // RTMB_FLAG_IMG_F64
+    bool diff = false;               // RTMB_FLAG_STORE_DIFF: d_w[0..1] / [2..3] hold p levels, d_inc the increments
+    void *d_inc[2] = {};             // increment of the source and of the receiver wavefield
     float wmax = 0.f;                // max |Ricker sample|
     rtmb::ScaleRec *d_scale = nullptr;
     int sc_cap = 0, sc_next = 0;

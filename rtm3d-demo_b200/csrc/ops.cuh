@@ -71,6 +71,11 @@ cudaError_t launch_upb(double *P, double *upb, int lt, int rw, const Geom &g, cu
 cudaError_t launch_image(double *img, const double *ps, const double *pr, int z0, int z1, const Geom &g,
                          cudaStream_t s);
 
+// Increment storage (RTMB_FLAG_STORE_DIFF): from the forward pass's last level p and increment d
+// (16-bit, StoreType store, records sp and sd) to the backward pass's start: pout = p - d (record so,
+// written here), d = -d in place.  n % 8 == 0.
+cudaError_t launch_diff_rewind(int store, const void *p, void *d, void *pout, const ScaleRec *sp, const ScaleRec *sd,
+                               ScaleRec *so, size_t n, cudaStream_t s);
 // *out = max |x| over n floats.
 cudaError_t launch_absmax(const float *x, size_t n, float *out, cudaStream_t s);
 // *out = max amax over n scale records.

@@ -101,8 +101,9 @@ cudaError_t launch_step(const StepArgs &a, int order, bool exact, cudaStream_t s
     dim3 grid((a.nze + kTZ - 1) / kTZ, (nyi + kTY - 1) / kTY, (nxi + a.chunk - 1) / a.chunk);
     const uintptr_t al = reinterpret_cast<uintptr_t>(a.P) | reinterpret_cast<uintptr_t>(a.PP) |
                          reinterpret_cast<uintptr_t>(a.V) | reinterpret_cast<uintptr_t>(a.img) |
-                         reinterpret_cast<uintptr_t>(a.ps);
+                         reinterpret_cast<uintptr_t>(a.ps) | reinterpret_cast<uintptr_t>(a.Pout);
     const bool aligned = (a.nze % 4 == 0) && (al % 16 == 0);
+    if (a.diff && a.store == kStoreF32) return cudaErrorInvalidValue;  // increment storage: 16-bit forms
     if (a.store != kStoreF32 || a.img64) {
         if (!storage_form_supported(order, a.nze) || al % 16 != 0 || a.store == kStoreF32)
             return cudaErrorInvalidValue;

@@ -101,6 +101,12 @@ struct StepArgs {
     // 2D models (nx == 1, the reference's rtmStep2D): computed planes restricted to [x_lo, x_hi)
     // when x_hi > 0, with the x coefficients zero (so lap = acmy + acmz exactly)
     int x_lo, x_hi;
+    // increment storage (16-bit forms only): P holds p(t), PP the increment d(t) = p(t) - p(t-1),
+    // updated in place to d(t+1); p(t+1) goes to Pout.  sc_pp is d(t)'s record, sc_out p(t+1)'s,
+    // sc_out2 d(t+1)'s.
+    int diff;
+    void *Pout;
+    ScaleRec *sc_out2;
 };
 
 // Exponent of a produced level: the smallest e with bound * 2^-e < 2^15.  bound is

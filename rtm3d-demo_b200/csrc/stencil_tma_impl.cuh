@@ -264,15 +264,19 @@ __device__ __forceinline__ void taper_tile(T *st, const float *tab, const StepAr
 // IMG: the epilogue accumulates the image.
 // T: storage type of P, PP and ps (float: the FP32 form, bit-identical to the plain-load kernel;
 // __half / __nv_bfloat16: scaled 16-bit storage).  IT: image type (float or double).
+// DF: increment storage (16-bit forms, no taper): the core ring's first tile is the increment
+// d(t) = p(t) - p(t-1) instead of p(t-1); the launch writes d(t+1) = d(t) + v2dt2 lap p(t) in place
+// and p(t+1) = p(t) + d(t+1) to StepArgs::Pout, each with its own exponent.
 // The body of one CTA: the tile (bx, by) of the (z, y) plane and x chunk bz of the volume that
 // (maps, a) describe; the stencil coefficients come from coef (for the compiler, a kernel
 // parameter at a fixed offset, so the FMAs take them straight from the constant bank).
-template <int H, bool EXACT, int TAPER, bool IMG, typename T, typename IT>
+template <int H, bool EXACT, int TAPER, bool IMG, typename T, typename IT, bool DF = false>
 __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArgs &a, const StepArgs &coef, int bx,
                                               int by, int bz) {
     using S = TmaShape<H, IMG, T, IT>;
     using ST = Stor<T>;
     constexpr bool SC = ST::kScaled;
+    static_assert(!DF || (SC && TAPER == kTaperNone), "increment storage: 16-bit forms without taper");
     // ALL: every face tapered; UPPER: the upper border only; TWS: the fields are stored tapered
     constexpr bool ALL = TAPER == kTaperAll || TAPER == kTaperAllStored;
     constexpr bool UPPER = TAPER == kTaperUpper || TAPER == kTaperUpperStored;
@@ -370,18 +374,35 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
 
     // ---- scales of the 16-bit forms: the stored levels hold value * 2^-e
     float sP = 1.f, sPP = 1.f, sPS = 1.f, sOutInv = 1.f, sPPinv = 1.f, sKeep = 1.f;
+    float sDInv = 1.f, sKeepP = 1.f;  // increment storage: d(t+1)'s inverse scale, p re-store factor
     if constexpr (SC) {
         const ScaleRec rp = *a.sc_p, rpp = *a.sc_pp;
         sP = exp2i(rp.e);
         sPP = exp2i(rpp.e);
         sPPinv = exp2i(-rpp.e);
         if (IMG) sPS = exp2i(a.sc_ps->e);
-        const float bound = 8.f * fmaxf(__uint_as_float(rp.amax), __uint_as_float(rpp.amax)) + a.inj +
-                            (a.inj_dev ? *a.inj_dev : 0.f);
-        const int eN = storage_exponent(bound);
-        sOutInv = exp2i(-eN);
-        sKeep = exp2i(max(-126, min(127, rpp.e - eN)));  // re-stores cells outside the computed region
-        if (tid == 0 && bx == 0 && by == 0 && bz == 0) a.sc_out->e = eN;
+        const float inj = a.inj + (a.inj_dev ? *a.inj_dev : 0.f);
+        const float ap = __uint_as_float(rp.amax), app = __uint_as_float(rpp.amax);
+        if constexpr (DF) {
+            // |d(t+1)| <= |d(t)| + 4 max|p(t)| + injection (a stable step: v2dt2 sum|coef| <= 4),
+            // |p(t+1)| <= |p(t)| + |d(t+1)|; a receiver overwrite gives |d| <= |p| + |record|
+            const float bd = app + 4.f * ap + inj;
+            const int eD = storage_exponent(bd), eP = storage_exponent(ap + bd);
+            sOutInv = exp2i(-eP);
+            sDInv = exp2i(-eD);
+            sKeep = exp2i(max(-126, min(127, rpp.e - eD)));  // cells outside the computed region
+            sKeepP = exp2i(max(-126, min(127, rp.e - eP)));
+            if (tid == 0 && bx == 0 && by == 0 && bz == 0) {
+                a.sc_out->e = eP;
+                a.sc_out2->e = eD;
+            }
+        } else {
+            const float bound = 8.f * fmaxf(ap, app) + inj;
+            const int eN = storage_exponent(bound);
+            sOutInv = exp2i(-eN);
+            sKeep = exp2i(max(-126, min(127, rpp.e - eN)));  // re-stores cells outside the computed region
+            if (tid == 0 && bx == 0 && by == 0 && bz == 0) a.sc_out->e = eN;
+        }
     }
 
     // ---- per-thread constants, hoisted out of the plane loop.  The rare per-cell work (source,
@@ -446,6 +467,7 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
     float4 q[NQ];
     float nanacc = 0.f;  // stays 0 unless a NaN or an infinity is written
     float amax = 0.f;    // max |value| written (16-bit forms)
+    float amaxd = 0.f;   // max |increment| written (increment storage)
     // running ring positions: plane kin = i + 2H (slot, parity), the centre plane i + H (slot), the
     // core plane i (slot, parity)
     int s_in = (2 * H) % D, ph_in = ((2 * H) / D) & 1, s_mid = H % D, s_core = 0, ph_core = 0;
@@ -660,9 +682,13 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                 }
             }
             float npp[kVZ];
+            float dn[kVZ];  // increment storage: d(t+1)
 #pragma unroll
             for (int e = 0; e < kVZ; ++e) {
-                if (EXACT) {
+                if (DF) {  // d(t+1) = d(t) + v2dt2 lap p(t), p(t+1) = p(t) + d(t+1)
+                    dn[e] = fmaf(get(vv, e), lap[e] * sP, ppv[e] * sPP);
+                    npp[e] = fmaf(get(qc, e), sP, dn[e]);
+                } else if (EXACT) {
                     const float two_p = 2.f * get(qc, e);
                     const float d = two_p - ppv[e];
                     const float vl = get(vv, e) * lap[e];
@@ -679,13 +705,23 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                 for (int e = 0; e < kVZ; ++e) {
                     const int z = z0 + e;
                     const bool v = (vmask >> e) & 1u;
-                    if (x == a.sxe && y == a.sye && z == a.sze && v) npp[e] = npp[e] + __ldg(a.wavelet + a.it);
+                    if (x == a.sxe && y == a.sye && z == a.sze && v) {
+                        const float w = __ldg(a.wavelet + a.it);
+                        npp[e] = npp[e] + w;
+                        if (DF) dn[e] = dn[e] + w;
+                    }
                     if (REC && e == rec_e) {
                         float *rp = const_cast<float *>(rec_p);
                         const float rv = IMG ? rec_v : *rp;
-                        if (a.rec_mode == kRecSample) *rp = npp[e];
-                        else if (a.rec_mode == kRecOverwrite) npp[e] = rv;
-                        else npp[e] = npp[e] + rv;
+                        if (a.rec_mode == kRecSample) {
+                            *rp = npp[e];
+                        } else if (a.rec_mode == kRecOverwrite) {
+                            if (DF) dn[e] = rv - get(qc, e) * sP;  // p(t+1) = record, d(t+1) = record - p(t)
+                            npp[e] = rv;
+                        } else {
+                            npp[e] = npp[e] + rv;
+                            if (DF) dn[e] = dn[e] + rv;
+                        }
                     }
                     if (upb_cta && v && z >= a.blen - H && z < a.blen) {
                         float *up = a.upb + ((size_t)x * a.nye + y) * H + (z - (a.blen - H));
@@ -747,8 +783,25 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                 }
             }
             float4 out;
+            if constexpr (DF) {  // d(t+1) in place, p(t+1) to Pout
+                float4 od;
 #pragma unroll
-            for (int e = 0; e < kVZ; ++e) {
+                for (int e = 0; e < kVZ; ++e) {
+                    const bool v = (vmask >> e) & 1u;
+                    put(od, e, v ? dn[e] * sDInv : get(pp_raw, e) * sKeep);
+                    put(out, e, v ? npp[e] * sOutInv : get(qc, e) * sKeepP);
+                    if (v) {
+                        amax = fmaxf(amax, fabsf(npp[e]));
+                        amaxd = fmaxf(amaxd, fabsf(dn[e]));
+                    }
+                    nanacc = fmaf(0.f, npp[e], nanacc);
+                    nanacc = fmaf(0.f, dn[e], nanacc);
+                }
+                ST::st4(PPp + (size_t)x * plane, od);
+                ST::st4(reinterpret_cast<T *>(a.Pout) + row_off + (size_t)x * plane, out);
+            }
+#pragma unroll
+            for (int e = 0; e < kVZ && !DF; ++e) {
                 const bool v = (vmask >> e) & 1u;
                 float o;
                 if (SC) {
@@ -761,7 +814,9 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                 }
                 put(out, e, o);
             }
-            if (TWS && q_cta && x < a.blen && y >= a.nye - a.blen) {  // quirk cells: plane blen's CTA writes them
+            if (DF) {
+                // stored above
+            } else if (TWS && q_cta && x < a.blen && y >= a.nye - a.blen) {  // quirk cells: plane blen's CTA writes them
 #pragma unroll
                 for (int e = 0; e < kVZ; ++e) {
                     const int z = z0 + e;
@@ -796,6 +851,10 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
     if constexpr (SC) {
         const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(amax));
         if (lane == 0 && m) atomicMax(&a.sc_out->amax, m);
+        if constexpr (DF) {
+            const unsigned md = __reduce_max_sync(0xffffffffu, __float_as_uint(amaxd));
+            if (lane == 0 && md) atomicMax(&a.sc_out2->amax, md);
+        }
     }
     return;
 
@@ -804,10 +863,10 @@ drain:
     if (a.err) atomicOr(a.err, 2u);
 }
 
-template <int H, bool EXACT, int TAPER, bool IMG, typename T = float, typename IT = float>
+template <int H, bool EXACT, int TAPER, bool IMG, typename T = float, typename IT = float, bool DF = false>
 __global__ void __launch_bounds__(kTmaThreads, 2)
     tma_step_kernel(const __grid_constant__ TmaMaps maps, const __grid_constant__ StepArgs a) {
-    tma_step_body<H, EXACT, TAPER, IMG, T, IT>(maps, a, a, blockIdx.x, blockIdx.y, blockIdx.z);
+    tma_step_body<H, EXACT, TAPER, IMG, T, IT, DF>(maps, a, a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Several volumes in one launch (the batched multi-shot drivers): shot s owns the linear blocks
@@ -892,12 +951,13 @@ cudaError_t launch_tma_h(const TmaMaps &maps, const StepArgs &a, bool exact, int
 template <typename T>
 cudaError_t launch_tma_store(const TmaMaps &maps, const StepArgs &a, int taper, bool img, bool img64, dim3 grid,
                              cudaStream_t s) {
-    static unsigned long long attr_done[12] = {};
+    static unsigned long long attr_done[16] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (a.tw & kTwStored) taper = taper == kTaperAll ? kTaperAllStored : -1;  // 16-bit forms: modeling only
     if (taper < 0) return cudaErrorInvalidValue;
-    const int variant = (img ? (img64 ? 8 : 4) : 0) + taper;
+    if (a.diff && (taper != kTaperNone || !a.Pout || !a.sc_out2)) return cudaErrorInvalidValue;
+    const int variant = a.diff ? 12 + (img ? (img64 ? 2 : 1) : 0) : (img ? (img64 ? 8 : 4) : 0) + taper;
     auto run = [&](void (*kern)(TmaMaps, StepArgs), size_t smem) -> cudaError_t {
         const unsigned long long bit = 1ull << (dev & 63);
         if (!(attr_done[variant] & bit)) {
@@ -909,8 +969,15 @@ cudaError_t launch_tma_store(const TmaMaps &maps, const StepArgs &a, int taper, 
         return cudaGetLastError();
     };
 #define RTMB_TMA_STORE_CASE(TP, IM, IT)                                                          \
-    if (taper == TP && img == IM && (!IM || img64 == (sizeof(IT) == 8)))                         \
+    if (!a.diff && taper == TP && img == IM && (!IM || img64 == (sizeof(IT) == 8)))              \
         return run(tma_step_kernel<4, false, TP, IM, T, IT>, TmaShape<4, IM, T, IT>::smem(TP));
+#define RTMB_TMA_DIFF_CASE(IM, IT)                                                               \
+    if (a.diff && img == IM && (!IM || img64 == (sizeof(IT) == 8)))                              \
+        return run(tma_step_kernel<4, false, kTaperNone, IM, T, IT, true>, TmaShape<4, IM, T, IT>::smem(kTaperNone));
+    RTMB_TMA_DIFF_CASE(false, float)
+    RTMB_TMA_DIFF_CASE(true, float)
+    RTMB_TMA_DIFF_CASE(true, double)
+#undef RTMB_TMA_DIFF_CASE
     RTMB_TMA_STORE_CASE(kTaperNone, false, float)
     RTMB_TMA_STORE_CASE(kTaperUpper, false, float)
     RTMB_TMA_STORE_CASE(kTaperAll, false, float)

@@ -28,6 +28,7 @@ FLAG_STORE_BF16 = 0x80
 FLAG_IMG_F64 = 0x100
 FLAG_NO_DUAL = 0x200
 FLAG_NO_TAPER_STORE = 0x400
+FLAG_STORE_DIFF = 0x800
 BC_ABC, BC_HBC, BC_RBC, BC_LEARNED = 1, 2, 3, 4
 CLOSURE_NPARAM, CLOSURE_NIN = 3169, 64
 

@@ -185,3 +185,44 @@ def test_storage_rejects_hbc_migration(cuda, oracle):
     with pytest.raises(rtmb.RtmbError) as e:
         ctx.migrate_shot(case["sx"], case["sy"], case["sz"], rec, img)
     assert e.value.code == rtmb.RTMB_EINVAL
+
+
+@pytest.mark.parametrize("img64", [False, True], ids=["img32", "img64"])
+@pytest.mark.parametrize("store", ["f16", "bf16"])
+def test_increment_storage_migration_image(cuda, oracle, store, img64):
+    """RTMB_FLAG_STORE_DIFF: the level and its increment each in 16 bits.  The image stays within
+    the two-level form's bound against the FP64 oracle and is closer to it than the two-level form
+    on the same case (the increment keeps the precision that p(t) - p(t-1) loses)."""
+    case = CASES["mid"]
+    p = oracle_params(case)
+    rec, _ = oracle.model_shot(p, velocity(oracle, case, "abc"))
+    v2 = velocity(oracle, case, "rbc")
+    ref = migrate_f64(case, v2, rec, "rbc", cuda)
+    extra = rtmb.FLAG_IMG_F64 if img64 else 0
+    got = migrate_form(case, v2, rec, cuda, STORE_FLAG[store] | rtmb.FLAG_STORE_DIFF | extra)
+    two = migrate_form(case, v2, rec, cuda, STORE_FLAG[store] | extra)
+    err, err2 = rel_l2(got, ref), rel_l2(two, ref)
+    print(f"image rel-L2 vs FP64: {store} increment {err:.3e}, two-level {err2:.3e}")
+    assert err <= TOL_IMG[store], err
+    assert err < err2, (err, err2)
+
+
+def test_increment_storage_scope(cuda, oracle):
+    """The increment form migrates with RBC; modeling and HBC migration are refused, and so is the
+    flag without a 16-bit type."""
+    import torch
+    case = CASES["golden"]
+    flags = rtmb.FLAG_STORE_F16 | rtmb.FLAG_STORE_DIFF
+    for bc, call in (("hbc", "model"), ("hbc", "migrate")):
+        ctx = ctx_for(case, bc, flags)
+        ctx.load_v2dt2(velocity(oracle, case, bc), from_host=True)
+        rec = torch.zeros(rec_shape(case), dtype=torch.float32, device=cuda)
+        with pytest.raises(rtmb.RtmbError) as e:
+            if call == "model":
+                ctx.model_shot(case["sx"], case["sy"], case["sz"], rec)
+            else:
+                img = torch.zeros(ctx.padded_shape, dtype=torch.float32, device=cuda)
+                ctx.migrate_shot(case["sx"], case["sy"], case["sz"], rec, img)
+        assert e.value.code == rtmb.RTMB_EINVAL
+    with pytest.raises(rtmb.RtmbError):
+        ctx_for(case, "rbc", rtmb.FLAG_STORE_DIFF)
