@@ -439,7 +439,14 @@ def run_b200(args, rank: int, world: int, local_rank: int) -> dict | None:
     params = rtmb.Params.from_input(p, flags=flags, device=local_rank)
     v, vpe, v2, v2m = build_inputs(p, with_abc=True)
     stream = torch.cuda.Stream(device=dev)
-    sx, sy, sz = p["sx"], p["sy"], p["sz"]
+    # shot-parallel ranks (rtmb.survey): one shot position per rank on a line through the surface
+    # centre, 8 cells apart, dealt as the reference deals its shot list (shotNumber = sh0 + rank)
+    from rtmb import survey
+    line = dict(p, source_count_x=world, source_count_y=1, source_distance_x=8, source_distance_y=1,
+                source_start_x=p["sx"] - 4 * (world - 1), source_start_y=p["sy"], source_depth_z=p["sz"])
+    shots = survey.shot_positions(line)
+    (k_mine,) = survey.rank_shots(len(shots), rank, world)
+    sx, sy, sz = shots[k_mine]
     rec_shape = (1, p["receiver_count_x"], p["receiver_count_y"], p["nt"])
 
     # the shot record: this library's modeling pass on the ABC-bordered model
@@ -476,9 +483,8 @@ def run_b200(args, rank: int, world: int, local_rank: int) -> dict | None:
             ctx.migrate_shot(sx, sy, sz, rec, img)
             ctx.image_stack(stack, img)           # the shot image stack (RTMAcousticController.cpp:223-225)
         if world > 1:
-            import torch.distributed as dist
             with torch.cuda.stream(stream):
-                dist.all_reduce(stack)            # images summed across shot-parallel ranks
+                survey.join_stacks(stack, exact=False)  # the ranks' stacks summed on rank 0 (NCCL)
         e1.record(stream)
         stream.synchronize()
     ms = e0.elapsed_time(e1)
