@@ -366,10 +366,31 @@ int rtmb_migrate_batch(rtmb_ctx *ctx, uint32_t nshots, const rtmb_shot *shots, d
                        uint32_t sny, uint32_t snz);
 
 /* ------------------------------------------------------------------ autotuner (no reference counterpart)
- * Times the context's step kernel (its storage and arithmetic form, on its geometry, with the
- * loaded v2dt2) for a set of x-chunk lengths (x planes per CTA: 8 .. 256) and keeps the fastest for
- * every later launch of the context.  The in-plane tile (64 z x 16 y, four z-points per thread) and
- * the ring depths are compiled in.  Optional outputs: the chosen chunk and its time per step (ms). */
+ * The reference launches a fixed 10^3-thread block grid (RTMGPUPlatform.cpp:167-196); here the
+ * launch shape of the step kernels is measured on the context's own geometry, form and v2dt2.
+ *
+ * rtmb_autotune_full times, with CUDA events on the context's stream (2 warm-up and 5 timed
+ * launches per candidate):
+ *   - the single-wavefield step (forward form plus imaging form) for every launch variant -- the
+ *     in-plane tile (0: 64 z x 16 y, 1: 32 x 32, 2: 64 x 8 at three CTAs per SM, 3: 64 x 16 with
+ *     shallower load rings) -- and every x-chunk length (x planes per CTA, 8 .. 256).  Variants 1-3
+ *     exist for the FP32 forms without taper at stencil order 8; other forms tune the chunk only;
+ *   - where the dual-wavefield backward step applies (FP32 FMA RBC migration, order 8): its x-chunk,
+ *     and the dual step against the source and receiver steps as two launches.
+ * The fastest choices are kept for every later launch of the context (rtmb_tuning; results do not
+ * change: every variant computes the same arithmetic per point).  rtmb_autotune is the same call
+ * reporting only the chunk and the step time. */
+typedef struct rtmb_tuning {
+    uint32_t variant;     /* launch variant of the single-wavefield step (see above) */
+    uint32_t chunk;       /* x planes per CTA of that step */
+    uint32_t dual;        /* 1: dual-wavefield backward step, 0: two launches per backward time step */
+    uint32_t dual_chunk;  /* x planes per CTA of the dual step */
+    float ms_step;        /* forward step (ms) with the chosen variant and chunk */
+    float ms_backward;    /* one backward time step (ms): the dual launch, or source + receiver steps */
+} rtmb_tuning;
+int rtmb_autotune_full(rtmb_ctx *ctx, rtmb_tuning *out);
+/* Applies a tuning (for example one measured earlier on the same geometry). */
+int rtmb_set_tuning(rtmb_ctx *ctx, const rtmb_tuning *t);
 int rtmb_autotune(rtmb_ctx *ctx, uint32_t *chunk_out, float *ms_out);
 /* Sets the x-chunk length directly (the default is chosen from the grid at rtmb_create). */
 int rtmb_set_chunk(rtmb_ctx *ctx, uint32_t chunk);

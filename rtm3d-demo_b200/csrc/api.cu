@@ -106,6 +106,7 @@ rtmb::StepArgs base_args(const rtmb_ctx *c) {
     std::memset(&a, 0, sizeof a);
     a.nxe = c->nxe; a.nye = c->nye; a.nze = c->nze; a.blen = (int)c->p.blen;
     a.chunk = c->chunk;
+    a.variant = c->variant;
     const int o = (int)c->p.stencil_order;
     a.iso = 1;
     for (int i = 0; i <= o; ++i) {
@@ -903,7 +904,7 @@ int migrate_impl(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const flo
     // FP32 FMA form: the source and receiver steps of one time step in one launch (RBC: with the
     // upper taper of HBC the two launches measured faster, 1.83 against 2.99 ms at 592^3)
     const bool dual = !st && !exact(ctx) && p.stencil_order == 8 && tma_ok(ctx) && !(p.flags & RTMB_FLAG_NO_DUAL) &&
-                      p.nx > 1 && !hbc;
+                      p.nx > 1 && !hbc && ctx->use_dual != 0;
     for (int it = (int)p.nt - 1; it >= 0; --it) {
         if (dual && it < (int)p.nt - 2) {
             src.P = s_cur; src.PP = s_prev; src.it = it;
@@ -1373,57 +1374,156 @@ int rtmb_migrate_batch(rtmb_ctx *ctx, uint32_t nshots, const rtmb_shot *shots, d
 
 // ------------------------------------------------------------------ autotuner
 
-int rtmb_autotune(rtmb_ctx *ctx, uint32_t *chunk_out, float *ms_out) {
+}  // extern "C"
+
+namespace {
+
+// Mean time (ms) of `reps` launches of fn after `warm` untimed ones, on the context's stream.
+template <typename F>
+int time_launches(rtmb_ctx *ctx, cudaEvent_t e0, cudaEvent_t e1, F fn, float *ms, int warm = 2, int reps = 5) {
+    for (int w = 0; w < warm; ++w) LAUNCH(fn());
+    CK(cudaEventRecord(e0, ctx->stream));
+    for (int r = 0; r < reps; ++r) LAUNCH(fn());
+    CK(cudaEventRecord(e1, ctx->stream));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaEventElapsedTime(ms, e0, e1));
+    *ms /= reps;
+    return RTMB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rtmb_autotune_full(rtmb_ctx *ctx, rtmb_tuning *out) {
     if (!ctx) return RTMB_EINVAL;
     if (!ctx->d_v2dt2) return fail(ctx, RTMB_EINVAL, "rtmb_autotune: load v2dt2 first");
     int rc = alloc_driver(ctx);
     if (rc) return rc;
+    const rtmb_params &p = ctx->p;
     const bool st = ctx->store != rtmb::kStoreF32;
-    rtmb::ScaleRec *rec3 = nullptr;
+    const int order = (int)p.stencil_order;
+    // scratch of the measurement: scale records (16-bit forms) and an image volume
+    rtmb::ScaleRec *rec5 = nullptr;
     if (st) {
-        CK(cudaMalloc(&rec3, 3 * sizeof(rtmb::ScaleRec)));
-        CK(cudaMemsetAsync(rec3, 0, 3 * sizeof(rtmb::ScaleRec), ctx->stream));
+        CK(cudaMalloc(&rec5, 5 * sizeof(rtmb::ScaleRec)));
+        CK(cudaMemsetAsync(rec5, 0, 5 * sizeof(rtmb::ScaleRec), ctx->stream));
     }
-    CK(cudaMemsetAsync(ctx->d_w[0], 0, wave_bytes(ctx), ctx->stream));
-    CK(cudaMemsetAsync(ctx->d_w[1], 0, wave_bytes(ctx), ctx->stream));
-    const int nxi = ctx->nxe - 2 * ctx->h;
-    // candidates: x planes per CTA.  Short chunks give more CTAs but re-read a 2h-plane halo per
-    // chunk; long chunks re-read less but may leave SMs idle in the last wave.
-    const int cand[] = {8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256};
+    void *img = nullptr;
+    const size_t img_bytes = ctx->n * (ctx->img64 ? sizeof(double) : sizeof(float));
+    CK(cudaMalloc(&img, img_bytes));
+    CK(cudaMemsetAsync(img, 0, img_bytes, ctx->stream));
+    for (int k = 0; k < 4; ++k) CK(cudaMemsetAsync(ctx->d_w[k], 0, wave_bytes(ctx), ctx->stream));
+    for (int k = 0; ctx->diff && k < 2; ++k) CK(cudaMemsetAsync(ctx->d_inc[k], 0, wave_bytes(ctx), ctx->stream));
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    const int saved = ctx->chunk;
-    float best = 1e30f;
-    int best_chunk = saved;
-    for (int c : cand) {
-        if (c > nxi) break;
-        ctx->chunk = c;
+    auto release = [&]() {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (rec5) cudaFree(rec5);
+        cudaFree(img);
+    };
+    // the step forms of the context: forward (no image) and receiver (image of the source level)
+    auto args = [&](bool with_img) {
         rtmb::StepArgs a = base_args(ctx);
         a.V = ctx->d_v2dt2;
         a.P = ctx->d_w[0];
         a.PP = ctx->d_w[1];
         a.store = ctx->store;
-        if (st) { a.sc_p = rec3; a.sc_pp = rec3 + 1; a.sc_out = rec3 + 2; a.inj = 1.f; }
-        for (int w = 0; w < 2; ++w) LAUNCH(rtmb::launch_step(a, (int)ctx->p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
-        CK(cudaEventRecord(e0, ctx->stream));
-        const int reps = 5;
-        for (int r = 0; r < reps; ++r)
-            LAUNCH(rtmb::launch_step(a, (int)ctx->p.stencil_order, exact(ctx), ctx->stream, tma_ok(ctx)));
-        CK(cudaEventRecord(e1, ctx->stream));
-        CK(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, e0, e1));
-        ms /= reps;
-        if (ms < best) { best = ms; best_chunk = c; }
+        if (st) { a.sc_p = rec5; a.sc_pp = rec5 + 1; a.sc_out = rec5 + 2; a.sc_out2 = rec5 + 3; a.inj = 1.f; }
+        if (ctx->diff) { a.diff = 1; a.Pout = ctx->d_w[2]; a.PP = static_cast<float *>(ctx->d_inc[0]); }
+        if (with_img) {
+            a.img = static_cast<float *>(img);
+            a.img64 = ctx->img64;
+            a.ps = ctx->d_w[3];
+            a.sc_ps = rec5 ? rec5 + 4 : nullptr;
+            a.img_z0 = 0;
+            a.img_z1 = ctx->nze;
+        }
+        return a;
+    };
+    const int nxi = ctx->nxe - 2 * ctx->h;
+    const int cand[] = {8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256};
+    // launch variants exist for the FP32 forms without taper at order 8 on the TMA kernel
+    const bool variants = !st && order == 8 && tma_ok(ctx) && ctx->nze % 4 == 0;
+    const int nv = variants ? rtmb::kStepVariants : 1;
+    float best = 1e30f, best_fwd = 0.f;
+    int best_v = 0, best_c = ctx->chunk;
+    for (int v = 0; v < nv && !rc; ++v) {
+        for (int c : cand) {
+            if (c > nxi) break;
+            ctx->variant = v;
+            ctx->chunk = c;
+            rtmb::StepArgs af = args(false), ai = args(true);
+            float tf = 0.f, ti = 0.f;
+            if ((rc = time_launches(ctx, e0, e1, [&] { return rtmb::launch_step(af, order, exact(ctx), ctx->stream, tma_ok(ctx)); }, &tf)))
+                break;
+            if ((rc = time_launches(ctx, e0, e1, [&] { return rtmb::launch_step(ai, order, exact(ctx), ctx->stream, tma_ok(ctx)); }, &ti)))
+                break;
+            if (tf + ti < best) { best = tf + ti; best_fwd = tf; best_v = v; best_c = c; }
+        }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (rec3) cudaFree(rec3);
-    ctx->chunk = best_chunk;
-    if (chunk_out) *chunk_out = (uint32_t)best_chunk;
-    if (ms_out) *ms_out = best;
+    if (rc) { release(); return rc; }
+    ctx->variant = best_v;
+    ctx->chunk = best_c;
+    // backward time step: the dual launch against the source and receiver steps as two launches
+    float two = 0.f;
+    {
+        rtmb::StepArgs as = args(false), ai = args(true);
+        rc = time_launches(ctx, e0, e1, [&] {
+            cudaError_t e = rtmb::launch_step(as, order, exact(ctx), ctx->stream, tma_ok(ctx));
+            return e != cudaSuccess ? e : rtmb::launch_step(ai, order, exact(ctx), ctx->stream, tma_ok(ctx));
+        }, &two);
+    }
+    const bool dual_ok = !rc && !st && !exact(ctx) && order == 8 && tma_ok(ctx) && !(p.flags & RTMB_FLAG_NO_DUAL) &&
+                         p.nx > 1 && p.boundary == RTMB_BC_RBC;
+    float best_dual = 1e30f;
+    int best_dc = ctx->dual_chunk;
+    for (int c : cand) {
+        if (!dual_ok || rc || c > nxi) break;
+        rtmb::StepArgs src = args(false), rcv = args(true);
+        src.P = ctx->d_w[0]; src.PP = ctx->d_w[1];
+        rcv.P = ctx->d_w[2]; rcv.PP = ctx->d_w[3]; rcv.ps = nullptr;
+        rcv.chunk = c;
+        if (!rtmb::dual_step_supported(src, rcv, order)) break;
+        float t = 0.f;
+        if ((rc = time_launches(ctx, e0, e1, [&] { return rtmb::launch_dual_step(src, rcv, order, false, ctx->stream); }, &t)))
+            break;
+        if (t < best_dual) { best_dual = t; best_dc = c; }
+    }
+    release();
+    if (rc) return rc;
+    ctx->dual_chunk = best_dc;
+    ctx->use_dual = dual_ok ? (best_dual < two ? 1 : 0) : -1;
+    if (out) {
+        out->variant = (uint32_t)ctx->variant;
+        out->chunk = (uint32_t)ctx->chunk;
+        out->dual = ctx->use_dual == 1;
+        out->dual_chunk = (uint32_t)ctx->dual_chunk;
+        out->ms_step = best_fwd;
+        out->ms_backward = ctx->use_dual == 1 ? best_dual : two;
+    }
     return check_err_flag(ctx);
+}
+
+int rtmb_set_tuning(rtmb_ctx *ctx, const rtmb_tuning *t) {
+    if (!ctx || !t || !t->chunk || !t->dual_chunk || t->variant >= (uint32_t)rtmb::kStepVariants)
+        return fail(ctx, RTMB_EINVAL, "rtmb_set_tuning: bad tuning");
+    ctx->variant = (int)t->variant;
+    ctx->chunk = (int)t->chunk;
+    ctx->dual_chunk = (int)t->dual_chunk;
+    ctx->use_dual = t->dual ? 1 : 0;
+    return RTMB_OK;
+}
+
+int rtmb_autotune(rtmb_ctx *ctx, uint32_t *chunk_out, float *ms_out) {
+    rtmb_tuning t{};
+    const int rc = rtmb_autotune_full(ctx, &t);
+    if (rc) return rc;
+    if (chunk_out) *chunk_out = t.chunk;
+    if (ms_out) *ms_out = t.ms_step;
+    return RTMB_OK;
 }
 
 int rtmb_set_chunk(rtmb_ctx *ctx, uint32_t chunk) {

@@ -27,6 +27,8 @@ struct rtmb_ctx {
     float *d_rec = nullptr, *d_img = nullptr;  // staging for the host-buffer forms
     int chunk = 0;
     int dual_chunk = 0;  // x planes per CTA of the dual-wavefield backward step (64 x 8 tiles)
+    int variant = 0;     // launch variant of the TMA step kernel (rtmb_autotune_full)
+    int use_dual = -1;   // -1: the default rule; 0 / 1: the autotuner's choice
     uint64_t launches = 0;
     // storage forms (RTMB_FLAG_STORE_*): element type of d_w, one scale record per stored level
     int store = rtmb::kStoreF32;

@@ -72,9 +72,9 @@ cudaError_t store_dispatch(const StepArgs &a, dim3 grid, cudaStream_t s) {
     return detail::launch_tma_store<__nv_bfloat16>(maps, a, a.taper_mode, a.img != nullptr, a.img64 != 0, grid, s);
 }
 
-template <int H>
-cudaError_t tma_dispatch(const StepArgs &a, bool exact, dim3 grid, cudaStream_t s, bool *used) {
-    using S = detail::TmaShape<H, false>;
+template <int H, int V>
+cudaError_t tma_dispatch_v(const StepArgs &a, bool exact, cudaStream_t s, bool *used) {
+    using S = detail::TmaShape<H, false, float, float, V>;
     *used = false;
     auto enc = tensor_map_encoder();
     if (!enc) return cudaSuccess;
@@ -82,14 +82,30 @@ cudaError_t tma_dispatch(const StepArgs &a, bool exact, dim3 grid, cudaStream_t 
     // the FP32 forward forms of the TMA kernel sample no receivers (their drivers gather them from
     // the stored level): the plain-load form does it in the step
     if (!a.img && a.rec_mode != kRecNone) return cudaSuccess;
+    const int nxi = a.nxe - 2 * H, nyi = a.nye - 2 * H;
+    const dim3 grid((a.nze + S::TZ - 1) / S::TZ, (nyi + S::TY - 1) / S::TY, (nxi + a.chunk - 1) / a.chunk);
     detail::TmaMaps maps;
     std::memset(&maps, 0, sizeof maps);
-    bool ok = encode(enc, &maps.p, a.P, a, S::SPITCH, S::SROWS) && encode(enc, &maps.pp, a.PP, a, kTZ, kTY) &&
-              encode(enc, &maps.v, a.V, a, kTZ, kTY);
-    if (a.img) ok = ok && encode(enc, &maps.ps, a.ps, a, kTZ, kTY) && encode(enc, &maps.img, a.img, a, kTZ, kTY);
+    bool ok = encode(enc, &maps.p, a.P, a, S::SPITCH, S::SROWS) && encode(enc, &maps.pp, a.PP, a, S::TZ, S::TY) &&
+              encode(enc, &maps.v, a.V, a, S::TZ, S::TY);
+    if (a.img) ok = ok && encode(enc, &maps.ps, a.ps, a, S::TZ, S::TY) && encode(enc, &maps.img, a.img, a, S::TZ, S::TY);
     if (!ok) return cudaSuccess;  // fall back to the plain-load form
     *used = true;
     return detail::launch_tma_h<H>(maps, a, exact, a.taper_mode, a.img != nullptr, grid, s);
+}
+
+// The launch variants (tile shape, ring depths) serve the FP32 forms without taper at order 8; the
+// others run variant 0.
+template <int H>
+cudaError_t tma_dispatch(const StepArgs &a, bool exact, cudaStream_t s, bool *used) {
+    const int v = (H == 4 && a.taper_mode == kTaperNone && !a.tw) ? a.variant : 0;
+    switch (v) {
+    case 0: return tma_dispatch_v<H, 0>(a, exact, s, used);
+    case 1: return tma_dispatch_v<H, 1>(a, exact, s, used);
+    case 2: return tma_dispatch_v<H, 2>(a, exact, s, used);
+    case 3: return tma_dispatch_v<H, 3>(a, exact, s, used);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 }  // namespace
@@ -113,10 +129,10 @@ cudaError_t launch_step(const StepArgs &a, int order, bool exact, cudaStream_t s
         bool used = false;
         cudaError_t e = cudaSuccess;
         switch (h) {
-        case 1: e = tma_dispatch<1>(a, exact, grid, s, &used); break;
-        case 2: e = tma_dispatch<2>(a, exact, grid, s, &used); break;
-        case 3: e = tma_dispatch<3>(a, exact, grid, s, &used); break;
-        case 4: e = tma_dispatch<4>(a, exact, grid, s, &used); break;
+        case 1: e = tma_dispatch<1>(a, exact, s, &used); break;
+        case 2: e = tma_dispatch<2>(a, exact, s, &used); break;
+        case 3: e = tma_dispatch<3>(a, exact, s, &used); break;
+        case 4: e = tma_dispatch<4>(a, exact, s, &used); break;
         default: break;  // orders above 8 use the plain-load form
         }
         if (used || e != cudaSuccess) return e;
@@ -136,6 +152,15 @@ cudaError_t launch_step(const StepArgs &a, int order, bool exact, cudaStream_t s
 }
 
 bool storage_form_supported(int order, int nze) { return order == 8 && nze % 8 == 0; }
+
+void variant_tile(int variant, int *tz, int *ty) {
+    switch (variant) {
+    case 1: *tz = detail::Variant<1>::TZ; *ty = detail::Variant<1>::TY; break;
+    case 2: *tz = detail::Variant<2>::TZ; *ty = detail::Variant<2>::TY; break;
+    case 3: *tz = detail::Variant<3>::TZ; *ty = detail::Variant<3>::TY; break;
+    default: *tz = detail::Variant<0>::TZ; *ty = detail::Variant<0>::TY; break;
+    }
+}
 
 cudaError_t launch_step_batch(const StepArgs *args, int nshots, int order, bool exact, cudaStream_t s) {
     static_assert(sizeof(detail::BatchArgs) <= 32000, "kernel parameters above the 32 KB limit");

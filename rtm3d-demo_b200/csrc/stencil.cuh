@@ -107,7 +107,14 @@ struct StepArgs {
     int diff;
     void *Pout;
     ScaleRec *sc_out2;
+    // launch variant of the TMA step kernel (tile shape and ring depths, 0 = default): taken by the
+    // FP32 forms without taper at order 8, ignored elsewhere
+    int variant;
 };
+
+// In-plane tile (z, y) of a launch variant of the TMA step kernel (stencil_tma_impl.cuh: Variant).
+void variant_tile(int variant, int *tz, int *ty);
+constexpr int kStepVariants = 4;
 
 // Exponent of a produced level: the smallest e with bound * 2^-e < 2^15.  bound is
 // 8 * max(amax(P), amax(PP)) + injection: a stable step (v^2 dt^2 * sum|coef| <= 4 over the three

@@ -80,18 +80,46 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
 
 __device__ __forceinline__ float4 ld_f4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 
-// Barrier 1 over the kThreads consumer threads only (the producer warp never joins it).
-__device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kThreads) : "memory"); }
+// Barrier 1 over the NT consumer threads only (the producer warp never joins it).
+template <int NT>
+__device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory"); }
+template <int NT>
 __device__ __forceinline__ bool consumer_sync_or(bool v) {
     uint32_t out;
     asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, 1, %2, p;\n selp.u32 %0, 1, 0, q;\n}\n"
                  : "=r"(out)
-                 : "r"((uint32_t)v), "n"(kThreads)
+                 : "r"((uint32_t)v), "n"(NT)
                  : "memory");
     return out != 0;
 }
 
 constexpr int kTmaThreads = kThreads + 32;  // eight consumer warps and one producer warp
+
+// Launch variants of the step kernel (StepArgs::variant, picked per context by rtmb_autotune):
+// the in-plane tile (TZ along z, TY along y; four z points per consumer thread) and the depth of
+// the P ring (slots beyond the centre plane: DX, DX_IMG for the imaging form) and of the core ring
+// (R, R_IMG); MINB CTAs per SM.  Variant 0 is the default and the only one of the taper forms.
+template <int V>
+struct Variant;
+template <>
+struct Variant<0> {  // 64 x 16, deep rings
+    static constexpr int TZ = 64, TY = 16, DX = 6, DX_IMG = 5, R = 4, R_IMG = 3, MINB = 2;
+};
+template <>
+struct Variant<1> {  // 32 x 32: fewer halo rows per point (40 x 40 tile for 32 x 32 points)
+    static constexpr int TZ = 32, TY = 32, DX = 6, DX_IMG = 5, R = 4, R_IMG = 3, MINB = 2;
+};
+template <>
+struct Variant<2> {  // 64 x 8 with three CTAs per SM
+    static constexpr int TZ = 64, TY = 8, DX = 6, DX_IMG = 5, R = 4, R_IMG = 3, MINB = 3;
+};
+template <>
+struct Variant<3> {  // 64 x 16, shallow rings (less shared memory per CTA, shorter lookahead)
+    static constexpr int TZ = 64, TY = 16, DX = 4, DX_IMG = 4, R = 3, R_IMG = 2, MINB = 2;
+};
+constexpr int kVariants = 4;
+template <int V>
+constexpr int variant_threads() { return (Variant<V>::TZ / kVZ) * Variant<V>::TY + 32; }
 
 // Tensor maps of one launch.  p: box {TZ + 2ZH, TY + 2H, 1}; the others: box {TZ, TY, 1}.
 struct TmaMaps {
@@ -180,24 +208,26 @@ __device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
     return r;
 }
 
-// Shared-memory plan of one variant.  T: storage type of P/PP/ps; IT: image type.
-template <int H, bool IMG, typename T = float, typename IT = float>
+// Shared-memory plan of one variant.  T: storage type of P/PP/ps; IT: image type; V: launch variant.
+template <int H, bool IMG, typename T = float, typename IT = float, int V = 0>
 struct TmaShape {
+    static constexpr int TZ = Variant<V>::TZ, TY = Variant<V>::TY;
+    static constexpr int NT = (TZ / kVZ) * TY;  // consumer threads
     static constexpr int EALIGN = 16 / (int)sizeof(T) > 4 ? 16 / (int)sizeof(T) : 4;
     static constexpr int ZH = ((H + EALIGN - 1) / EALIGN) * EALIGN;  // z halo: whole 16-byte units
-    static constexpr int SROWS = kTY + 2 * H;
-    static constexpr int SPITCH = kTZ + 2 * ZH;
+    static constexpr int SROWS = TY + 2 * H;
+    static constexpr int SPITCH = TZ + 2 * ZH;
     static constexpr int STAGE = SROWS * SPITCH;  // elements written by one P tile load
     static constexpr int SALIGN = 128 / (int)sizeof(T);
     static constexpr int STRIDE = ((STAGE + SALIGN - 1) / SALIGN) * SALIGN;  // P slot pitch: 128 B
-    static constexpr int CORE = kTZ * kTY;  // elements of one core tile
+    static constexpr int CORE = TZ * TY;  // elements of one core tile
     // core slot, in bytes: PP (T), V (float) [, PS (T), IMG (IT)]
     static constexpr int OFF_V = CORE * (int)sizeof(T);
     static constexpr int OFF_PS = OFF_V + CORE * 4;
     static constexpr int OFF_IMG = OFF_PS + CORE * (int)sizeof(T);
     static constexpr int CSLOT = IMG ? OFF_IMG + CORE * (int)sizeof(IT) : OFF_PS;
-    static constexpr int D = IMG ? H + 5 : H + 6;  // P slots
-    static constexpr int R = IMG ? 3 : 4;          // core slots
+    static constexpr int D = H + (IMG ? Variant<V>::DX_IMG : Variant<V>::DX);  // P slots
+    static constexpr int R = IMG ? Variant<V>::R_IMG : Variant<V>::R;           // core slots
     static_assert(2 * H <= D && D >= H + 2, "warm-up planes and the lookahead must fit in the P ring");
     static constexpr size_t PRING_BYTES = (size_t)D * STRIDE * sizeof(T);
     static constexpr size_t SMEM = PRING_BYTES + (size_t)R * CSLOT + 2 * (D + R) * sizeof(uint64_t);
@@ -226,7 +256,7 @@ __device__ __forceinline__ void taper_tile(T *st, const float *tab, const StepAr
     bool xb;
     const float fx = taper_factor(a.taper, a.blen, a.nxe, x, xb);
     constexpr int U = SPITCH / 4;  // four cells per unit
-    for (int w = tid; w < S::SROWS * U; w += kThreads) {
+    for (int w = tid; w < S::SROWS * U; w += S::NT) {
         const int r = w / U, u = w - r * U;
         const int yy = yt0 - H + r;
         if (yy >= a.nye) continue;
@@ -270,10 +300,12 @@ __device__ __forceinline__ void taper_tile(T *st, const float *tab, const StepAr
 // The body of one CTA: the tile (bx, by) of the (z, y) plane and x chunk bz of the volume that
 // (maps, a) describe; the stencil coefficients come from coef (for the compiler, a kernel
 // parameter at a fixed offset, so the FMAs take them straight from the constant bank).
-template <int H, bool EXACT, int TAPER, bool IMG, typename T, typename IT, bool DF = false>
+template <int H, bool EXACT, int TAPER, bool IMG, typename T, typename IT, bool DF = false, int V = 0>
 __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArgs &a, const StepArgs &coef, int bx,
                                               int by, int bz) {
-    using S = TmaShape<H, IMG, T, IT>;
+    using S = TmaShape<H, IMG, T, IT, V>;
+    static_assert(V == 0 || TAPER == kTaperNone, "the taper forms run the default variant");
+    constexpr int kTZ = S::TZ, kTY = S::TY, kThreads = S::NT;  // this variant's tile and consumer threads
     using ST = Stor<T>;
     constexpr bool SC = ST::kScaled;
     static_assert(!DF || (SC && TAPER == kTaperNone), "increment storage: 16-bit forms without taper");
@@ -484,7 +516,7 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
         wait_p(k, 0);
         if (CB && plane_needs_taper(k)) taper_stage(k, k);
     }
-    if (CB ? consumer_sync_or(bad_wait) : bad_wait) goto drain;
+    if (CB ? consumer_sync_or<kThreads>(bad_wait) : bad_wait) goto drain;
 #pragma unroll
     for (int k = 0; k < 2 * H; ++k) q[k + 1] = ST::ld4(pring + k * STRIDE + (ty + H) * SPITCH + col);
 #pragma unroll
@@ -516,7 +548,7 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
             if constexpr (CB) {
                 if (plane_needs_taper(kin)) {  // the pass is collective: all warps take this branch
                     taper_stage(kin, s_in);
-                    if (consumer_sync_or(bad_wait)) goto drain;
+                    if (consumer_sync_or<kThreads>(bad_wait)) goto drain;
                 }
             } else if (bad_wait) {
                 goto drain;  // a timed-out wait leaves the data undefined; stop without computing
@@ -863,10 +895,10 @@ drain:
     if (a.err) atomicOr(a.err, 2u);
 }
 
-template <int H, bool EXACT, int TAPER, bool IMG, typename T = float, typename IT = float, bool DF = false>
-__global__ void __launch_bounds__(kTmaThreads, 2)
+template <int H, bool EXACT, int TAPER, bool IMG, typename T = float, typename IT = float, bool DF = false, int V = 0>
+__global__ void __launch_bounds__(variant_threads<V>(), Variant<V>::MINB)
     tma_step_kernel(const __grid_constant__ TmaMaps maps, const __grid_constant__ StepArgs a) {
-    tma_step_body<H, EXACT, TAPER, IMG, T, IT, DF>(maps, a, a, blockIdx.x, blockIdx.y, blockIdx.z);
+    tma_step_body<H, EXACT, TAPER, IMG, T, IT, DF, V>(maps, a, a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // Several volumes in one launch (the batched multi-shot drivers): shot s owns the linear blocks
@@ -908,24 +940,27 @@ template <int H>
 cudaError_t launch_tma_h(const TmaMaps &maps, const StepArgs &a, bool exact, int taper, bool img, dim3 grid,
                          cudaStream_t s) {
     // the dynamic shared-memory opt-in, once per (variant, device)
-    static unsigned long long attr_done[20] = {};
+    static unsigned long long attr_done[20 * kVariants] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (a.tw & kTwStored) taper = taper == kTaperAll ? kTaperAllStored : (taper == kTaperUpper ? kTaperUpperStored : -1);
     if (taper < 0) return cudaErrorInvalidValue;
-    const int variant = (exact ? 10 : 0) + (img ? 5 : 0) + taper;
-    auto run = [&](void (*kern)(TmaMaps, StepArgs), size_t smem) -> cudaError_t {
+    const int lv = (taper == kTaperNone && H == 4) ? a.variant : 0;  // launch variant: RBC forms of order 8
+    if (lv < 0 || lv >= kVariants) return cudaErrorInvalidValue;
+    const int variant = 20 * lv + (exact ? 10 : 0) + (img ? 5 : 0) + taper;
+    auto run = [&](void (*kern)(TmaMaps, StepArgs), size_t smem, int threads) -> cudaError_t {
         const unsigned long long bit = 1ull << (dev & 63);
         if (!(attr_done[variant] & bit)) {
             cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
             attr_done[variant] |= bit;
         }
-        kern<<<grid, kTmaThreads, smem, s>>>(maps, a);
+        kern<<<grid, threads, smem, s>>>(maps, a);
         return cudaGetLastError();
     };
 #define RTMB_TMA_CASE(EX, TP, IM) \
-    if (exact == EX && taper == TP && img == IM) return run(tma_step_kernel<H, EX, TP, IM>, TmaShape<H, IM>::smem(TP));
+    if (lv == 0 && exact == EX && taper == TP && img == IM) \
+        return run(tma_step_kernel<H, EX, TP, IM>, TmaShape<H, IM>::smem(TP), kTmaThreads);
     RTMB_TMA_CASE(true, kTaperNone, false)
     RTMB_TMA_CASE(true, kTaperUpper, false)
     RTMB_TMA_CASE(true, kTaperAll, false)
@@ -943,6 +978,16 @@ cudaError_t launch_tma_h(const TmaMaps &maps, const StepArgs &a, bool exact, int
     RTMB_TMA_CASE(false, kTaperUpper, true)
     RTMB_TMA_CASE(false, kTaperUpperStored, true)
 #undef RTMB_TMA_CASE
+    if constexpr (H == 4) {
+#define RTMB_TMA_VCASE(VV, EX, IM)                                                                         \
+    if (lv == VV && exact == EX && img == IM)                                                              \
+        return run(tma_step_kernel<H, EX, kTaperNone, IM, float, float, false, VV>,                          \
+                   TmaShape<H, IM, float, float, VV>::smem(kTaperNone), variant_threads<VV>());
+        RTMB_TMA_VCASE(1, true, false) RTMB_TMA_VCASE(1, true, true) RTMB_TMA_VCASE(1, false, false) RTMB_TMA_VCASE(1, false, true)
+        RTMB_TMA_VCASE(2, true, false) RTMB_TMA_VCASE(2, true, true) RTMB_TMA_VCASE(2, false, false) RTMB_TMA_VCASE(2, false, true)
+        RTMB_TMA_VCASE(3, true, false) RTMB_TMA_VCASE(3, true, true) RTMB_TMA_VCASE(3, false, false) RTMB_TMA_VCASE(3, false, true)
+#undef RTMB_TMA_VCASE
+    }
     return cudaErrorInvalidValue;
 }
 

@@ -119,6 +119,8 @@ SYMBOLS = [
                               C.c_uint64, C.POINTER(C.c_uint64)], C.c_int),
     ("rtmb_closure_set", [_vp, _vp, C.c_float, C.c_float], C.c_int),
     ("rtmb_autotune", [_vp, C.POINTER(_u32), C.POINTER(C.c_float)], C.c_int),
+    ("rtmb_autotune_full", [_vp, _vp], C.c_int),
+    ("rtmb_set_tuning", [_vp, _vp], C.c_int),
     ("rtmb_migrate_batch", [_vp, _u32, _vp, _vp, _u32, _u32, _u32], C.c_int),
     ("rtmb_set_chunk", [_vp, _u32], C.c_int),
 ]
@@ -158,6 +160,15 @@ def _ptr(t) -> int:
     if hasattr(t, "data_ptr"):
         return t.data_ptr()
     return t.ctypes.data
+
+
+class Tuning(C.Structure):
+    """rtmb_tuning: the launch choices rtmb_autotune_full measured for a context."""
+    _fields_ = [("variant", _u32), ("chunk", _u32), ("dual", _u32), ("dual_chunk", _u32),
+                ("ms_step", C.c_float), ("ms_backward", C.c_float)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Shot(C.Structure):
@@ -323,6 +334,17 @@ class Context:
         c, ms = _u32(0), C.c_float(0)
         self._check(self.L.rtmb_autotune(self.h, C.byref(c), C.byref(ms)))
         return int(c.value), float(ms.value)
+
+    def autotune_full(self) -> dict:
+        """Picks the launch variant (tile shape, ring depths), the x-chunk lengths and the dual
+        backward step or two launches for this context; returns the rtmb_tuning fields."""
+        t = Tuning()
+        self._check(self.L.rtmb_autotune_full(self.h, C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, t: dict) -> None:
+        tt = Tuning(**{k: t[k] for k, _ in Tuning._fields_})
+        self._check(self.L.rtmb_set_tuning(self.h, C.byref(tt)))
 
     def set_chunk(self, chunk: int):
         self._check(self.L.rtmb_set_chunk(self.h, chunk))
