@@ -344,9 +344,12 @@ int rtmb_closure_set(rtmb_ctx *ctx, const float *params, float min_scale, float 
 
 /* ------------------------------------------------------------------ batched multi-shot migration
  * No reference counterpart (the reference migrates one shot per process, RTMAcousticController.cpp:
- * 193-242).  Up to 12 shots, each on its own aperture sub-volume of the survey (sizes may differ),
- * advance together: every time step of the batch is one launch of the step kernel over all shots'
- * volumes; with RTMB_FLAG_USE_GRAPH the whole batch's time loop is one CUDA graph.  Each shot's image
+ * 193-242).  Any number of shots, each on its own aperture sub-volume of the survey (sizes may
+ * differ), run in groups of batch_group shots (default 12, at most 24; rtmb_set_batch_group,
+ * rtmb_autotune_batch): the shots of a group advance together, every time step of the group is one
+ * launch of the step kernel over all its shots' volumes, and with RTMB_FLAG_USE_GRAPH the group's
+ * whole time loop is one CUDA graph.  A group's wavefields and shot images are allocated for the
+ * group and freed after it.  Each shot's image
  * is added, without its border, to the survey's FP64 stack at the aperture's origin.  The context
  * supplies what the shots share: blen, nt, ntstep, stencil_order (8), dx/dy/dz, dt, fpeak,
  * boundary (RBC) and the form flags (FP32 exact or FMA, or a 16-bit storage flag with or without
@@ -364,6 +367,14 @@ typedef struct rtmb_shot {
 /* stack: survey image (snx * sny * snz doubles, device), added to. */
 int rtmb_migrate_batch(rtmb_ctx *ctx, uint32_t nshots, const rtmb_shot *shots, double *stack, uint32_t snx,
                        uint32_t sny, uint32_t snz);
+/* Shots per launch of rtmb_migrate_batch (1 .. 24). */
+int rtmb_set_batch_group(rtmb_ctx *ctx, uint32_t shots_per_launch);
+/* Times the batched forward step (2 warm-up and 5 timed launches, CUDA events) for 1, 2, 3, 4, 6, 8,
+ * 12, 16 and 24 shots per launch on the first shots of the batch and keeps the group size with the
+ * highest point-update rate for the context's later batches.  Optional outputs: the group size and
+ * its rate (G point-updates/s). */
+int rtmb_autotune_batch(rtmb_ctx *ctx, uint32_t nshots, const rtmb_shot *shots, uint32_t *group_out,
+                        float *rate_out);
 
 /* ------------------------------------------------------------------ autotuner (no reference counterpart)
  * The reference launches a fixed 10^3-thread block grid (RTMGPUPlatform.cpp:167-196); here the

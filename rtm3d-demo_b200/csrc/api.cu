@@ -1203,14 +1203,18 @@ void shot_receivers(rtmb::StepArgs &a, const rtmb_ctx *ctx, const BatchShot &b, 
 
 extern "C" {
 
-int rtmb_migrate_batch(rtmb_ctx *ctx, uint32_t nshots, const rtmb_shot *shots, double *stack, uint32_t snx,
-                       uint32_t sny, uint32_t snz) {
-    if (!ctx || !shots || !stack) return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: null pointer");
+}  // extern "C"
+
+namespace {
+
+// One group of at most kMaxBatch shots of rtmb_migrate_batch: their per-shot state is allocated
+// here, their time loops advance together (one launch per step for the group, one CUDA graph with
+// RTMB_FLAG_USE_GRAPH), and their images are added to the survey stack.  With forward_only, only
+// `steps` forward steps run (the autotuner's measurement; nothing is stacked) and *ms receives
+// their mean device time.
+int migrate_group(rtmb_ctx *ctx, uint32_t nshots, const rtmb_shot *shots, double *stack, uint32_t snx,
+                  uint32_t sny, uint32_t snz, int forward_only = 0, float *ms = nullptr) {
     const rtmb_params &p = ctx->p;
-    if (nshots == 0 || nshots > 12) return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: 1 to 12 shots per batch");
-    if (ctx->diff) return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: the increment storage form runs single shots");
-    if (p.boundary != RTMB_BC_RBC || p.stencil_order != 8 || (int)p.blen < ctx->h || p.nx == 1)
-        return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: boundary RBC, stencil_order 8, blen >= 4, 3D (nx > 1)");
     const bool st = ctx->store != rtmb::kStoreF32;
     const size_t es = st ? 2 : 4;
     const bool img64 = st;  // the 16-bit forms stack through an FP64 shot image, FP32 through FP32
@@ -1282,6 +1286,29 @@ int rtmb_migrate_batch(rtmb_ctx *ctx, uint32_t nshots, const rtmb_shot *shots, d
             scP[k] = sh[k].next_scale(); scPP[k] = sh[k].next_scale();
             srP[k] = sh[k].next_scale(); srPP[k] = sh[k].next_scale();
         }
+    }
+    if (forward_only) {  // the autotuner's measurement: forward steps of this group
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        bool ok = cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess;
+        for (int it = 0; ok && it < forward_only + 2; ++it) {
+            if (it == 2) ok = cudaEventRecord(e0, ctx->stream) == cudaSuccess;
+            for (uint32_t k = 0; k < nshots; ++k) {
+                rtmb::StepArgs &a = args[k];
+                a = shot_args(ctx, sh[k]);
+                a.P = sP[k]; a.PP = sPP[k]; a.it = 0;
+                if (st) { a.sc_p = scP[k]; a.sc_pp = scPP[k]; a.sc_out = srP[k]; a.inj = ctx->wmax; }
+            }
+            ++ctx->launches;
+            ok = ok && rtmb::launch_step_batch(args.data(), (int)nshots, order, exact(ctx), ctx->stream) == cudaSuccess;
+        }
+        ok = ok && cudaEventRecord(e1, ctx->stream) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
+             cudaEventElapsedTime(ms, e0, e1) == cudaSuccess;
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (ms) *ms /= forward_only;
+        cudaStreamSynchronize(ctx->stream);
+        release();
+        return ok ? RTMB_OK : fail(ctx, RTMB_ECUDA, "rtmb_autotune_batch: measurement failed");
     }
     {
         GraphScope graph(ctx, 2);
@@ -1371,6 +1398,63 @@ int rtmb_migrate_batch(rtmb_ctx *ctx, uint32_t nshots, const rtmb_shot *shots, d
     release();
     return rc;
 }
+
+}  // namespace
+
+extern "C" {
+
+int rtmb_migrate_batch(rtmb_ctx *ctx, uint32_t nshots, const rtmb_shot *shots, double *stack, uint32_t snx,
+                       uint32_t sny, uint32_t snz) {
+    if (!ctx || !shots || !stack) return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: null pointer");
+    const rtmb_params &p = ctx->p;
+    if (nshots == 0) return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: no shots");
+    if (ctx->diff) return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: the increment storage form runs single shots");
+    if (p.boundary != RTMB_BC_RBC || p.stencil_order != 8 || (int)p.blen < ctx->h || p.nx == 1)
+        return fail(ctx, RTMB_EINVAL, "rtmb_migrate_batch: boundary RBC, stencil_order 8, blen >= 4, 3D (nx > 1)");
+    // groups of batch_group shots, in order: each group's time loop runs with its shots together
+    const uint32_t g = (uint32_t)ctx->batch_group;
+    for (uint32_t k0 = 0; k0 < nshots; k0 += g) {
+        const int rc = migrate_group(ctx, nshots - k0 < g ? nshots - k0 : g, shots + k0, stack, snx, sny, snz);
+        if (rc) return rc;
+    }
+    return RTMB_OK;
+}
+
+int rtmb_set_batch_group(rtmb_ctx *ctx, uint32_t shots_per_launch) {
+    if (!ctx || shots_per_launch == 0 || shots_per_launch > (uint32_t)rtmb::kMaxBatchShots)
+        return fail(ctx, RTMB_EINVAL, "rtmb_set_batch_group: 1 to %d shots per launch", rtmb::kMaxBatchShots);
+    ctx->batch_group = (int)shots_per_launch;
+    return RTMB_OK;
+}
+
+int rtmb_autotune_batch(rtmb_ctx *ctx, uint32_t nshots, const rtmb_shot *shots, uint32_t *group_out, float *rate_out) {
+    if (!ctx || !shots || nshots == 0) return fail(ctx, RTMB_EINVAL, "rtmb_autotune_batch: no shots");
+    if (ctx->diff) return fail(ctx, RTMB_EINVAL, "rtmb_autotune_batch: the increment storage form runs single shots");
+    const rtmb_params &p = ctx->p;
+    if (p.boundary != RTMB_BC_RBC || p.stencil_order != 8 || (int)p.blen < ctx->h || p.nx == 1)
+        return fail(ctx, RTMB_EINVAL, "rtmb_autotune_batch: boundary RBC, stencil_order 8, blen >= 4, 3D (nx > 1)");
+    // the rate (padded points per ms) of the batched forward step for each group size, measured
+    // on the first shots of the batch
+    const uint32_t cand[] = {1, 2, 3, 4, 6, 8, 12, 16, 24};
+    float best = 0.f;
+    uint32_t best_g = (uint32_t)ctx->batch_group;
+    for (uint32_t g : cand) {
+        if (g > nshots || g > (uint32_t)rtmb::kMaxBatchShots) break;
+        float ms = 0.f;
+        const int rc = migrate_group(ctx, g, shots, nullptr, 0, 0, 0, 5, &ms);
+        if (rc) return rc;
+        double pts = 0;
+        for (uint32_t k = 0; k < g; ++k)
+            pts += (double)(shots[k].nx + 2 * p.blen) * (shots[k].ny + 2 * p.blen) * (shots[k].nz + 2 * p.blen);
+        const float rate = ms > 0.f ? (float)(pts / ms) : 0.f;
+        if (rate > best) { best = rate; best_g = g; }
+    }
+    ctx->batch_group = (int)best_g;
+    if (group_out) *group_out = best_g;
+    if (rate_out) *rate_out = best * 1e-6f;  // G point-updates per second
+    return check_err_flag(ctx);
+}
+
 
 // ------------------------------------------------------------------ autotuner
 

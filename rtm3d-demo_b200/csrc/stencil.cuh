@@ -115,6 +115,8 @@ struct StepArgs {
 // In-plane tile (z, y) of a launch variant of the TMA step kernel (stencil_tma_impl.cuh: Variant).
 void variant_tile(int variant, int *tz, int *ty);
 constexpr int kStepVariants = 4;
+// Shots per launch of the batched step kernel (their arguments travel as kernel parameters).
+constexpr int kMaxBatchShots = 24;
 
 // Exponent of a produced level: the smallest e with bound * 2^-e < 2^15.  bound is
 // 8 * max(amax(P), amax(PP)) + injection: a stable step (v^2 dt^2 * sum|coef| <= 4 over the three
@@ -134,7 +136,7 @@ cudaError_t launch_step(const StepArgs &a, int order, bool exact, cudaStream_t s
 
 // One launch of the step kernel over several volumes (the batched multi-shot drivers): order 8, no
 // taper, TMA-aligned volumes, the same form and the same stencil coefficients for every shot
-// (args[0]'s are used).  At most 12 shots.
+// (args[0]'s are used).  At most kMaxBatchShots shots.
 cudaError_t launch_step_batch(const StepArgs *args, int nshots, int order, bool exact, cudaStream_t s);
 
 // The dual-wavefield backward step of RBC migration: src advances the reconstructed source

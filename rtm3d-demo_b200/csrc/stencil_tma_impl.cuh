@@ -904,7 +904,7 @@ __global__ void __launch_bounds__(variant_threads<V>(), Variant<V>::MINB)
 // Several volumes in one launch (the batched multi-shot drivers): shot s owns the linear blocks
 // [start[s], start[s+1]), laid out as its own (gx, gy, gz) grid.  All shots share the stencil
 // coefficients (coef) and the kernel variant; everything else is per shot.
-constexpr int kMaxBatch = 12;
+constexpr int kMaxBatch = kMaxBatchShots;
 struct BatchArgs {
     int nshots;
     int start[kMaxBatch + 1];

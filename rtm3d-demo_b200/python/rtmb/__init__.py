@@ -120,6 +120,8 @@ SYMBOLS = [
     ("rtmb_closure_set", [_vp, _vp, C.c_float, C.c_float], C.c_int),
     ("rtmb_autotune", [_vp, C.POINTER(_u32), C.POINTER(C.c_float)], C.c_int),
     ("rtmb_autotune_full", [_vp, _vp], C.c_int),
+    ("rtmb_set_batch_group", [_vp, _u32], C.c_int),
+    ("rtmb_autotune_batch", [_vp, _u32, _vp, C.POINTER(_u32), C.POINTER(C.c_float)], C.c_int),
     ("rtmb_set_tuning", [_vp, _vp], C.c_int),
     ("rtmb_migrate_batch", [_vp, _u32, _vp, _vp, _u32, _u32, _u32], C.c_int),
     ("rtmb_set_chunk", [_vp, _u32], C.c_int),
@@ -328,6 +330,16 @@ class Context:
         arr = (Shot * len(shots))(*shots)
         nx, ny, nz = stack.shape
         self._check(self.L.rtmb_migrate_batch(self.h, len(shots), C.cast(arr, _vp), _ptr(stack), nx, ny, nz))
+
+    def set_batch_group(self, shots_per_launch: int) -> None:
+        self._check(self.L.rtmb_set_batch_group(self.h, shots_per_launch))
+
+    def autotune_batch(self, shots):
+        """Picks the shots per launch of migrate_batch; returns (group size, G point-updates/s)."""
+        arr = (Shot * len(shots))(*shots)
+        g, r = _u32(0), C.c_float(0)
+        self._check(self.L.rtmb_autotune_batch(self.h, len(shots), C.cast(arr, _vp), C.byref(g), C.byref(r)))
+        return int(g.value), float(r.value)
 
     def autotune(self):
         """Picks the fastest x-chunk length for this context; returns (chunk, ms per step)."""

@@ -97,3 +97,54 @@ def test_batch_matches_single_shots(cuda, flags):
     assert np.array_equal(got, ref), np.abs(got - ref).max()
     launches = ctx.launches
     assert launches <= 3 * NT + 2 * len(shots), launches  # one launch per batch step, not per shot
+
+
+# more shots than one launch group, apertures clipped at every survey edge (origin 0 and far edge)
+EDGE_APERTURES = APERTURES + [
+    (24, 20, 40, 36),  # reaches the far x and y edges (24 + 40 = 64, 20 + 36 = 56)
+    (0, 24, 28, 32),   # x from 0, y to the far edge
+    (36, 0, 28, 24),   # x to the far edge, y from 0
+    (12, 12, 36, 36),
+]
+
+
+def build_edge_shots(cuda):
+    global APERTURES
+    saved = APERTURES
+    APERTURES = EDGE_APERTURES
+    try:
+        return build_shots(cuda)
+    finally:
+        APERTURES = saved
+
+
+@pytest.mark.parametrize("group", [1, 3, 12])
+def test_batch_groups_match_single_shots(cuda, group):
+    """Seven shots on apertures clipped at the survey's edges, run in launch groups of 1, 3 (3 + 3 + 1)
+    and 12 shots: the stack equals the single-shot drivers' bit for bit whatever the grouping."""
+    import torch
+    shots, keep = build_edge_shots(cuda)
+    nx, ny, nz = VOLUME
+    ctx = rtmb.Context(rtmb.Params.from_input(params(nx, ny, nz, 1, 1), flags=rtmb.FLAG_FAST_FMA | rtmb.FLAG_USE_GRAPH,
+                                              device=0))
+    ctx.set_batch_group(group)
+    stack = torch.zeros(VOLUME, dtype=torch.float64, device=cuda)
+    ctx.migrate_batch(shots, stack)
+    ctx.sync()
+    ref = one_by_one(shots, rtmb.FLAG_FAST_FMA, cuda)
+    assert np.array_equal(stack.cpu().numpy(), ref)
+
+
+def test_autotune_batch_picks_a_group_and_keeps_results(cuda):
+    import torch
+    shots, keep = build_edge_shots(cuda)
+    nx, ny, nz = VOLUME
+    ctx = rtmb.Context(rtmb.Params.from_input(params(nx, ny, nz, 1, 1), flags=rtmb.FLAG_FAST_FMA, device=0))
+    g, rate = ctx.autotune_batch(shots)
+    assert g in (1, 2, 3, 4, 6) and rate > 0
+    stack = torch.zeros(VOLUME, dtype=torch.float64, device=cuda)
+    ctx.migrate_batch(shots, stack)
+    ctx.sync()
+    assert np.array_equal(stack.cpu().numpy(), one_by_one(shots, rtmb.FLAG_FAST_FMA, cuda))
+    with pytest.raises(rtmb.RtmbError):
+        ctx.set_batch_group(25)
