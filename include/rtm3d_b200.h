@@ -341,6 +341,20 @@ int rtmb_closure_collect(rtmb_ctx *wide, uint32_t sx, uint32_t sy, uint32_t sz, 
  * of the wavefront, where the network is not trained); the others are multiplied by
  * 1 - damp * ((4 - depth) / 4)^2 each step, depth 0 at the outer face (0 <= damp < 1). */
 int rtmb_closure_set(rtmb_ctx *ctx, const float *params, float min_scale, float damp);
+/* The closure's judge and fallback.  Runs the same modeling shot on three contexts of the same
+ * model, receivers, nt and device -- `learned` (RTMB_BC_LEARNED with its closure installed), `hbc`
+ * (the plain taper border, 32 cells by design) and `wide` (a border so wide that no reflection
+ * returns within nt) -- and measures each bordered run's reflected energy as the record rel-L2
+ * against the wide run's record (on device, double accumulation).  The learned context passes when
+ * it reflects no more than the taper border; otherwise it is marked fallen back.  Outputs: both
+ * reflections. */
+int rtmb_closure_judge(rtmb_ctx *learned, rtmb_ctx *hbc, rtmb_ctx *wide, uint32_t sx, uint32_t sy, uint32_t sz,
+                       float *refl_learned, float *refl_hbc);
+/* Modeling with the judged boundary: the learned context's shot when its closure passed its judge,
+ * else the fallback (taper-border) context's shot; *ran (optional) receives RTMB_BC_LEARNED or the
+ * fallback's boundary.  The learned context must have been judged. */
+int rtmb_model_shot_judged(rtmb_ctx *learned, rtmb_ctx *fallback, uint32_t sx, uint32_t sy, uint32_t sz, float *rec,
+                           int *ran);
 
 /* ------------------------------------------------------------------ batched multi-shot migration
  * No reference counterpart (the reference migrates one shot per process, RTMAcousticController.cpp:

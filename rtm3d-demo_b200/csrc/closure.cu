@@ -13,6 +13,7 @@
 
 #include "closure.cuh"
 #include "ctx.hpp"
+#include "ops.cuh"
 #include "umma.cuh"
 
 namespace rtmb {
@@ -791,6 +792,84 @@ int rtmb_closure_set(rtmb_ctx *ctx, const float *params, float min_scale, float 
         cudaStreamSynchronize(ctx->stream) != cudaSuccess)
         return RTMB_ECUDA;
     return RTMB_OK;
+}
+
+// Reflected energy of a bordered run: the record rel-L2 against the wide run's record, both modeled
+// on device (the same model, receivers and shot; only the border differs).
+namespace {
+int model_record(rtmb_ctx *c, uint32_t sx, uint32_t sy, uint32_t sz, float *rec) {
+    const int rc = rtmb_model_shot(c, sx, sy, sz, rec);
+    return rc ? rc : rtmb_sync(c);
+}
+}  // namespace
+
+int rtmb_closure_judge(rtmb_ctx *learned, rtmb_ctx *hbc, rtmb_ctx *wide, uint32_t sx, uint32_t sy, uint32_t sz,
+                       float *refl_learned, float *refl_hbc) {
+    if (!learned || !hbc || !wide) return RTMB_EINVAL;
+    const rtmb_params &a = learned->p, &b = hbc->p, &w = wide->p;
+    auto same = [](const rtmb_params &x, const rtmb_params &y) {
+        return x.nx == y.nx && x.ny == y.ny && x.nz == y.nz && x.nt == y.nt && x.ntstep == y.ntstep &&
+               x.receiver_start_x == y.receiver_start_x && x.receiver_start_y == y.receiver_start_y &&
+               x.receiver_depth_z == y.receiver_depth_z && x.receiver_distance_x == y.receiver_distance_x &&
+               x.receiver_distance_y == y.receiver_distance_y && x.receiver_count_x == y.receiver_count_x &&
+               x.receiver_count_y == y.receiver_count_y && x.device == y.device;
+    };
+    if (a.boundary != RTMB_BC_LEARNED || !learned->d_cparams || b.boundary == RTMB_BC_LEARNED ||
+        w.boundary == RTMB_BC_LEARNED || !same(a, b) || !same(a, w) || w.blen <= b.blen) {
+        learned->err = "rtmb_closure_judge: a learned context with its closure installed, a taper-border context "
+                       "and a wider one, on the same model, receivers, nt and device";
+        return RTMB_EINVAL;
+    }
+    if (cudaSetDevice(learned->device) != cudaSuccess) return RTMB_ECUDA;
+    const size_t nrec = (size_t)a.nt * a.receiver_count_x * a.receiver_count_y;
+    float *rec = nullptr;
+    double *acc = nullptr;
+    if (cudaMalloc(&rec, 3 * nrec * sizeof(float)) != cudaSuccess || cudaMalloc(&acc, 4 * sizeof(double)) != cudaSuccess) {
+        if (rec) cudaFree(rec);
+        learned->err = "rtmb_closure_judge: device allocation failed";
+        return RTMB_ENOMEM;
+    }
+    int rc = model_record(wide, sx, sy, sz, rec);
+    if (!rc) rc = model_record(learned, sx, sy, sz, rec + nrec);
+    if (!rc) rc = model_record(hbc, sx, sy, sz, rec + 2 * nrec);
+    double h[4] = {0, 0, 0, 0};
+    if (!rc) {
+        cudaStream_t s = learned->stream;
+        const bool ok = cudaMemsetAsync(acc, 0, 4 * sizeof(double), s) == cudaSuccess &&
+                        rtmb::launch_sqdiff(rec + nrec, rec, nrec, acc, s) == cudaSuccess &&
+                        rtmb::launch_sqdiff(rec + 2 * nrec, rec, nrec, acc + 2, s) == cudaSuccess &&
+                        cudaMemcpyAsync(h, acc, sizeof h, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+                        cudaStreamSynchronize(s) == cudaSuccess;
+        if (!ok) rc = RTMB_ECUDA;
+    }
+    cudaFree(rec);
+    cudaFree(acc);
+    if (rc) return rc;
+    const float rl = h[1] > 0 ? (float)std::sqrt(h[0] / h[1]) : 0.f;
+    const float rh = h[3] > 0 ? (float)std::sqrt(h[2] / h[3]) : 0.f;
+    // the judge: the learned strip may reflect no more than the 32-cell taper border
+    learned->closure_verdict = rl <= rh ? 1 : 2;
+    if (refl_learned) *refl_learned = rl;
+    if (refl_hbc) *refl_hbc = rh;
+    return RTMB_OK;
+}
+
+int rtmb_model_shot_judged(rtmb_ctx *learned, rtmb_ctx *fallback, uint32_t sx, uint32_t sy, uint32_t sz, float *rec,
+                           int *ran) {
+    if (!learned || !fallback || !rec) return RTMB_EINVAL;
+    if (learned->closure_verdict == 0) {
+        learned->err = "rtmb_model_shot_judged: judge the closure first (rtmb_closure_judge)";
+        return RTMB_EINVAL;
+    }
+    if (fallback->p.boundary == RTMB_BC_LEARNED || fallback->p.nt != learned->p.nt ||
+        fallback->p.receiver_count_x != learned->p.receiver_count_x ||
+        fallback->p.receiver_count_y != learned->p.receiver_count_y) {
+        learned->err = "rtmb_model_shot_judged: the fallback context must be a taper-border context of the same shot geometry";
+        return RTMB_EINVAL;
+    }
+    const bool use_learned = learned->closure_verdict == 1;
+    if (ran) *ran = use_learned ? RTMB_BC_LEARNED : (int)fallback->p.boundary;
+    return rtmb_model_shot(use_learned ? learned : fallback, sx, sy, sz, rec);
 }
 
 int rtmb_closure_collect(rtmb_ctx *wide, uint32_t sx, uint32_t sy, uint32_t sz, uint32_t t0, uint32_t tstride,

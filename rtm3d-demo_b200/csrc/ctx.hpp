@@ -56,6 +56,7 @@ struct rtmb_ctx {
     float *d_side = nullptr;
     float *d_cparams = nullptr;
     float closure_min_scale = 0.f, closure_damp = 0.f;
+    int closure_verdict = 0;  // rtmb_closure_judge: 0 not judged, 1 passed, 2 fell back to the taper border
     // FP64 GPU oracle (f64.cu)
     double *d_f64[4] = {};
     double *d_upb64 = nullptr;

@@ -148,6 +148,24 @@ __global__ void absmax_kernel(const float *__restrict__ x, size_t n, unsigned *o
     if ((threadIdx.x & 31) == 0 && b) atomicMax(out, b);
 }
 
+// out[0] += sum (a - b)^2, out[1] += sum b^2 over n floats, in double (zero beforehand)
+__global__ void sqdiff_kernel(const float *__restrict__ a, const float *__restrict__ b, size_t n, double *out) {
+    double d2 = 0.0, b2 = 0.0;
+    for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
+        const double d = (double)a[o] - (double)b[o];
+        d2 += d * d;
+        b2 += (double)b[o] * (double)b[o];
+    }
+    for (int k = 16; k; k >>= 1) {
+        d2 += __shfl_xor_sync(0xffffffffu, d2, k);
+        b2 += __shfl_xor_sync(0xffffffffu, b2, k);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(out, d2);
+        atomicAdd(out + 1, b2);
+    }
+}
+
 // max amax over n scale records into *out (zero beforehand)
 __global__ void scale_max_kernel(const ScaleRec *__restrict__ r, int n, unsigned *out) {
     unsigned m = 0;
@@ -304,6 +322,12 @@ cudaError_t launch_scale_max(const ScaleRec *r, int n, float *out, cudaStream_t 
     cudaError_t e = cudaMemsetAsync(out, 0, sizeof(float), s);
     if (e != cudaSuccess || n <= 0) return e;
     scale_max_kernel<<<1, 256, 0, s>>>(r, n, reinterpret_cast<unsigned *>(out));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sqdiff(const float *a, const float *b, size_t n, double *out, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    sqdiff_kernel<<<grid1d(n), 256, 0, s>>>(a, b, n, out);
     return cudaGetLastError();
 }
 

@@ -78,6 +78,8 @@ cudaError_t launch_diff_rewind(int store, const void *p, void *d, void *pout, co
                                ScaleRec *so, size_t n, cudaStream_t s);
 // *out = max |x| over n floats.
 cudaError_t launch_absmax(const float *x, size_t n, float *out, cudaStream_t s);
+// out[0] += sum (a - b)^2, out[1] += sum b^2 over n floats (double accumulators, zero beforehand).
+cudaError_t launch_sqdiff(const float *a, const float *b, size_t n, double *out, cudaStream_t s);
 // *out = max amax over n scale records.
 cudaError_t launch_scale_max(const ScaleRec *r, int n, float *out, cudaStream_t s);
 // out = (float) a over n values.

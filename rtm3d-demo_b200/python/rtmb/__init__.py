@@ -120,6 +120,8 @@ SYMBOLS = [
     ("rtmb_closure_set", [_vp, _vp, C.c_float, C.c_float], C.c_int),
     ("rtmb_autotune", [_vp, C.POINTER(_u32), C.POINTER(C.c_float)], C.c_int),
     ("rtmb_autotune_full", [_vp, _vp], C.c_int),
+    ("rtmb_closure_judge", [_vp, _vp, _vp, _u32, _u32, _u32, C.POINTER(C.c_float), C.POINTER(C.c_float)], C.c_int),
+    ("rtmb_model_shot_judged", [_vp, _vp, _u32, _u32, _u32, _vp, C.POINTER(_i32)], C.c_int),
     ("rtmb_set_batch_group", [_vp, _u32], C.c_int),
     ("rtmb_autotune_batch", [_vp, _u32, _vp, C.POINTER(_u32), C.POINTER(C.c_float)], C.c_int),
     ("rtmb_set_tuning", [_vp, _vp], C.c_int),
@@ -317,6 +319,20 @@ class Context:
     def closure_set(self, params, min_scale: float = 0.0, damp: float = 0.0):
         """Installs the learned closure (device or host float32 params) in a BC_LEARNED context."""
         self._check(self.L.rtmb_closure_set(self.h, _ptr(params), min_scale, damp))
+
+    def closure_judge(self, hbc: "Context", wide: "Context", sx: int, sy: int, sz: int):
+        """Judges this learned context against the taper border (rtmb_closure_judge); returns
+        (reflection of the learned strip, reflection of the taper border, passed)."""
+        rl, rh = C.c_float(0), C.c_float(0)
+        self._check(self.L.rtmb_closure_judge(self.h, hbc.h, wide.h, sx, sy, sz, C.byref(rl), C.byref(rh)))
+        return float(rl.value), float(rh.value), bool(rl.value <= rh.value)
+
+    def model_shot_judged(self, fallback: "Context", sx: int, sy: int, sz: int, rec) -> int:
+        """Modeling with the judged boundary; returns the boundary that ran (BC_LEARNED or the
+        fallback's)."""
+        ran = _i32(0)
+        self._check(self.L.rtmb_model_shot_judged(self.h, fallback.h, sx, sy, sz, _ptr(rec), C.byref(ran)))
+        return int(ran.value)
 
     def closure_collect(self, sx, sy, sz, t0, tstride, per_step, seed, min_scale, X, R) -> int:
         """Training pairs from a modeling shot on this (wide) context; returns the row count."""

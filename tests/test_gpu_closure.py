@@ -176,3 +176,43 @@ def test_learned_closure_beats_the_plain_8_cell_border(cuda):
     assert e_l < e_8
     # plain HBC decides: the run falls back to it when the closure reflects more than 32 cells do
     assert rtmb.closure_falls_back(e_l, e_32) == (e_l > e_32)
+
+
+def _ctx(case, blen, learned=False):
+    prm = rtmb.Params.from_input(params_for(case, blen, "hbc"), device=0)
+    if learned:
+        prm.boundary = rtmb.BC_LEARNED
+    ctx = rtmb.Context(prm)
+    ctx.load_v2dt2(rtmb.v2dt2(rtmb.prepare_velocity(velocity(case), blen, "abc"), case["dt"]), from_host=True)
+    return ctx
+
+
+def test_judge_falls_back_to_the_taper_border(cuda):
+    """rtmb_closure_judge runs the shot with the learned strip, the 32-cell taper and a wide border
+    and measures both reflections on the device; an untrained network (random weights) reflects
+    more than the taper, so the judged modeling call runs the taper-border context and says so, and
+    its record is that context's record bit for bit.  The measured reflections agree with the same
+    rel-L2 computed on the host."""
+    import torch
+    case, wide, shot = CASE, 72, (22, 19, 5)
+    learned, hbc, wctx = _ctx(case, 8, learned=True), _ctx(case, 32), _ctx(case, wide)
+    learned.closure_set(to_dev(rtmb.closure_init(3), cuda), 0.0, 0.3)
+    with pytest.raises(rtmb.RtmbError):  # not judged yet
+        learned.model_shot_judged(hbc, *shot, torch.zeros(1, device=cuda))
+    rl, rh, passed = learned.closure_judge(hbc, wctx, *shot)
+    n = case["nx"]
+    shape = (1, n // case["rdx"], case["ny"] // case["rdy"], case["nt"])
+    recs = {}
+    for name, c in (("wide", wctx), ("learned", learned), ("hbc", hbc)):
+        r = torch.zeros(shape, device=cuda)
+        c.model_shot(*shot, r)
+        c.sync()
+        recs[name] = r.cpu().numpy()
+    assert abs(rl - rel_l2(recs["learned"], recs["wide"])) <= 1e-4 * max(1.0, rl)
+    assert abs(rh - rel_l2(recs["hbc"], recs["wide"])) <= 1e-4 * max(1.0, rh)
+    assert not passed and rl > rh
+    out = torch.zeros(shape, device=cuda)
+    ran = learned.model_shot_judged(hbc, *shot, out)
+    learned.sync()
+    assert ran == rtmb.BC_HBC
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), recs["hbc"].view(np.uint32))
