@@ -605,41 +605,60 @@ def survey_model(nx: int, ny: int, nz: int, dz: float, seed: int = 1234) -> np.n
 
 
 def run_batch(args) -> dict:
-    """Shots on uneven aperture sub-volumes of a survey, batched (rtmb_migrate_batch: one launch per
-    step for all shots, graph-captured time loop) against the single-shot driver one by one."""
+    """Shots on uneven aperture sub-volumes of a survey, batched (rtmb_migrate_batch: the shots of a
+    launch group advance together, one launch per step for the group, graph-captured time loop, the
+    group size picked by rtmb_autotune_batch) against the single-shot driver one by one.
+
+    --batch-config c4 (the batched configuration): a 1024 x 1024 x 512 survey at 12.5 m, 64 shots on
+    an 8 x 8 surface grid, apertures +-256 cells around the source clipped at the survey's edges
+    (320 to 512 cells wide), 40-cell RBC border, 10 Hz Ricker, 2500 steps, 16-bit storage; the
+    one-by-one comparison runs the 8 shots of the grid's diagonal (one per aperture width).
+    --batch-config small: a 512 x 512 x 256 survey, 12 shots on a 4 x 3 grid, apertures +-128, nt 500."""
     import torch
     import rtmb
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    snx, sny, snz = 2 * args.batch_size, 2 * args.batch_size, args.batch_size
-    blen, nt, dx = 40, args.batch_nt, 12.5
+    c4 = args.batch_config == "c4"
+    if c4:
+        snx, sny, snz, half, nt, gx, gy = 1024, 1024, 512, 256, 2500, 8, 8
+        form = args.form if args.form != "fp32_fma" else "fp16"
+    else:
+        snx, sny, snz, half, nt, gx, gy = 2 * args.batch_size, 2 * args.batch_size, args.batch_size, \
+            args.batch_size // 2, args.batch_nt, 4, 3
+        form = args.form
+    blen, dx = 40, 12.5
+    t_prep = time.time()
     v = survey_model(snx, sny, snz, dx)
-    half = args.batch_size // 2  # apertures +-half cells around the source, clipped at the survey edges
-    grid = [(int(snx * (i + 0.5) / 4), int(sny * (j + 0.5) / 3)) for i in range(4) for j in range(3)]
-    flags = form_flags(rtmb, args.form) | rtmb.FLAG_USE_GRAPH
+    grid = [(int(snx * (i + 0.5) / gx), int(sny * (j + 0.5) / gy)) for i in range(gx) for j in range(gy)]
+    flags = form_flags(rtmb, form) | rtmb.FLAG_USE_GRAPH
     keep, shots = [], []
-    rng = np.random.default_rng(7)
-    for k, (gx, gy) in enumerate(grid):
-        x0, x1 = max(0, gx - half), min(snx, gx + half)
-        y0, y1 = max(0, gy - half), min(sny, gy + half)
+    for k, (sx_, sy_) in enumerate(grid):
+        x0, x1 = max(0, sx_ - half), min(snx, sx_ + half)
+        y0, y1 = max(0, sy_ - half), min(sny, sy_ + half)
         nx, ny = x1 - x0, y1 - y0
-        ve = rtmb.prepare_velocity(v[x0:x1, y0:y1, :], blen, "rbc", seed=100 + k)
+        ve = rtmb.prepare_velocity(np.ascontiguousarray(v[x0:x1, y0:y1, :]), blen, "rbc", seed=100 + k)
         v2 = torch.from_numpy(rtmb.v2dt2(ve, 0.001)).to(dev)
+        del ve
         rcx, rcy = nx // 2, ny // 2
-        rec = torch.from_numpy((rng.standard_normal((1, rcx, rcy, nt)) * 1e-3).astype(np.float32)).to(dev)
+        gen = torch.Generator(device=dev).manual_seed(7 + k)
+        rec = torch.randn((1, rcx, rcy, nt), generator=gen, device=dev) * 1e-3
         keep += [v2, rec]
-        shots.append(rtmb.Shot(nx=nx, ny=ny, nz=snz, ox=x0, oy=y0, oz=0, sx=gx - x0, sy=gy - y0, sz=0,
+        shots.append(rtmb.Shot(nx=nx, ny=ny, nz=snz, ox=x0, oy=y0, oz=0, sx=sx_ - x0, sy=sy_ - y0, sz=0,
                                receiver_start_x=0, receiver_start_y=0, receiver_depth_z=0, receiver_distance_x=2,
                                receiver_distance_y=2, receiver_count_x=rcx, receiver_count_y=rcy,
                                v2dt2=v2.data_ptr(), rec=rec.data_ptr()))
+    del v
+    t_prep = time.time() - t_prep
     base = dict(nx=snx, ny=sny, nz=snz, blen=blen, nt=nt, ntstep=nt, stencil_order=8, dx=dx, dy=dx, dz=dx, dt=0.001,
                 fpeak=10.0, taper_factor=0.2, receiver_start_x=0, receiver_start_y=0, receiver_depth_z=0,
                 receiver_distance_x=2, receiver_distance_y=2, receiver_count_x=1, receiver_count_y=1,
                 boundary_condition="rbc")
     ctx = rtmb.Context(rtmb.Params.from_input(base, flags=flags, device=0))
+    group, rate = ctx.autotune_batch(shots)
     stack = torch.zeros((snx, sny, snz), dtype=torch.float64, device=dev)
-    ctx.migrate_batch(shots, stack)  # warm-up: graph capture and instantiation
-    ctx.sync()
+    if not c4:
+        ctx.migrate_batch(shots, stack)  # warm-up: graph capture and instantiation
+        ctx.sync()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     l0 = ctx.launches
     e0.record()
@@ -648,16 +667,20 @@ def run_batch(args) -> dict:
     ctx.sync()
     ms_batch = e0.elapsed_time(e1)
     launches_batch = ctx.launches - l0
-    # one by one: the single-shot driver per aperture, images stacked in FP64
+    pts_all = sum((s.nx + 2 * blen) * (s.ny + 2 * blen) * (snz + 2 * blen) for s in shots)
+    # one by one: the single-shot driver per aperture, images stacked in FP64 (the grid's diagonal
+    # for c4: one shot per aperture width)
+    subset = [shots[i * gy + i] for i in range(min(gx, gy))] if c4 else shots
     ms_single = 0.0
     pts = 0
-    for s in shots:
+    for s in subset:
         q = dict(base, nx=s.nx, ny=s.ny, receiver_count_x=s.receiver_count_x, receiver_count_y=s.receiver_count_y)
-        c = rtmb.Context(rtmb.Params.from_input(q, flags=form_flags(rtmb, args.form), device=0))
+        c = rtmb.Context(rtmb.Params.from_input(q, flags=form_flags(rtmb, form), device=0))
         c.load_v2dt2(s.v2dt2, from_host=False)
         acc = torch.zeros(c.padded_shape, dtype=torch.float64, device=dev)
-        c.migrate_shot_acc64(s.sx, s.sy, s.sz, s.rec, acc)
-        c.sync()
+        if not c4:
+            c.migrate_shot_acc64(s.sx, s.sy, s.sz, s.rec, acc)
+            c.sync()
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a0.record()
         c.migrate_shot_acc64(s.sx, s.sy, s.sz, s.rec, acc)
@@ -666,16 +689,21 @@ def run_batch(args) -> dict:
         ms_single += a0.elapsed_time(a1)
         pts += int(np.prod(c.padded_shape))
         c.close()
-    upd = pts * (3 * nt - 2)
+        del acc
+    upd_single = pts * (3 * nt - 2)
+    upd_batch = pts_all * (3 * nt - 2)
     sizes = sorted({(s.nx, s.ny) for s in shots})
-    return {"metric": "s per migrated shot, batched aperture shots", "workload": "batch",
+    gpt_b, gpt_1 = upd_batch / ms_batch / 1e6, upd_single / ms_single / 1e6
+    return {"metric": "s per migrated shot, batched aperture shots", "workload": f"batch_{args.batch_config}",
             "config": {"survey": [snx, sny, snz], "dx_m": dx, "shots": len(shots), "apertures_xy": sizes,
-                       "blen": blen, "nt": nt, "form": args.form, "fpeak_hz": 10.0},
-            "batched": {"s_per_shot": round(ms_batch / 1e3 / len(shots), 4), "gpt_s": round(upd / ms_batch / 1e6, 2),
-                        "launches": launches_batch},
-            "one_by_one": {"s_per_shot": round(ms_single / 1e3 / len(shots), 4),
-                           "gpt_s": round(upd / ms_single / 1e6, 2)},
-            "speedup": round(ms_single / ms_batch, 3)}
+                       "blen": blen, "nt": nt, "form": form, "fpeak_hz": 10.0, "graph": True,
+                       "shots_per_launch": group, "autotune_rate_gpt_s": round(rate, 2),
+                       "host_preparation_s": round(t_prep, 1)},
+            "batched": {"s_per_shot": round(ms_batch / 1e3 / len(shots), 4), "gpt_s": round(gpt_b, 2),
+                        "launches": launches_batch, "s_total": round(ms_batch / 1e3, 2)},
+            "one_by_one": {"shots": len(subset), "s_per_shot": round(ms_single / 1e3 / len(subset), 4),
+                           "gpt_s": round(gpt_1, 2)},
+            "speedup_per_point_update": round(gpt_b / gpt_1, 3)}
 
 
 # ------------------------------------------------------------------------------------------ model
@@ -866,7 +894,7 @@ def run_closure(args) -> dict:
     t0 = time.time()
     pilot, _ = model(wide, train[0])
     min_scale = 1e-4 * float(pilot.abs().max())
-    per_step, ts0, tstride = 4096, nt // 6, 2
+    per_step, ts0, tstride = args.closure_rows_per_step, nt // 6, 2
     cap = len(train) * per_step * ((nt - ts0) // tstride + 1)
     X = torch.zeros((cap, rtmb.CLOSURE_NIN), dtype=torch.bfloat16, device=dev)
     R = torch.zeros(cap, dtype=torch.float32, device=dev)
@@ -898,7 +926,29 @@ def run_closure(args) -> dict:
             res[key].append(float(torch.linalg.vector_norm((r - ref).double()) / torch.linalg.vector_norm(ref.double())))
             ms[key].append(t)
     mean = {k: float(np.mean(x)) for k, x in res.items()}
+    # the in-driver judge on the validation shot (rtmb_closure_judge) and the judged modeling call
+    # on each held-out shot (rtmb_model_shot_judged): the boundary that ran
+    def ctx_of(blen, closure=None):
+        par = rtmb.Params.from_input(prm(blen), flags=rtmb.FLAG_FAST_FMA, device=0)
+        if closure is not None:
+            par.boundary = rtmb.BC_LEARNED
+        c = rtmb.Context(par)
+        c.load_v2dt2(rtmb.v2dt2(rtmb.prepare_velocity(v, blen, "abc"), 0.001), from_host=True)
+        if closure is not None:
+            c.closure_set(closure, min_scale, 0.3)
+        return c
+    lc, hc, wc = ctx_of(8, params), ctx_of(32), ctx_of(wide)
+    j_l, j_h, passed = lc.closure_judge(hc, wc, *val)
+    ran = []
+    for sh in held:
+        r = torch.zeros((1, n // 2, n // 2, nt), device=dev)
+        ran.append("learned_8" if lc.model_shot_judged(hc, *sh, r) == rtmb.BC_LEARNED else "taper_32")
+    lc.sync()
+    for c in (lc, hc, wc):
+        c.close()
     return {"metric": "reflected energy (record rel-L2 vs wide-padded run) and modeling time", "workload": "closure",
+            "judge": {"shot": list(val), "reflection_learned_8": round(j_l, 4), "reflection_taper_32": round(j_h, 4),
+                      "passed": passed, "ran_on_held_out_shots": ran},
             "config": {"model": [n, n, n], "nt": nt, "wide_border": wide, "fpeak_hz": 15.0,
                        "train_shots": len(train), "eval_shots": len(held), "rows": rows,
                        "train_steps": args.closure_steps, "batch": 8192, "candidates": args.closure_candidates,
@@ -973,14 +1023,21 @@ def main():
     ap.add_argument("--fmig-band", type=float, nargs=2, default=(4.0, 20.0))
     ap.add_argument("--fmig-nwstep", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--batch-size", type=int, default=256, help="batch workload: survey 2s x 2s x s cells")
+    ap.add_argument("--batch-config", choices=("small", "c4"), default="small",
+                    help="batch workload: c4 = 64 shots on a 1024 x 1024 x 512 survey, nt 2500; small = 12 shots")
+    ap.add_argument("--batch-size", type=int, default=256, help="batch workload (small): survey 2s x 2s x s cells")
     ap.add_argument("--batch-nt", type=int, default=500)
+    ap.add_argument("--closure-config", choices=("small", "c5"), default="small",
+                    help="closure workload: c5 = 384^3 at 10 m, nt 2000, training on a 200-cell-padded run, 64 "
+                         "training and 16 held-out shots; small = the sizes given by the --closure-* options")
     ap.add_argument("--closure-size", type=int, default=96)
     ap.add_argument("--closure-nt", type=int, default=600)
     ap.add_argument("--closure-wide", type=int, default=120)
     ap.add_argument("--closure-train-shots", type=int, default=8)
     ap.add_argument("--closure-eval-shots", type=int, default=4)
     ap.add_argument("--closure-steps", type=int, default=8000)
+    ap.add_argument("--closure-rows-per-step", type=int, default=4096,
+                    help="training pairs sampled per collected time step of each training shot")
     ap.add_argument("--closure-candidates", type=int, default=3,
                     help="networks trained with different seeds; the one reflecting least on a validation shot is kept")
     ap.add_argument("--forms-nt", type=int, default=0,
@@ -996,6 +1053,9 @@ def main():
     ap.add_argument("--c3-grid", type=int, nargs=3, default=(896, 896, 512))
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.closure_config == "c5":
+        args.closure_size, args.closure_nt, args.closure_wide = 384, 2000, 200
+        args.closure_train_shots, args.closure_eval_shots, args.closure_rows_per_step = 64, 16, 2048
     if args.exact:
         args.form = "fp32_exact"
 
