@@ -254,9 +254,9 @@ def build_inputs(p: dict, with_abc: bool):
     return v, vpe, v2, v2m
 
 
-FORMS = ("fp32_exact", "fp32_fma", "fp16", "bf16", "fp16_img64", "bf16_img64", "fp16_diff", "bf16_diff",
-         "fp16_diff_img64")
-C3_FORMS = ("fp32_exact", "fp32_fma", "fp16", "bf16", "fp16_diff", "bf16_diff")
+FORMS = ("fp32_exact", "fp32_fma", "fp16", "bf16", "fp16_diff", "bf16_diff")
+C3_FORMS = FORMS
+ALL_FORMS = FORMS + ("fp16_img64", "bf16_img64", "fp16_diff_img64", "bf16_diff_img64")
 
 
 def form_flags(rtmb, form: str) -> int:
@@ -1009,7 +1009,7 @@ def main():
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--size", type=int, default=512, help="model edge in cells (workload: 512)")
     ap.add_argument("--nt", type=int, default=3000)
-    ap.add_argument("--form", choices=FORMS, default="fp32_fma", help="arithmetic/storage form of the timed shots")
+    ap.add_argument("--form", choices=ALL_FORMS, default="fp32_fma", help="arithmetic/storage form of the timed shots")
     ap.add_argument("--exact", action="store_true", help="same as --form fp32_exact")
     ap.add_argument("--workload", choices=("rtm", "batch", "closure", "fmig", "model", "precision"), default="rtm",
                     help="rtm: the single-shot RTM line (default); batch: batched aperture shots against "

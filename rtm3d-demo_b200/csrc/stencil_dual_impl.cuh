@@ -323,8 +323,8 @@ __global__ void __launch_bounds__(kDualThreads, 2)
         int p_issued = 0, c_issued = 0;
         for (int k = 0; k < nplanes && ok; ++k) {
             const int s = k % D;
-            if (k >= D && (!(ok = mbar_wait(&pempty_s[s], ((k / D) + 1) & 1)) ||
-                           !(ok = mbar_wait(&pempty_r[s], ((k / D) + 1) & 1))))
+            if (k >= D && (!(ok = mbar_wait_producer(&pempty_s[s], ((k / D) + 1) & 1)) ||
+                           !(ok = mbar_wait_producer(&pempty_r[s], ((k / D) + 1) & 1))))
                 break;
             mbar_expect_tx(&pfull_s[s], STAGE * 4);
             tma_load_3d(ring_s + s * STRIDE, &maps.ps, &pfull_s[s], zt0 - ZH, yt0 - H, xc0 - H + k);
@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(kDualThreads, 2)
             p_issued = k + 1;
             if (k >= 2 * H) {
                 const int i = k - 2 * H, cs = i % R;
-                if (i >= R && !(ok = mbar_wait(&cempty[cs], ((i / R) + 1) & 1))) break;
+                if (i >= R && !(ok = mbar_wait_producer(&cempty[cs], ((i / R) + 1) & 1))) break;
                 unsigned char *dst = cring + cs * CSLOT;
                 mbar_expect_tx(&cfull[cs], CSLOT);
                 tma_load_3d(dst, &maps.pps, &cfull[cs], zt0, yt0, xc0 + i);
@@ -346,11 +346,11 @@ __global__ void __launch_bounds__(kDualThreads, 2)
         if (!ok && a.err) atomicOr(a.err, 2u);
         // stay until every copy this CTA issued has landed (bounded), so none outlives the CTA
         for (int k = p_issued > D ? p_issued - D : 0; k < p_issued; ++k) {
-            if (!mbar_wait(&pfull_s[k % D], (k / D) & 1)) break;
-            if (!mbar_wait(&pfull_r[k % D], (k / D) & 1)) break;
+            if (!mbar_wait_producer(&pfull_s[k % D], (k / D) & 1)) break;
+            if (!mbar_wait_producer(&pfull_r[k % D], (k / D) & 1)) break;
         }
         for (int i = c_issued > R ? c_issued - R : 0; i < c_issued; ++i)
-            if (!mbar_wait(&cfull[i % R], (i / R) & 1)) break;
+            if (!mbar_wait_producer(&cfull[i % R], (i / R) & 1)) break;
         return;
     }
     if (tid < kGThreads)

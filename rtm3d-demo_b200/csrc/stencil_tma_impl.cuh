@@ -70,6 +70,22 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
     return true;
 }
 
+// The producer's bounded wait for a free slot: the same limit as mbar_wait, with a sleep between
+// polls (32 ns doubling to 512 ns).  The producer runs several planes ahead of the consumers and
+// spends most of its time waiting for them; polling without a pause would take issue slots from the
+// consumer warps of its SM sub-partition.
+__device__ __forceinline__ bool mbar_wait_producer(uint64_t *bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    unsigned ns = 32;
+    while (!mbar_try_wait(bar, parity)) {
+        if (clock64() - t0 > (1ll << 32)) return false;
+        __nanosleep(ns);
+        ns = ns < 512 ? 2 * ns : 512;
+    }
+    return true;
+}
+
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0, int c1,
                                             int c2) {
     asm volatile(
@@ -376,13 +392,13 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
         int p_issued = 0, c_issued = 0;
         for (int k = 0; k < nplanes && ok; ++k) {
             const int s = k % D;
-            if (k >= D && !(ok = mbar_wait(&pempty[s], ((k / D) + 1) & 1))) break;
+            if (k >= D && !(ok = mbar_wait_producer(&pempty[s], ((k / D) + 1) & 1))) break;
             mbar_expect_tx(&pfull[s], STAGE * sizeof(T));
             tma_load_3d(pring + s * STRIDE, &maps.p, &pfull[s], zt0 - ZH, yt0 - H, xc0 - H + k);
             p_issued = k + 1;
             if (k >= 2 * H) {
                 const int i = k - 2 * H, cs = i % R;
-                if (i >= R && !(ok = mbar_wait(&cempty[cs], ((i / R) + 1) & 1))) break;
+                if (i >= R && !(ok = mbar_wait_producer(&cempty[cs], ((i / R) + 1) & 1))) break;
                 unsigned char *dst = cring + cs * CSLOT;
                 mbar_expect_tx(&cfull[cs], CSLOT);
                 tma_load_3d(dst, &maps.pp, &cfull[cs], zt0, yt0, xc0 + i);
@@ -397,9 +413,9 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
         if (!ok && a.err) atomicOr(a.err, 2u);
         // stay until every copy this CTA issued has landed (bounded), so none outlives the CTA
         for (int k = p_issued > D ? p_issued - D : 0; k < p_issued; ++k)
-            if (!mbar_wait(&pfull[k % D], (k / D) & 1)) break;
+            if (!mbar_wait_producer(&pfull[k % D], (k / D) & 1)) break;
         for (int i = c_issued > R ? c_issued - R : 0; i < c_issued; ++i)
-            if (!mbar_wait(&cfull[i % R], (i / R) & 1)) break;
+            if (!mbar_wait_producer(&cfull[i % R], (i / R) & 1)) break;
         return;
     }
     const int lane = tid & 31;

@@ -211,7 +211,7 @@ def test_increment_storage_scope(cuda, oracle):
     """The increment form migrates with RBC; modeling and HBC migration are refused, and so is the
     flag without a 16-bit type."""
     import torch
-    case = CASES["golden"]
+    case = CASES["mid"]  # nz + 2 blen = 128: rows of 16-bit values in whole 16-byte units
     flags = rtmb.FLAG_STORE_F16 | rtmb.FLAG_STORE_DIFF
     for bc, call in (("hbc", "model"), ("hbc", "migrate")):
         ctx = ctx_for(case, bc, flags)
