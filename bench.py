@@ -236,6 +236,16 @@ def run_reference_program(binary: str, p: dict, v: np.ndarray, rec: np.ndarray |
     return t, upd, threads, out_rec
 
 
+def workload_config(args, p: dict, world: int) -> dict:
+    """The workload description shared by both arms of the benchmark."""
+    b = p["blen"]
+    return {"workload": f"rtm_rbc_{args.size}^3_nt{args.nt}",
+            "grid": [p["nx"] + 2 * b, p["ny"] + 2 * b, p["nz"] + 2 * b], "nt": p["nt"], "stencil_order": 8,
+            "boundary": "rbc", "shots_per_step_per_gpu": 1,
+            "l2": "inputs larger than L2 (%.0f MB per wavefield)" % (n_points(p) * 4 / 1e6),
+            "parallelism": f"shot-parallel x{world}"}
+
+
 def ref_gpu_bin() -> str:
     return os.path.join(ROOT, "oracle", "_ref", "RTM3D_GPU.bin")
 
@@ -279,7 +289,7 @@ def rel_l2_dev(a, ref, ref_norm: float) -> float:
 
 
 def compare_forms(p: dict, v2: np.ndarray, v2m: np.ndarray | None, rec_full, dev, nt_cmp: int,
-                  forms=FORMS) -> dict:
+                  forms=FORMS, autotune: bool = True) -> dict:
     """Per-form device time and error against the FP64 GPU oracle on the same grid, over nt_cmp
     steps (the full nt by default): the migrated image of the given record (image rel-L2) and, when
     v2m (the modeling velocity) is given, the modeled shot record (record rel-L2)."""
@@ -316,6 +326,8 @@ def compare_forms(p: dict, v2: np.ndarray, v2m: np.ndarray | None, rec_full, dev
         fl = form_flags(rtmb, name)
         c = rtmb.Context(rtmb.Params.from_input(q, flags=fl, device=d))
         c.load_v2dt2(v2, from_host=True)
+        if autotune:
+            c.autotune_full()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -462,6 +474,8 @@ def run_b200(args, rank: int, world: int, local_rank: int) -> dict | None:
     ctx = rtmb.Context(params)
     ctx.set_stream(stream.cuda_stream)
     ctx.load_v2dt2(v2, from_host=True)
+    # the launch shape measured on this context (rtmb_autotune_full), before the warm-up
+    tuning = ctx.autotune_full() if not args.no_autotune else None
     shape = ctx.padded_shape
     with torch.cuda.stream(stream):
         img = torch.zeros(shape, dtype=torch.float32, device=dev)
@@ -540,11 +554,9 @@ def run_b200(args, rank: int, world: int, local_rank: int) -> dict | None:
         "vs_baseline": None,
         "dtype": {"fp32_exact": "f32", "fp32_fma": "f32-fma"}.get(args.form, args.form + "-storage/f32-math"),
         "data": "synthetic (seeded salt model; record from this library's modeling pass)",
-        "config": {"workload": f"rtm_rbc_{args.size}^3_nt{args.nt}", "grid": list(shape), "nt": p["nt"],
-                   "stencil_order": 8, "boundary": "rbc", "shots_per_step_per_gpu": 1,
-                   "form": args.form,
-                   "l2": "inputs larger than L2 (%.0f MB per wavefield)" % (n_points(p) * 4 / 1e6),
-                   "parallelism": f"shot-parallel x{world}"},
+        "config": workload_config(args, p, world),
+        "form": args.form,
+        "tuning": tuning,
         "e2e": {"value": round(e2e_value, 3), "unit": "Gpt/s",
                 "h2d_bytes_per_step": int(np.prod(rec_shape) * 4), "d2h_bytes_per_step": int(np.prod(shape) * 4)},
         "gpu_launches": int(launches),
@@ -992,8 +1004,9 @@ def run_reference_arm(args, rank: int) -> dict | None:
         "value": round(value, 4), "unit": "Gpt/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(1e3 * sum(secs) / len(secs), 1), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded salt model, seeded random record)",
-        "config": {"workload": f"rtm_rbc_{args.size}^3_nt{args.nt}", "nt_sample": nts, "boundary": "rbc",
-                   "stencil_order": 8},
+        "config": workload_config(args, p, 1),
+        "sample": {"nt": nts, "sweeps": 3 * nts - 2, "note": "each step is one run of the reference program on the "
+                                                              "workload with nt cut to the sample"},
         "cpu_baseline": {"value": round(value, 4), "unit": "Gpt/s", "cores": thr, "kind": "reference",
                          "sample": f"RTM3D.bin RBC migration, nt={nts} ({3 * nts - 2} sweeps of {n_points(p)} "
                                    f"points) per step, its own migration timer"},
@@ -1047,6 +1060,8 @@ def main():
     ap.add_argument("--ref-gpu-nt", type=int, default=100,
                     help="steps of the reference GPU program's RBC migration sample")
     ap.add_argument("--no-reference-gpu", action="store_true", help="skip the reference GPU program bar")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch shape instead of measuring it (rtmb_autotune_full) per context")
     ap.add_argument("--c3", dest="c3", action="store_true", default=True,
                     help="add the precision configuration (896 x 896 x 512) to the default line (default)")
     ap.add_argument("--no-c3", dest="c3", action="store_false")
