@@ -461,8 +461,9 @@ def run_b200(args, rank: int, world: int, local_rank: int) -> dict | None:
     sx, sy, sz = shots[k_mine]
     rec_shape = (1, p["receiver_count_x"], p["receiver_count_y"], p["nt"])
 
-    # the shot record: this library's modeling pass on the ABC-bordered model
-    mctx = rtmb.Context(rtmb.Params.from_input(dict(p, boundary_condition="hbc"), flags=flags, device=local_rank))
+    # the shot record: this library's modeling pass (FP32, FMA form) on the ABC-bordered model
+    mctx = rtmb.Context(rtmb.Params.from_input(dict(p, boundary_condition="hbc"), flags=rtmb.FLAG_FAST_FMA,
+                                               device=local_rank))
     mctx.set_stream(stream.cuda_stream)
     with torch.cuda.stream(stream):
         rec = torch.zeros(rec_shape, dtype=torch.float32, device=dev)
