@@ -8,7 +8,9 @@ the GPU forward pass, the gradients and the feature layout:
     y  = w3 . h2 + b3,     loss = mean_i (y_i - r_i)^2
 
 x is the row of 64 BF16 features.  Gradients treat the BF16 roundings as identity (straight-through),
-as the library's backward kernels do.
+as the library's backward kernels do.  The backward pass runs on the tensor cores, whose operands
+are BF16: the pre-activation gradients dz2 and dz1 enter the products dz2 W2, dz1^T x, dz2^T h1 and
+the bias sums rounded to BF16, as restated in grad() below.
 """
 import numpy as np
 
@@ -55,8 +57,8 @@ def grad(p: np.ndarray, X: np.ndarray, R: np.ndarray):
     n = len(y)
     e = y - np.asarray(R, np.float64)
     dy = 2.0 * e / n
-    dz2 = (dy[:, None] * w3[None, :]) * (1.0 - h2 * h2)
-    dz1 = (dz2 @ W2b) * (1.0 - h1 * h1)
+    dz2 = bf16(((dy[:, None] * w3[None, :]) * (1.0 - h2 * h2)).astype(np.float32)).astype(np.float64)
+    dz1 = bf16(((dz2 @ W2b) * (1.0 - h1 * h1)).astype(np.float32)).astype(np.float64)
     x = np.asarray(X, np.float64)
     g = np.zeros(NPARAM)
     g[OFF_W1:OFF_B1] = (dz1.T @ x).ravel()

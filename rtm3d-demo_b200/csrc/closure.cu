@@ -118,9 +118,10 @@ __device__ __forceinline__ bool bar_wait(uint64_t *bar, uint32_t parity) {
 
 // Weights into shared memory (BF16, canonical K-major), biases and w3 in FP32; TMEM allocation and
 // the MMA barrier.  Every thread of the 128-thread CTA calls it.
-__device__ void mlp_setup(MlpSmem &sm, const float *__restrict__ prm) {
+template <class SM, uint32_t NCOLS = kTmemCols>
+__device__ void mlp_setup(SM &sm, const float *__restrict__ prm) {
     const int tid = threadIdx.x;
-    if (tid < 32) umma::tmem_alloc(&sm.tmem, kTmemCols);
+    if (tid < 32) umma::tmem_alloc(&sm.tmem, NCOLS);
     for (int i = tid; i < kHid * kIn; i += kTile) {
         const int r = i / kIn, k = i % kIn;
         *reinterpret_cast<__nv_bfloat16 *>(sm.w1 + umma::kmajor_offset(r, k, kLboB)) =
@@ -159,7 +160,8 @@ __device__ __forceinline__ void put_row(unsigned char *tile, int m, const float 
 // One tile: the caller has written every row of a1.  Returns, for this thread's row, y (the network
 // output) and optionally the hidden activations (h1 rounded to BF16, as layer 2 sees it; h2 FP32).
 // phase: the MMA barrier's next parity, advanced by two.  false: a wait ran out (uniform).
-__device__ bool mlp_tile(MlpSmem &sm, uint32_t &phase, float *y, float *h1_out, float *h2_out) {
+template <class SM>
+__device__ bool mlp_tile(SM &sm, uint32_t &phase, float *y, float *h1_out, float *h2_out) {
     const int tid = threadIdx.x, warp = tid >> 5;
     const uint32_t lane_base = sm.tmem + ((uint32_t)(warp * 32) << 16);
     umma::fence_smem_to_async();
@@ -215,12 +217,13 @@ __device__ bool mlp_tile(MlpSmem &sm, uint32_t &phase, float *y, float *h1_out, 
     return true;
 }
 
-__device__ void mlp_teardown(MlpSmem &sm) {
+template <class SM, uint32_t NCOLS = kTmemCols>
+__device__ void mlp_teardown(SM &sm) {
     umma::fence_before_sync();
     __syncthreads();
     if (threadIdx.x < 32) {
         umma::fence_after_sync();
-        umma::tmem_dealloc(sm.tmem, kTmemCols);
+        umma::tmem_dealloc(sm.tmem, NCOLS);
     }
 }
 
@@ -449,68 +452,194 @@ __global__ void gather_batch_kernel(const __nv_bfloat16 *__restrict__ X, const f
     if (threadIdx.x == 0) Rb[i] = R[src];
 }
 
-// Backward, per row: loss contribution and the pre-activation gradients of both hidden layers.
-// The network as trained: z1 = W1b x + b1, h1 = bf16(tanh z1), z2 = W2b h1 + b2, h2 = tanh z2,
-// y = w3 . h2 + b3 with W1b, W2b the BF16 weights; loss = mean (y - r)^2.  Gradients treat the BF16
-// roundings as identity (straight-through).
-__global__ void backward_rows_kernel(const float *__restrict__ prm, const float *__restrict__ y,
-                                     const float *__restrict__ R, const float *__restrict__ H1,
-                                     const float *__restrict__ H2, int B, float *dZ1, float *dZ2, float *dY,
-                                     float *loss) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    float l = 0.f;
-    if (i < B) {
-        const float e = y[i] - R[i];
-        l = e * e / B;
-        const float dy = 2.f * e / B;
-        dY[i] = dy;
-        float d2[kHid];
-#pragma unroll
-        for (int j = 0; j < kHid; ++j) {
-            const float h = H2[(long long)i * kHid + j];
-            d2[j] = dy * prm[kOffW3 + j] * (1.f - h * h);
-            dZ2[(long long)i * kHid + j] = d2[j];
-        }
-#pragma unroll 4
-        for (int k = 0; k < kHid; ++k) {
-            float a = 0.f;
-#pragma unroll
-            for (int j = 0; j < kHid; ++j)
-                a = fmaf(__bfloat162float(__float2bfloat16_rn(prm[kOffW2 + j * kHid + k])), d2[j], a);
-            const float h = H1[(long long)i * kHid + k];
-            dZ1[(long long)i * kHid + k] = a * (1.f - h * h);
-        }
-    }
-    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
-    if ((threadIdx.x & 31) == 0) atomicAdd(loss, l);
+// ------------------------------------------------------------------ tensor-core training step
+
+// The gradient of one batch on the tensor cores.  Per tile of 128 rows (one row per thread): the
+// forward pass (mlp_tile), then dz2 = dy w3 (1 - h2^2) and the MMA dh1 = dz2 W2 (M 128, N 32,
+// K 32: A = dz2 in BF16, B = W2^T) with dz1 = dh1 (1 - h1^2), then ONE MMA for every weight and
+// bias gradient of the two hidden layers over the tile's rows (M 128, N 64, K 128):
+//     A = [X^T; H1^T; ones; 0]  (rows: 64 features, 32 hidden units, one row of ones, padding)
+//     B = [dZ1^T; dZ2^T]        (rows: 32 + 32 pre-activation gradients)
+// so D[0:64, 0:32] = X^T dZ1 = dW1^T, D[64:96, 32:64] = H1^T dZ2 = dW2^T and the ones row gives
+// db1, db2 (D[96, 0:64]); the other blocks of D are not read.  D accumulates in TMEM over the CTA's
+// tiles.  dw3, db3 and the loss are sums over rows of scalars, reduced per CTA.  Each CTA writes its
+// partial gradient (and loss) to part[blockIdx.x]; grad_sum_kernel adds the CTAs in order, so a
+// gradient is reproducible for a given batch size.  dz1 and dz2 enter the MMAs rounded to BF16
+// (the operand type), the bias gradients included; everything accumulates in FP32.
+constexpr int kGradN = 2 * kHid;                    // B rows of the weight-gradient MMA
+constexpr int kLboGA = (kTile / 8) * 128;           // A: 16 row groups per K chunk
+constexpr int kLboGB = (kGradN / 8) * 128;          // B: 8 row groups per K chunk
+constexpr uint32_t kIdescG = umma::idesc_bf16_f32(kTile, kGradN);
+constexpr uint32_t kTmemColsG = 256;                // [0, 64): forward, [64, 96): dh1, [128, 192): D
+constexpr uint32_t kColDh1 = 64, kColG = 128;
+constexpr int kRowOnes = kIn + kHid;                // the ones row of A (96)
+constexpr int kPartStride = kNParam + 1;            // a CTA's partial gradient and loss
+
+struct __align__(128) GradSmem {
+    unsigned char a1[kTile * kIn * 2];     // features, BF16, K-major
+    unsigned char a2[kTile * kHid * 2];    // hidden layer 1, then dz2 (BF16, K-major)
+    unsigned char w1[kHid * kIn * 2];      // W1 (N = 32 rows, K = 64)
+    unsigned char w2[kHid * kHid * 2];     // W2
+    unsigned char w2t[kHid * kHid * 2];    // W2^T, the backward B operand
+    unsigned char ga[kTile * kTile * 2];   // A of the weight-gradient MMA (M 128, K 128)
+    unsigned char gb[kGradN * kTile * 2];  // B of the weight-gradient MMA (N 64, K 128)
+    float b1[kHid], b2[kHid], w3[kHid], b3;
+    float red[kTile / 32][kHid + 2];       // per-warp sums of dw3, db3 and the loss
+    uint64_t bar;
+    uint32_t tmem;
+    unsigned char pad[16384];              // as in MlpSmem
+};
+
+__device__ __forceinline__ void put_bf16(unsigned char *tile, int r, int m, int lbo, float v) {
+    *reinterpret_cast<__nv_bfloat16 *>(tile + umma::kmajor_offset(r, m, lbo)) = __float2bfloat16_rn(v);
 }
 
-// Parameter gradients: one thread per parameter, summing over the B rows of the batch.
-__global__ void grad_reduce_kernel(const __nv_bfloat16 *__restrict__ Xb, const float *__restrict__ H1,
-                                   const float *__restrict__ H2, const float *__restrict__ dZ1,
-                                   const float *__restrict__ dZ2, const float *__restrict__ dY, int B, float *g) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= kNParam) return;
-    float a = 0.f;
-    if (p < kOffB1) {
-        const int j = p / kIn, k = p % kIn;
-        for (int i = 0; i < B; ++i) a = fmaf(dZ1[(long long)i * kHid + j], __bfloat162float(Xb[(long long)i * kIn + k]), a);
-    } else if (p < kOffW2) {
-        const int j = p - kOffB1;
-        for (int i = 0; i < B; ++i) a += dZ1[(long long)i * kHid + j];
-    } else if (p < kOffB2) {
-        const int j = (p - kOffW2) / kHid, k = (p - kOffW2) % kHid;
-        for (int i = 0; i < B; ++i) a = fmaf(dZ2[(long long)i * kHid + j], H1[(long long)i * kHid + k], a);
-    } else if (p < kOffW3) {
-        const int j = p - kOffB2;
-        for (int i = 0; i < B; ++i) a += dZ2[(long long)i * kHid + j];
-    } else if (p < kOffB3) {
-        const int j = p - kOffW3;
-        for (int i = 0; i < B; ++i) a = fmaf(dY[i], H2[(long long)i * kHid + j], a);
-    } else {
-        for (int i = 0; i < B; ++i) a += dY[i];
+// One K-major MMA chain D (+)= A B^T of nk16 K steps, issued by thread 0, completion awaited by all.
+__device__ __forceinline__ bool mma_chain(uint64_t *bar, uint32_t &phase, uint32_t tmem_d, const unsigned char *A,
+                                          int lbo_a, const unsigned char *B, int lbo_b, uint32_t idesc, int nk16,
+                                          bool accumulate) {
+    umma::fence_smem_to_async();
+    umma::fence_before_sync();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        umma::fence_after_sync();
+        for (int s = 0; s < nk16; ++s)
+            umma::mma_bf16(tmem_d, umma::smem_desc(A + s * 2 * lbo_a, lbo_a, 128),
+                           umma::smem_desc(B + s * 2 * lbo_b, lbo_b, 128), idesc, accumulate || s > 0);
+        umma::commit(bar);
     }
-    g[p] = a;
+    const bool ok = __syncthreads_and(bar_wait(bar, phase & 1));
+    phase ^= 1;
+    umma::fence_after_sync();
+    return ok;
+}
+
+__global__ void __launch_bounds__(kTile) mlp_grad_kernel(const float *__restrict__ prm,
+                                                         const __nv_bfloat16 *__restrict__ X,
+                                                         const float *__restrict__ R, long long n, float *part,
+                                                         unsigned *err) {
+    extern __shared__ __align__(128) unsigned char gsm_raw[];
+    GradSmem &sm = *reinterpret_cast<GradSmem *>(gsm_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // W2^T, and the rows of A the tiles never write: the ones row and the padding
+    for (int i = tid; i < kHid * kHid; i += kTile) {
+        const int r = i / kHid, k = i % kHid;  // W2^T[r][k] = W2[k][r]
+        put_bf16(sm.w2t, r, k, (kHid / 8) * 128, prm[kOffW2 + k * kHid + r]);
+    }
+    for (int i = tid; i < (kTile - kRowOnes) * kTile; i += kTile) {
+        const int r = kRowOnes + i / kTile, m = i % kTile;
+        put_bf16(sm.ga, r, m, kLboGA, r == kRowOnes ? 1.f : 0.f);
+    }
+    mlp_setup<GradSmem, kTmemColsG>(sm, prm);
+    const uint32_t lane_base = sm.tmem + ((uint32_t)(warp * 32) << 16);
+    const float inv_n = 1.f / (float)n;
+    float dw3[kHid], db3 = 0.f, lsum = 0.f;
+#pragma unroll
+    for (int j = 0; j < kHid; ++j) dw3[j] = 0.f;
+    uint32_t phase = 0;
+    int done = 0;
+    bool ok = true;
+    const long long ntiles = (n + kTile - 1) / kTile;
+    for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        const long long row = t * kTile + tid;
+        const bool valid = row < n;
+        {
+            float f[kIn];
+            if (valid) {
+                const uint4 *src = reinterpret_cast<const uint4 *>(X + row * kIn);
+#pragma unroll
+                for (int c = 0; c < kIn / 8; ++c) {
+                    const uint4 u = __ldg(src + c);
+                    const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&u);
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const float2 v = __bfloat1622float2(h[j]);
+                        f[8 * c + 2 * j] = v.x;
+                        f[8 * c + 2 * j + 1] = v.y;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < kIn; ++k) f[k] = 0.f;
+            }
+            put_row(sm.a1, tid, f, kIn, kLboA);
+#pragma unroll
+            for (int k = 0; k < kIn; ++k) put_bf16(sm.ga, k, tid, kLboGA, f[k]);  // X^T
+        }
+        float y, h1[kHid], h2[kHid];
+        if (!(ok = mlp_tile(sm, phase, &y, h1, h2))) break;
+        const float e = valid ? y - R[row] : 0.f;
+        const float dy = 2.f * e * inv_n;
+        lsum += e * e * inv_n;
+        db3 += dy;
+        float dz[kHid];
+#pragma unroll
+        for (int j = 0; j < kHid; ++j) {
+            dz[j] = dy * sm.w3[j] * (1.f - h2[j] * h2[j]);
+            dw3[j] = fmaf(dy, h2[j], dw3[j]);
+            put_bf16(sm.gb, kHid + j, tid, kLboGB, dz[j]);  // dZ2^T
+            put_bf16(sm.ga, kIn + j, tid, kLboGA, h1[j]);    // H1^T (h1 holds BF16 values)
+        }
+        put_row(sm.a2, tid, dz, kHid, kLboA);  // the layer-2 MMA has completed (mlp_tile waited)
+        // dh1 = dz2 W2
+        if (!(ok = mma_chain(&sm.bar, phase, sm.tmem + kColDh1, sm.a2, kLboA, sm.w2t, (kHid / 8) * 128, kIdesc,
+                             kHid / 16, false)))
+            break;
+        umma::tmem_ld32(lane_base + kColDh1, dz);
+#pragma unroll
+        for (int k = 0; k < kHid; ++k) put_bf16(sm.gb, k, tid, kLboGB, dz[k] * (1.f - h1[k] * h1[k]));  // dZ1^T
+        // every weight and bias gradient of the hidden layers, accumulated over the tiles
+        if (!(ok = mma_chain(&sm.bar, phase, sm.tmem + kColG, sm.ga, kLboGA, sm.gb, kLboGB, kIdescG, kTile / 16,
+                             done > 0)))
+            break;
+        ++done;
+    }
+    if (!ok) {
+        if (tid == 0 && err) atomicOr(err, 2u);
+    } else if (done > 0) {
+        float *out = part + (size_t)blockIdx.x * kPartStride;
+        float g[32];
+        umma::tmem_ld32(lane_base + kColG, g);  // D row tid, columns 0 .. 31 (the dZ1 block)
+        if (tid < kIn) {
+#pragma unroll
+            for (int i = 0; i < kHid; ++i) out[kOffW1 + i * kIn + tid] = g[i];   // dW1[i][tid]
+        } else if (tid == kRowOnes) {
+#pragma unroll
+            for (int i = 0; i < kHid; ++i) out[kOffB1 + i] = g[i];
+        }
+        umma::tmem_ld32(lane_base + kColG + kHid, g);  // columns 32 .. 63 (the dZ2 block)
+        if (tid >= kIn && tid < kRowOnes) {
+#pragma unroll
+            for (int i = 0; i < kHid; ++i) out[kOffW2 + i * kHid + (tid - kIn)] = g[i];  // dW2[i][tid - 64]
+        } else if (tid == kRowOnes) {
+#pragma unroll
+            for (int i = 0; i < kHid; ++i) out[kOffB2 + i] = g[i];
+        }
+        // dw3, db3 and the loss: warp sums, then the warps in order
+#pragma unroll
+        for (int j = 0; j < kHid + 2; ++j) {
+            float v = j < kHid ? dw3[j] : (j == kHid ? db3 : lsum);
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) sm.red[warp][j] = v;
+        }
+        __syncthreads();
+        if (tid < kHid + 2) {
+            float v = 0.f;
+            for (int w = 0; w < kTile / 32; ++w) v += sm.red[w][tid];
+            out[tid < kHid ? kOffW3 + tid : (tid == kHid ? kOffB3 : kNParam)] = v;
+        }
+    }
+    mlp_teardown<GradSmem, kTmemColsG>(sm);
+}
+
+// g[p] = sum over the CTAs' partials, in CTA order; the loss (index kNParam) into *loss.
+__global__ void grad_sum_kernel(const float *__restrict__ part, int nparts, float *g, float *loss) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p > kNParam) return;
+    float a = 0.f;
+    for (int c = 0; c < nparts; ++c) a += part[(size_t)c * kPartStride + p];
+    if (p < kNParam) g[p] = a;
+    else if (loss) *loss = a;
 }
 
 // Adam (beta1 0.9, beta2 0.999, eps 1e-8) with bias correction; step counts from 1.
@@ -524,6 +653,22 @@ __global__ void adam_kernel(float *prm, const float *__restrict__ g, float *m, f
     v[p] = vv;
     const float mh = mm / (1.f - powf(b1, (float)step)), vh = vv / (1.f - powf(b2, (float)step));
     prm[p] -= lr * mh / (sqrtf(vh) + 1e-8f);
+}
+
+// Grid of mlp_grad_kernel (one CTA per tile up to two per SM; its dynamic shared memory opted in
+// once per device), or 0 when the attribute cannot be set.
+int grad_grid(long long tiles) {
+    static unsigned long long done = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(done & bit)) {
+        if (cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(GradSmem)) !=
+            cudaSuccess)
+            return 0;
+        done |= bit;
+    }
+    return (int)(tiles < 2 * 148 ? tiles : 2 * 148);
 }
 
 int grid_for(long long tiles) {
@@ -651,22 +796,18 @@ int rtmb_closure_grad(const float *params, const void *X, const float *R, uint32
                       void *stream) {
     if (!params || !X || !R || !grad || !loss || !n) return cfail(RTMB_EINVAL, "rtmb_closure_grad: bad argument");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    float *buf = nullptr;
-    const size_t nb = (size_t)n * (1 + 4 * kHid + 1);
-    CKC(cudaMallocAsync(&buf, nb * sizeof(float) + 16, s));
-    float *y = buf, *H1 = y + n, *H2 = H1 + (size_t)n * kHid, *dZ1 = H2 + (size_t)n * kHid,
-          *dZ2 = dZ1 + (size_t)n * kHid, *dY = dZ2 + (size_t)n * kHid;
-    unsigned *err = reinterpret_cast<unsigned *>(buf + nb);
-    CKC(cudaMemsetAsync(err, 0, sizeof(unsigned), s));
-    CKC(cudaMemsetAsync(loss, 0, sizeof(float), s));
-    const auto *Xb = static_cast<const __nv_bfloat16 *>(X);
     const long long tiles = ((long long)n + kTile - 1) / kTile;
-    mlp_forward_kernel<<<grid_for(tiles), kTile, 0, s>>>(params, Xb, n, y, H1, H2, err);
-    backward_rows_kernel<<<(n + 127) / 128, 128, 0, s>>>(params, y, R, H1, H2, (int)n, dZ1, dZ2, dY, loss);
-    grad_reduce_kernel<<<(kNParam + 127) / 128, 128, 0, s>>>(Xb, H1, H2, dZ1, dZ2, dY, (int)n, grad);
+    const int grid = grad_grid(tiles);
+    if (grid <= 0) return cfail(RTMB_ECUDA, "rtmb_closure_grad: kernel set-up failed");
+    float *part = nullptr;
+    CKC(cudaMallocAsync(&part, ((size_t)grid * kPartStride + 4) * sizeof(float), s));
+    unsigned *err = reinterpret_cast<unsigned *>(part + (size_t)grid * kPartStride);
+    CKC(cudaMemsetAsync(part, 0, ((size_t)grid * kPartStride + 4) * sizeof(float), s));
+    mlp_grad_kernel<<<grid, kTile, sizeof(GradSmem), s>>>(params, static_cast<const __nv_bfloat16 *>(X), R, n, part, err);
+    grad_sum_kernel<<<(kNParam + 1 + 127) / 128, 128, 0, s>>>(part, grid, grad, loss);
     CKC(cudaGetLastError());
     const int rc = read_err(err, s);
-    cudaFreeAsync(buf, s);
+    cudaFreeAsync(part, s);
     return rc;
 }
 
@@ -675,25 +816,25 @@ int rtmb_closure_train(float *params, const void *X, const float *R, uint64_t n,
     if (!params || !X || !R || !n || !batch || batch > 65536) return cfail(RTMB_EINVAL, "rtmb_closure_train: bad argument");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const size_t B = batch;
-    const size_t nf = 3 * kNParam + B * (2 + 4 * kHid + 1) + steps + 4;
+    const long long tiles = ((long long)B + kTile - 1) / kTile;
+    const int grid = grad_grid(tiles);
+    if (grid <= 0) return cfail(RTMB_ECUDA, "rtmb_closure_train: kernel set-up failed");
+    const size_t nf = 3 * kNParam + B + (size_t)grid * kPartStride + steps + 4;
     float *buf = nullptr;
     __nv_bfloat16 *Xb = nullptr;
     CKC(cudaMallocAsync(&buf, nf * sizeof(float), s));
     CKC(cudaMallocAsync(&Xb, B * kIn * sizeof(__nv_bfloat16), s));
     CKC(cudaMemsetAsync(buf, 0, nf * sizeof(float), s));
-    float *g = buf, *m = g + kNParam, *v = m + kNParam, *Rb = v + kNParam, *y = Rb + B, *H1 = y + B,
-          *H2 = H1 + B * kHid, *dZ1 = H2 + B * kHid, *dZ2 = dZ1 + B * kHid, *dY = dZ2 + B * kHid, *losses = dY + B;
+    float *g = buf, *m = g + kNParam, *v = m + kNParam, *Rb = v + kNParam, *part = Rb + B,
+          *losses = part + (size_t)grid * kPartStride;
     unsigned *err = reinterpret_cast<unsigned *>(losses + steps);
     const auto *Xd = static_cast<const __nv_bfloat16 *>(X);
-    const long long tiles = ((long long)B + kTile - 1) / kTile;
-    const int fgrid = grid_for(tiles);
     for (uint32_t st = 0; st < steps; ++st) {
         gather_batch_kernel<<<(unsigned)B, 32, 0, s>>>(Xd, R, (long long)n, (int)B, mix64(seed * 1000003ull + st), noise,
                                                        Xb, Rb);
-        mlp_forward_kernel<<<fgrid, kTile, 0, s>>>(params, Xb, (long long)B, y, H1, H2, err);
-        backward_rows_kernel<<<(unsigned)((B + 127) / 128), 128, 0, s>>>(params, y, Rb, H1, H2, (int)B, dZ1, dZ2, dY,
-                                                                       losses + st);
-        grad_reduce_kernel<<<(kNParam + 127) / 128, 128, 0, s>>>(Xb, H1, H2, dZ1, dZ2, dY, (int)B, g);
+        // forward, backward and every weight gradient on the tensor cores, then the CTAs' sums
+        mlp_grad_kernel<<<grid, kTile, sizeof(GradSmem), s>>>(params, Xb, Rb, (long long)B, part, err);
+        grad_sum_kernel<<<(kNParam + 1 + 127) / 128, 128, 0, s>>>(part, grid, g, losses + st);
         adam_kernel<<<(kNParam + 127) / 128, 128, 0, s>>>(params, g, m, v, (int)st + 1, lr);
         CKC(cudaGetLastError());
     }
