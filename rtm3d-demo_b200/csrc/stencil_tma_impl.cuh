@@ -29,8 +29,6 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
-#include <type_traits>
-
 #include "stencil_common.cuh"
 
 namespace rtmb {
@@ -244,24 +242,11 @@ struct TmaShape {
     static constexpr int OFF_PS = OFF_V + CORE * 4;
     static constexpr int OFF_IMG = OFF_PS + CORE * (int)sizeof(T);
     static constexpr int CSLOT = IMG ? OFF_IMG + CORE * (int)sizeof(IT) : OFF_PS;
-    // 16-bit storage with the FP64 image: a shallower core ring and W ring keep two CTAs per SM
-    static constexpr bool WIDE_IMG64 = sizeof(T) == 2 && IMG && sizeof(IT) == 8;
     static constexpr int D = H + (IMG ? Variant<V>::DX_IMG : Variant<V>::DX);  // P slots
-    static constexpr int R = IMG ? (WIDE_IMG64 ? 2 : Variant<V>::R_IMG) : Variant<V>::R;  // core slots
+    static constexpr int R = IMG ? Variant<V>::R_IMG : Variant<V>::R;           // core slots
     static_assert(2 * H <= D && D >= H + 2, "warm-up planes and the lookahead must fit in the P ring");
     static constexpr size_t PRING_BYTES = (size_t)D * STRIDE * sizeof(T);
-    // 16-bit forms: the W ring holds FP32 copies of the P tiles the stencil reads its y and z taps
-    // from (each value widened once, by one thread, instead of at every tap that reads it): WS slots
-    // of SROWS x WPITCH floats with a z halo of WZH columns
-    static constexpr bool WIDE = sizeof(T) == 2;
-    static constexpr int WZH = ((H + 3) / 4) * 4;
-    static constexpr int WPITCH = TZ + 2 * WZH;
-    static constexpr int WSTAGE = SROWS * WPITCH;
-    static constexpr int WS = WIDE ? (WIDE_IMG64 ? H + 1 : H + 2) : 0;  // >= H + 1: never the centre's slot
-    static constexpr size_t WOFF = PRING_BYTES + (size_t)R * CSLOT;
-    static constexpr size_t WBYTES = (size_t)WS * WSTAGE * sizeof(float);
-    static constexpr size_t BAR_OFF = WOFF + WBYTES;
-    static constexpr size_t SMEM = BAR_OFF + 2 * (D + R + WS) * sizeof(uint64_t);
+    static constexpr size_t SMEM = PRING_BYTES + (size_t)R * CSLOT + 2 * (D + R) * sizeof(uint64_t);
     // batched launches: one shot's StepArgs copied past the rings
     static constexpr size_t ARGS_OFF = (SMEM + 15) / 16 * 16;
     static constexpr size_t SMEM_BATCH = ARGS_OFF + sizeof(StepArgs);
@@ -355,19 +340,11 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
     extern __shared__ __align__(128) unsigned char smem[];
     T *pring = reinterpret_cast<T *>(smem);
     unsigned char *cring = smem + S::PRING_BYTES;
-    uint64_t *pfull = reinterpret_cast<uint64_t *>(smem + S::BAR_OFF);
+    uint64_t *pfull = reinterpret_cast<uint64_t *>(cring + R * CSLOT);
     uint64_t *cfull = pfull + D;
     uint64_t *pempty = cfull + R;
     uint64_t *cempty = pempty + D;
-    uint64_t *wfull = cempty + R;  // 16-bit forms: the W ring's barriers
-    uint64_t *wempty = wfull + S::WS;
     constexpr int NCW = kThreads / 32;  // consumer warps
-    // W1: the y and z taps come from the FP32 W ring (16-bit forms); otherwise from the P ring
-    constexpr bool W1 = S::WIDE;
-    constexpr int WS = S::WS, WPITCH = S::WPITCH, WZH = S::WZH, WSTAGE = S::WSTAGE;
-    float *wring = reinterpret_cast<float *>(smem + S::WOFF);
-    using TT = typename std::conditional<W1, float, T>::type;  // element type of the tap tile
-    constexpr int TZH = W1 ? WZH : ZH, TPITCH = W1 ? WPITCH : SPITCH;
 
     const int tid = threadIdx.x;
     const int tz = tid % ZQ, ty = tid / ZQ;
@@ -403,7 +380,6 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
     if (tid == 0) {
         for (int s = 0; s < D; ++s) { mbar_init(&pfull[s], 1); mbar_init(&pempty[s], NCW); }
         for (int s = 0; s < R; ++s) { mbar_init(&cfull[s], 1); mbar_init(&cempty[s], NCW); }
-        for (int s = 0; s < WS; ++s) { mbar_init(&wfull[s], NCW); mbar_init(&wempty[s], NCW); }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();  // the last block-wide barrier: the producer warp leaves below
@@ -535,37 +511,6 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
     auto taper_stage = [&](int k, int slot) {
         taper_tile<H, TAPER, IMG, T, IT>(pring + slot * STRIDE, tab, a, xc0 - H + k, yt0, zt0, tid);
     };
-    // W1: the FP32 copy of the P tile in slot pslot into W slot wslot.  own: this thread's four
-    // centre-row values, widened already for the x queue; the y halo rows (own columns) and the
-    // centre rows' z halo are widened here, a float4 group per thread
-    auto widen_tile = [&](int pslot, int wslot, const float4 &own) {
-        float *wd = wring + wslot * WSTAGE;
-        *reinterpret_cast<float4 *>(wd + (ty + H) * WPITCH + WZH + tz * kVZ) = own;
-        const T *src = pring + pslot * STRIDE;
-        constexpr int GI = kTZ / 4;            // interior column groups of a row
-        constexpr int GZ = WZH / 4;            // z-halo groups on each side
-        constexpr int NHY = 2 * H * GI;        // y halo rows, interior columns
-        constexpr int NHZ = kTY * 2 * GZ;      // z halo of the centre rows
-        for (int g = tid; g < NHY + NHZ; g += kThreads) {
-            int r, c4;
-            if (g < NHY) {
-                const int rr = g / GI;
-                r = rr < H ? rr : rr + kTY;
-                c4 = GZ + (g - rr * GI);
-            } else {
-                const int h = g - NHY, rr = h / (2 * GZ), cc = h - rr * (2 * GZ);
-                r = H + rr;
-                c4 = cc < GZ ? cc : GI + cc;
-            }
-            const float4 v = ST::ld4(src + r * SPITCH + 4 * c4 + (ZH - WZH));
-            *reinterpret_cast<float4 *>(wd + r * WPITCH + 4 * c4) = v;
-        }
-    };
-    auto ldt = [&](const TT *ptr) -> float4 {
-        if constexpr (W1) return ld_f4(ptr);
-        else return ST::ld4(ptr);
-    };
-    const int tcol = TZH + tz * kVZ;
 
     float4 q[NQ];
     float nanacc = 0.f;  // stays 0 unless a NaN or an infinity is written
@@ -577,7 +522,7 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
     // isotropic grids (dx = dy = dz) in the FP32 FMA form: packed pairs over the symmetric stencil
     // (14% fewer instructions; for the 16-bit forms the packing of the widened taps cost more than
     // it saved, measured 4% slower, so they keep the scalar chains)
-    const bool iso = !EXACT && (!SC || W1) && a.iso;
+    const bool iso = !EXACT && !SC && a.iso;
     f32x2 cpk[H + 1];
     cpk[0] = pk2(coef.cx[H] + coef.cy[H] + coef.cz[H], coef.cx[H] + coef.cy[H] + coef.cz[H]);
 #pragma unroll
@@ -590,13 +535,6 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
     if (CB ? consumer_sync_or<kThreads>(bad_wait) : bad_wait) goto drain;
 #pragma unroll
     for (int k = 0; k < 2 * H; ++k) q[k + 1] = ST::ld4(pring + k * STRIDE + (ty + H) * SPITCH + col);
-    if constexpr (W1) {  // planes H .. 2H-1 are the first centre planes: W planes 0 .. H-1
-#pragma unroll
-        for (int k = H; k < 2 * H; ++k) widen_tile(k, k - H, q[k + 1]);
-        __syncwarp();
-        if (lane == 0)
-            for (int w = 0; w < H; ++w) mbar_arrive(&wfull[w]);
-    }
 #pragma unroll
     for (int k = 0; k < H; ++k) release_p(k);  // planes 0 .. H-1 were only needed for the queue
 
@@ -622,6 +560,7 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                 }
             }
             wait_p(s_in, ph_in);
+            const T *s = pring + s_mid * STRIDE;  // the centre plane's tile
             if constexpr (CB) {
                 if (plane_needs_taper(kin)) {  // the pass is collective: all warps take this branch
                     taper_stage(kin, s_in);
@@ -633,31 +572,14 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
 #pragma unroll
             for (int k = 0; k < NQ - 1; ++k) q[k] = q[k + 1];  // advance the x queue
             q[NQ - 1] = ST::ld4(pring + s_in * STRIDE + (ty + H) * SPITCH + col);
-            const TT *s = reinterpret_cast<const TT *>(pring + s_mid * STRIDE);  // the centre plane's taps
-            int ws_c = 0;
-            if constexpr (W1) {
-                // W plane i + H (P plane kin) into its slot once every warp has read that slot's
-                // previous plane (i + H - WS, the centre of iteration i + H - WS); then the centre
-                // plane's W tile (W plane i)
-                const int wi = i + H, wsl = wi % WS;
-                if (wi >= WS && !(CB && bad_wait))
-                    bad_wait |= !__all_sync(0xffffffffu, mbar_wait(&wempty[wsl], ((wi / WS) + 1) & 1));
-                widen_tile(s_in, wsl, q[NQ - 1]);
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&wfull[wsl]);
-                ws_c = i % WS;
-                if (!(CB && bad_wait)) bad_wait |= !__all_sync(0xffffffffu, mbar_wait(&wfull[ws_c], (i / WS) & 1));
-                if (!CB && bad_wait) goto drain;
-                s = reinterpret_cast<const TT *>(wring + ws_c * WSTAGE);
-            }
 
             float lap[kVZ] = {0.f, 0.f, 0.f, 0.f};
             if (row_ok) {
-                float zr[kVZ + 2 * TZH];
+                float zr[kVZ + 2 * ZH];
 #pragma unroll
-                for (int k = 0; k < (kVZ + 2 * TZH) / 4; ++k) {
+                for (int k = 0; k < (kVZ + 2 * ZH) / 4; ++k) {
                     const float4 t4 =
-                        (k == TZH / 4) ? q[H] : ldt(s + (ty + H) * TPITCH + tcol - TZH + 4 * k);
+                        (k == ZH / 4) ? q[H] : ST::ld4(s + (ty + H) * SPITCH + col - ZH + 4 * k);
                     zr[4 * k + 0] = t4.x; zr[4 * k + 1] = t4.y; zr[4 * k + 2] = t4.z; zr[4 * k + 3] = t4.w;
                 }
                 if (EXACT) {
@@ -667,12 +589,12 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
 #pragma unroll
                     for (int io = 0; io < NQ; ++io) {
                         const float4 qx = q[io];
-                        const float4 ry = (io == H) ? q[H] : ldt(s + (ty + io) * TPITCH + tcol);
+                        const float4 ry = (io == H) ? q[H] : ST::ld4(s + (ty + io) * SPITCH + col);
 #pragma unroll
                         for (int e = 0; e < kVZ; ++e) {
                             ax[e] = ax[e] + get(qx, e) * coef.cx[io];
                             ay[e] = ay[e] + get(ry, e) * coef.cy[io];
-                            az[e] = az[e] + zr[TZH - H + e + io] * coef.cz[io];
+                            az[e] = az[e] + zr[ZH - H + e + io] * coef.cz[io];
                         }
                     }
 #pragma unroll
@@ -686,12 +608,12 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
 #pragma unroll
                     for (int k = 1; k <= H; ++k) {
                         const float4 xa = q[H + k], xb = q[H - k];
-                        const float4 ya = ldt(s + (ty + H + k) * TPITCH + tcol);
-                        const float4 yb = ldt(s + (ty + H - k) * TPITCH + tcol);
+                        const float4 ya = ST::ld4(s + (ty + H + k) * SPITCH + col);
+                        const float4 yb = ST::ld4(s + (ty + H - k) * SPITCH + col);
                         const f32x2 t0 = add2(add2(add2(pk2(xa.x, xa.y), pk2(xb.x, xb.y)), add2(pk2(ya.x, ya.y), pk2(yb.x, yb.y))),
-                                              add2(pk2(zr[TZH + k], zr[TZH + k + 1]), pk2(zr[TZH - k], zr[TZH - k + 1])));
+                                              add2(pk2(zr[ZH + k], zr[ZH + k + 1]), pk2(zr[ZH - k], zr[ZH - k + 1])));
                         const f32x2 t1 = add2(add2(add2(pk2(xa.z, xa.w), pk2(xb.z, xb.w)), add2(pk2(ya.z, ya.w), pk2(yb.z, yb.w))),
-                                              add2(pk2(zr[TZH + 2 + k], zr[TZH + 3 + k]), pk2(zr[TZH + 2 - k], zr[TZH + 3 - k])));
+                                              add2(pk2(zr[ZH + 2 + k], zr[ZH + 3 + k]), pk2(zr[ZH + 2 - k], zr[ZH + 3 - k])));
                         l0 = fma2(t0, cpk[k], l0);
                         l1 = fma2(t1, cpk[k], l1);
                     }
@@ -706,20 +628,17 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
                     for (int io = 0; io < NQ; ++io) {
                         if (io == H) continue;
                         const float4 qx = q[io];
-                        const float4 ry = ldt(s + (ty + io) * TPITCH + tcol);
+                        const float4 ry = ST::ld4(s + (ty + io) * SPITCH + col);
 #pragma unroll
                         for (int e = 0; e < kVZ; ++e) {
                             lap[e] = fmaf(get(qx, e), coef.cx[io], lap[e]);
                             lap[e] = fmaf(get(ry, e), coef.cy[io], lap[e]);
-                            lap[e] = fmaf(zr[TZH - H + e + io], coef.cz[io], lap[e]);
+                            lap[e] = fmaf(zr[ZH - H + e + io], coef.cz[io], lap[e]);
                         }
                     }
                 }
             }
             release_p(s_mid);  // the tile of plane x is no longer read
-            if constexpr (W1) {
-                if (lane == 0) mbar_arrive(&wempty[ws_c]);  // nor its FP32 copy (release_p synced the warp)
-            }
             // core tiles of plane x
             const int cs = s_core;
             if (CB && bad_wait) continue;  // run on to the next barrier (see wait_p)
