@@ -1,0 +1,78 @@
+"""Properties of the benchmark's RBC migration at its full grid size, where the CPU oracle cannot run.
+
+The workload's grid: a 512^3 model at 10 m with a 40-cell random border (592^3 padded), the seeded
+salt velocity, a 12 Hz Ricker at the surface centre and receivers every 2 cells over the surface;
+nt is cut to 600 steps to keep the test short (every step runs the same kernels as the 3000-step
+shot).  The record is this library's FP32 modeling pass of the same shot.
+
+* Linearity: the migration is linear in the record, and scaling every record value by a power of
+  two scales every intermediate value of the exact form (each product and sum rounds the same way
+  scaled), so migrate(2 rec) == 2 migrate(rec) and migrate(rec / 4) == migrate(rec) / 4 -- exactly,
+  except where values fall into the subnormal range (below 1.2e-38: the numerical tail of the
+  stencil ahead of each wavefront), whose fixed spacing does not scale; a rounding changed there
+  can reach only values within a few hundred ULPs of that range.  The test requires every image
+  value above 1e-20 in magnitude to match bit for bit and the rest to agree within 1e-24.
+* The FMA form stays within the image tolerance of the FP32 path (rel-L2 1e-4) against the exact
+  form, which is the reference CPU path's arithmetic.
+* The 16-bit increment storage form stays within rel-L2 1e-3 of the exact form.
+"""
+import numpy as np
+import pytest
+
+import rtmb
+from rtm_cases import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+N, NT = 512, 600
+
+
+@pytest.fixture(scope="module")
+def shot(cuda):
+    import torch
+    import bench
+    p = bench.workload(N, NT)
+    v = bench.salt_model(N)
+    v2 = rtmb.v2dt2(rtmb.prepare_velocity(v, p["blen"], "rbc", seed=1234), p["dt"])
+    v2m = rtmb.v2dt2(rtmb.prepare_velocity(v, p["blen"], "abc"), p["dt"])
+    m = rtmb.Context(rtmb.Params.from_input(dict(p, boundary_condition="hbc"), flags=rtmb.FLAG_FAST_FMA, device=0))
+    m.load_v2dt2(v2m, from_host=True)
+    rec = torch.zeros((1, p["receiver_count_x"], p["receiver_count_y"], NT), device=cuda)
+    m.model_shot(p["sx"], p["sy"], p["sz"], rec)
+    m.sync()
+    m.close()
+    return p, v2, rec
+
+
+def _migrate(p, v2, rec, flags, cuda):
+    import torch
+    ctx = rtmb.Context(rtmb.Params.from_input(p, flags=flags, device=0))
+    ctx.load_v2dt2(v2, from_host=True)
+    img = torch.zeros(ctx.padded_shape, device=cuda)
+    ctx.migrate_shot(p["sx"], p["sy"], p["sz"], rec, img)
+    ctx.sync()
+    ctx.close()
+    return img
+
+
+def test_exact_form_is_linear_in_the_record(cuda, shot):
+    p, v2, rec = shot
+    img = _migrate(p, v2, rec, 0, cuda)
+    assert float(img.abs().max()) > 0
+    for scale in (2.0, 0.25):
+        got = _migrate(p, v2, rec * scale, 0, cuda)
+        want = img * scale
+        big = want.abs() > 1e-20
+        assert bool((got[big] == want[big]).all()), f"scale {scale}: {int((got[big] != want[big]).sum())} cells differ"
+        assert float((got - want).abs().max()) <= 1e-24
+
+
+def test_fma_and_increment_forms_against_the_exact_form(cuda, shot):
+    p, v2, rec = shot
+    exact = _migrate(p, v2, rec, 0, cuda).cpu().numpy()
+    fma = _migrate(p, v2, rec, rtmb.FLAG_FAST_FMA, cuda).cpu().numpy()
+    inc = _migrate(p, v2, rec, rtmb.FLAG_STORE_F16 | rtmb.FLAG_STORE_DIFF, cuda).cpu().numpy()
+    e_fma, e_inc = rel_l2(fma, exact), rel_l2(inc, exact)
+    print(f"image rel-L2 vs exact at 592^3, nt {NT}: fma {e_fma:.3e}, fp16 increment {e_inc:.3e}")
+    assert e_fma <= 1e-4, e_fma
+    assert e_inc <= 1e-3, e_inc
