@@ -265,7 +265,7 @@ def build_inputs(p: dict, with_abc: bool):
 
 
 FORMS = ("fp32_exact", "fp32_fma", "fp16", "bf16", "fp16_diff", "bf16_diff")
-C3_FORMS = FORMS
+C3_FORMS = ("fp32_exact", "fp32_fma", "fp16", "bf16", "fp16_diff")
 ALL_FORMS = FORMS + ("fp16_img64", "bf16_img64", "fp16_diff_img64", "bf16_diff_img64")
 
 
