@@ -913,15 +913,18 @@ int migrate_impl(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const flo
             rcv.ps = nullptr;
             set_receivers(rcv, ctx, rmode, const_cast<float *>(rec), it);
             rcv.chunk = ctx->dual_chunk;
+            rcv.variant = ctx->dual_variant;
             if (rtmb::dual_step_supported(src, rcv, (int)p.stencil_order)) {
                 LAUNCH_CAT(RTMB_PROF_BACKWARD_DUAL,
                            rtmb::launch_dual_step(src, rcv, (int)p.stencil_order, exact(ctx), ctx->stream));
                 rcv.chunk = ctx->chunk;
+                rcv.variant = ctx->variant;
                 std::swap(s_cur, s_prev);
                 std::swap(rP, rPP);
                 continue;
             }
             rcv.chunk = ctx->chunk;
+            rcv.variant = ctx->variant;
         }
         if (it == (int)p.nt - 2) {
             s_cur = sP;
@@ -1563,22 +1566,27 @@ int rtmb_autotune_full(rtmb_ctx *ctx, rtmb_tuning *out) {
     const bool dual_ok = !rc && !st && !exact(ctx) && order == 8 && tma_ok(ctx) && !(p.flags & RTMB_FLAG_NO_DUAL) &&
                          p.nx > 1 && p.boundary == RTMB_BC_RBC;
     float best_dual = 1e30f;
-    int best_dc = ctx->dual_chunk;
-    for (int c : cand) {
-        if (!dual_ok || rc || c > nxi) break;
-        rtmb::StepArgs src = args(false), rcv = args(true);
-        src.P = ctx->d_w[0]; src.PP = ctx->d_w[1];
-        rcv.P = ctx->d_w[2]; rcv.PP = ctx->d_w[3]; rcv.ps = nullptr;
-        rcv.chunk = c;
-        if (!rtmb::dual_step_supported(src, rcv, order)) break;
-        float t = 0.f;
-        if ((rc = time_launches(ctx, e0, e1, [&] { return rtmb::launch_dual_step(src, rcv, order, false, ctx->stream); }, &t)))
-            break;
-        if (t < best_dual) { best_dual = t; best_dc = c; }
+    int best_dc = ctx->dual_chunk, best_dv = ctx->dual_variant;
+    for (int dv = 0; dv < 2 && dual_ok && !rc; ++dv) {
+        for (int c : cand) {
+            if (rc || c > nxi) break;
+            rtmb::StepArgs src = args(false), rcv = args(true);
+            src.P = ctx->d_w[0]; src.PP = ctx->d_w[1];
+            rcv.P = ctx->d_w[2]; rcv.PP = ctx->d_w[3]; rcv.ps = nullptr;
+            rcv.chunk = c;
+            rcv.variant = dv;
+            if (!rtmb::dual_step_supported(src, rcv, order)) break;
+            float t = 0.f;
+            if ((rc = time_launches(ctx, e0, e1, [&] { return rtmb::launch_dual_step(src, rcv, order, false, ctx->stream); },
+                                    &t)))
+                break;
+            if (t < best_dual) { best_dual = t; best_dc = c; best_dv = dv; }
+        }
     }
     release();
     if (rc) return rc;
     ctx->dual_chunk = best_dc;
+    ctx->dual_variant = best_dv;
     ctx->use_dual = dual_ok ? (best_dual < two ? 1 : 0) : -1;
     if (out) {
         out->variant = (uint32_t)ctx->variant;
@@ -1587,14 +1595,17 @@ int rtmb_autotune_full(rtmb_ctx *ctx, rtmb_tuning *out) {
         out->dual_chunk = (uint32_t)ctx->dual_chunk;
         out->ms_step = best_fwd;
         out->ms_backward = ctx->use_dual == 1 ? best_dual : two;
+        out->dual_variant = (uint32_t)ctx->dual_variant;
     }
     return check_err_flag(ctx);
 }
 
 int rtmb_set_tuning(rtmb_ctx *ctx, const rtmb_tuning *t) {
-    if (!ctx || !t || !t->chunk || !t->dual_chunk || t->variant >= (uint32_t)rtmb::kStepVariants)
+    if (!ctx || !t || !t->chunk || !t->dual_chunk || t->variant >= (uint32_t)rtmb::kStepVariants ||
+        t->dual_variant >= 2u)
         return fail(ctx, RTMB_EINVAL, "rtmb_set_tuning: bad tuning");
     ctx->variant = (int)t->variant;
+    ctx->dual_variant = (int)t->dual_variant;
     ctx->chunk = (int)t->chunk;
     ctx->dual_chunk = (int)t->dual_chunk;
     ctx->use_dual = t->dual ? 1 : 0;

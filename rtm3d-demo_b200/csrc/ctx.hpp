@@ -29,6 +29,7 @@ struct rtmb_ctx {
     int dual_chunk = 0;  // x planes per CTA of the dual-wavefield backward step (64 x 8 tiles)
     int variant = 0;     // launch variant of the TMA step kernel (rtmb_autotune_full)
     int use_dual = -1;   // -1: the default rule; 0 / 1: the autotuner's choice
+    int dual_variant = 0;  // launch variant (tile) of the dual backward step
     int batch_group = 12;  // shots per launch of rtmb_migrate_batch (rtmb_autotune_batch)
     uint64_t launches = 0;
     // storage forms (RTMB_FLAG_STORE_*): element type of d_w, one scale record per stored level

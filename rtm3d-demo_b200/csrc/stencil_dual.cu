@@ -45,17 +45,19 @@ bool dual_step_supported(const StepArgs &src, const StepArgs &rcv, int order) {
            dual_encoder() != nullptr;
 }
 
-cudaError_t launch_dual_step(const StepArgs &src, const StepArgs &rcv, int order, bool exact, cudaStream_t s) {
-    if (!dual_step_supported(src, rcv, order) || rcv.chunk <= 0) return cudaErrorInvalidValue;
-    using S = detail::DualShape<4>;
-    constexpr int TY = detail::kDTY;
+namespace {
+
+template <int DV>
+cudaError_t launch_dual_v(const StepArgs &src, const StepArgs &rcv, bool exact, cudaStream_t s) {
+    using S = detail::DualShape<4, DV>;
+    constexpr int TZ = S::TZ, TY = S::TY;
     auto enc = dual_encoder();
     detail::DualMaps m;
     std::memset(&m, 0, sizeof m);
     const bool ok = encode_f32(enc, &m.ps, src.P, rcv, S::SPITCH, S::SROWS) &&
                     encode_f32(enc, &m.pr, rcv.P, rcv, S::SPITCH, S::SROWS) &&
-                    encode_f32(enc, &m.pps, src.PP, rcv, kTZ, TY) && encode_f32(enc, &m.ppr, rcv.PP, rcv, kTZ, TY) &&
-                    encode_f32(enc, &m.v, rcv.V, rcv, kTZ, TY) && encode_f32(enc, &m.img, rcv.img, rcv, kTZ, TY);
+                    encode_f32(enc, &m.pps, src.PP, rcv, TZ, TY) && encode_f32(enc, &m.ppr, rcv.PP, rcv, TZ, TY) &&
+                    encode_f32(enc, &m.v, rcv.V, rcv, TZ, TY) && encode_f32(enc, &m.img, rcv.img, rcv, TZ, TY);
     if (!ok) return cudaErrorInvalidValue;
     detail::DualArgs d;
     d.s = src;
@@ -63,8 +65,20 @@ cudaError_t launch_dual_step(const StepArgs &src, const StepArgs &rcv, int order
     d.s.chunk = rcv.chunk;
     const int nxi = rcv.nxe - 8, nyi = rcv.nye - 8;
     if (nxi <= 0 || nyi <= 0 || rcv.nze <= 8) return cudaSuccess;
-    dim3 grid((rcv.nze + kTZ - 1) / kTZ, (nyi + TY - 1) / TY, (nxi + rcv.chunk - 1) / rcv.chunk);
-    return detail::launch_dual_h<4>(m, d, exact, rcv.taper_mode, grid, s);
+    dim3 grid((rcv.nze + TZ - 1) / TZ, (nyi + TY - 1) / TY, (nxi + rcv.chunk - 1) / rcv.chunk);
+    return detail::launch_dual_h<4>(m, d, exact, rcv.taper_mode, DV, grid, s);
+}
+
+}  // namespace
+
+// rcv.variant selects the dual step's launch variant (0: 64 x 8 tiles, 1: 32 x 16).
+cudaError_t launch_dual_step(const StepArgs &src, const StepArgs &rcv, int order, bool exact, cudaStream_t s) {
+    if (!dual_step_supported(src, rcv, order) || rcv.chunk <= 0) return cudaErrorInvalidValue;
+    switch (rcv.variant) {
+    case 0: return launch_dual_v<0>(src, rcv, exact, s);
+    case 1: return launch_dual_v<1>(src, rcv, exact, s);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 }  // namespace rtmb

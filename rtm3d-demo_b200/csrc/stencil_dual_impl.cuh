@@ -18,9 +18,25 @@
 namespace rtmb {
 namespace detail {
 
-constexpr int kDTY = 8;                        // tile rows (y)
+constexpr int kDTY = 8;                        // tile rows (y) of the default variant
 constexpr int kGThreads = (kTZ / kVZ) * kDTY;  // consumer threads per wavefield: 128
 constexpr int kDualThreads = 2 * kGThreads + 32;
+
+// Launch variants of the dual step (StepArgs::variant of the receiver arguments, picked by
+// rtmb_autotune_full): the in-plane tile, 128 consumer threads per wavefield in both.
+//   0: 64 (z) x 8 (y); 1: 32 x 16 (a 40 x 24 halo tile for 512 points instead of 72 x 16, and
+//   z tiles of 32 cells, which waste less of a row whose length is not a multiple of 64)
+template <int DV>
+struct DualTile;
+template <>
+struct DualTile<0> {
+    static constexpr int TZ = 64, TY = 8;
+};
+template <>
+struct DualTile<1> {
+    static constexpr int TZ = 32, TY = 16;
+};
+constexpr int kDualVariants = 2;
 
 struct DualMaps {
     CUtensorMap ps, pr;            // halo boxes of S and R
@@ -32,14 +48,16 @@ struct DualArgs {
     StepArgs r;  // the receiver step (receiver injection, image; no taper)
 };
 
-template <int H>
+template <int H, int DV = 0>
 struct DualShape {
+    static constexpr int TZ = DualTile<DV>::TZ, TY = DualTile<DV>::TY;
+    static_assert((TZ / kVZ) * TY == kGThreads, "128 consumer threads per wavefield");
     static constexpr int ZH = ((H + 3) / 4) * 4;
-    static constexpr int SROWS = kDTY + 2 * H;
-    static constexpr int SPITCH = kTZ + 2 * ZH;
+    static constexpr int SROWS = TY + 2 * H;
+    static constexpr int SPITCH = TZ + 2 * ZH;
     static constexpr int STAGE = SROWS * SPITCH;
     static constexpr int STRIDE = ((STAGE + 31) / 32) * 32;  // 128-byte slots
-    static constexpr int CORE = kTZ * kDTY;
+    static constexpr int CORE = TZ * TY;
     static constexpr int OFF_PPR = CORE * 4, OFF_V = 2 * CORE * 4, OFF_IMG = 3 * CORE * 4, CSLOT = 4 * CORE * 4;
     static constexpr int D = H + 4, R = 3, E = 3;
     static_assert(2 * H <= D, "warm-up planes must fit in the P rings");
@@ -50,12 +68,13 @@ struct DualShape {
 };
 
 // One wavefield's consumer warps.  ROLE 0: source (S), ROLE 1: receiver (R) with the image.
-template <int H, bool EXACT, int TAPER, int ROLE>
+template <int H, bool EXACT, int TAPER, int ROLE, int DV = 0>
 __device__ __forceinline__ void dual_consumer(const StepArgs &a, const StepArgs &coef, const float *pring,
                                               const unsigned char *cring, float *xring, uint64_t *pfull,
                                               uint64_t *pempty, uint64_t *cfull, uint64_t *cempty, uint64_t *xfull,
                                               uint64_t *xempty, int tid, int zt0, int yt0, int xc0, int n) {
-    using S = DualShape<H>;
+    using S = DualShape<H, DV>;
+    constexpr int kTZ = S::TZ;  // this variant's tile width (z)
     constexpr int ZH = S::ZH, SPITCH = S::SPITCH, STRIDE = S::STRIDE, D = S::D, R = S::R,
                   E = S::E, CSLOT = S::CSLOT, CORE = S::CORE;
     constexpr int NQ = 2 * H + 1;
@@ -282,10 +301,11 @@ drain:
     if (a.err) atomicOr(a.err, 2u);
 }
 
-template <int H, bool EXACT, int TAPER>
+template <int H, bool EXACT, int TAPER, int DV = 0>
 __global__ void __launch_bounds__(kDualThreads, 2)
     dual_step_kernel(const __grid_constant__ DualMaps maps, const __grid_constant__ DualArgs d) {
-    using S = DualShape<H>;
+    using S = DualShape<H, DV>;
+    constexpr int kTZ = S::TZ, kDTY = S::TY;
     constexpr int ZH = S::ZH, STAGE = S::STAGE, STRIDE = S::STRIDE, D = S::D, R = S::R, E = S::E, CSLOT = S::CSLOT;
     extern __shared__ __align__(128) unsigned char smem[];
     float *ring_s = reinterpret_cast<float *>(smem);
@@ -354,31 +374,37 @@ __global__ void __launch_bounds__(kDualThreads, 2)
         return;
     }
     if (tid < kGThreads)
-        dual_consumer<H, EXACT, TAPER, 0>(d.s, d.r, ring_s, cring, xring, pfull_s, pempty_s, cfull, cempty, xfull,
-                                          xempty, tid, zt0, yt0, xc0, n);
+        dual_consumer<H, EXACT, TAPER, 0, DV>(d.s, d.r, ring_s, cring, xring, pfull_s, pempty_s, cfull, cempty, xfull,
+                                              xempty, tid, zt0, yt0, xc0, n);
     else
-        dual_consumer<H, EXACT, TAPER, 1>(d.r, d.r, ring_r, cring, xring, pfull_r, pempty_r, cfull, cempty, xfull,
-                                          xempty, tid - kGThreads, zt0, yt0, xc0, n);
+        dual_consumer<H, EXACT, TAPER, 1, DV>(d.r, d.r, ring_r, cring, xring, pfull_r, pempty_r, cfull, cempty, xfull,
+                                              xempty, tid - kGThreads, zt0, yt0, xc0, n);
 }
 
 template <int H>
-cudaError_t launch_dual_h(const DualMaps &maps, const DualArgs &d, bool exact, int taper, dim3 grid, cudaStream_t s) {
-    static unsigned long long attr_done[4] = {};
+cudaError_t launch_dual_h(const DualMaps &maps, const DualArgs &d, bool exact, int taper, int dv, dim3 grid,
+                          cudaStream_t s) {
+    static unsigned long long attr_done[2 * kDualVariants] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    const int variant = exact ? 1 : 0;
-    auto run = [&](void (*kern)(DualMaps, DualArgs)) -> cudaError_t {
+    if (dv < 0 || dv >= kDualVariants) return cudaErrorInvalidValue;
+    const int variant = 2 * dv + (exact ? 1 : 0);
+    auto run = [&](void (*kern)(DualMaps, DualArgs), size_t smem) -> cudaError_t {
         const unsigned long long bit = 1ull << (dev & 63);
         if (!(attr_done[variant] & bit)) {
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DualShape<H>::SMEM);
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
             attr_done[variant] |= bit;
         }
-        kern<<<grid, kDualThreads, DualShape<H>::SMEM, s>>>(maps, d);
+        kern<<<grid, kDualThreads, smem, s>>>(maps, d);
         return cudaGetLastError();
     };
     if (taper != kTaperNone) return cudaErrorInvalidValue;
-    return exact ? run(dual_step_kernel<H, true, kTaperNone>) : run(dual_step_kernel<H, false, kTaperNone>);
+    if (dv == 1)
+        return exact ? run(dual_step_kernel<H, true, kTaperNone, 1>, DualShape<H, 1>::SMEM)
+                     : run(dual_step_kernel<H, false, kTaperNone, 1>, DualShape<H, 1>::SMEM);
+    return exact ? run(dual_step_kernel<H, true, kTaperNone>, DualShape<H>::SMEM)
+                 : run(dual_step_kernel<H, false, kTaperNone>, DualShape<H>::SMEM);
 }
 
 }  // namespace detail

@@ -169,7 +169,7 @@ def _ptr(t) -> int:
 class Tuning(C.Structure):
     """rtmb_tuning: the launch choices rtmb_autotune_full measured for a context."""
     _fields_ = [("variant", _u32), ("chunk", _u32), ("dual", _u32), ("dual_chunk", _u32),
-                ("ms_step", C.c_float), ("ms_backward", C.c_float)]
+                ("ms_step", C.c_float), ("ms_backward", C.c_float), ("dual_variant", _u32)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -371,7 +371,7 @@ class Context:
         return t.as_dict()
 
     def set_tuning(self, t: dict) -> None:
-        tt = Tuning(**{k: t[k] for k, _ in Tuning._fields_})
+        tt = Tuning(**{k: t.get(k, 0) for k, _ in Tuning._fields_})
         self._check(self.L.rtmb_set_tuning(self.h, C.byref(tt)))
 
     def set_chunk(self, chunk: int):
