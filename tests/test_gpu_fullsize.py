@@ -5,13 +5,15 @@ salt velocity, a 12 Hz Ricker at the surface centre and receivers every 2 cells 
 nt is cut to 600 steps to keep the test short (every step runs the same kernels as the 3000-step
 shot).  The record is this library's FP32 modeling pass of the same shot.
 
+* Determinism: the same shot migrated twice gives the same image bit for bit.
 * Linearity: the migration is linear in the record, and scaling every record value by a power of
   two scales every intermediate value of the exact form (each product and sum rounds the same way
-  scaled), so migrate(2 rec) == 2 migrate(rec) and migrate(rec / 4) == migrate(rec) / 4 -- exactly,
-  except where values fall into the subnormal range (below 1.2e-38: the numerical tail of the
-  stencil ahead of each wavefront), whose fixed spacing does not scale; a rounding changed there
-  can reach only values within a few hundred ULPs of that range.  The test requires every image
-  value above 1e-20 in magnitude to match bit for bit and the rest to agree within 1e-24.
+  scaled) -- except where values fall into the subnormal range (below 1.2e-38), whose fixed spacing
+  does not scale.  The record holds such values (receivers the direct wave has not reached yet
+  record the stencil's numerical tail), and their rounding differences spread through the
+  receiver wavefield at the level of single subnormal units, so the test requires
+  migrate(2 rec) = 2 migrate(rec) to rel-L2 1e-12 (FP32 rounding alone is 6e-8 per operation) and
+  reports the fraction of bit-identical image values.
 * The FMA form stays within the image tolerance of the FP32 path (rel-L2 1e-4) against the exact
   form, which is the reference CPU path's arithmetic.
 * The 16-bit increment storage form stays within rel-L2 1e-3 of the exact form.
@@ -55,16 +57,24 @@ def _migrate(p, v2, rec, flags, cuda):
     return img
 
 
-def test_exact_form_is_linear_in_the_record(cuda, shot):
+def test_exact_form_is_deterministic_and_linear_in_the_record(cuda, shot):
     p, v2, rec = shot
     img = _migrate(p, v2, rec, 0, cuda)
     assert float(img.abs().max()) > 0
+    again = _migrate(p, v2, rec, 0, cuda)
+    assert bool((again == img).all()), f"{int((again != img).sum())} cells differ between two identical runs"
     for scale in (2.0, 0.25):
-        got = _migrate(p, v2, rec * scale, 0, cuda)
-        want = img * scale
-        big = want.abs() > 1e-20
-        assert bool((got[big] == want[big]).all()), f"scale {scale}: {int((got[big] != want[big]).sum())} cells differ"
-        assert float((got - want).abs().max()) <= 1e-24
+        got = _migrate(p, v2, rec * scale, 0, cuda).double()
+        want = img.double() * scale
+        err = float(torch_norm(got - want) / torch_norm(want))
+        same = float((got == want).double().mean())
+        print(f"scale {scale}: rel-L2 {err:.3e}, {100 * same:.2f}% of the image bit-identical")
+        assert err <= 1e-12, err
+
+
+def torch_norm(t):
+    import torch
+    return torch.linalg.vector_norm(t)
 
 
 def test_fma_and_increment_forms_against_the_exact_form(cuda, shot):
