@@ -404,8 +404,9 @@ int rtmb_autotune_batch(rtmb_ctx *ctx, uint32_t nshots, const rtmb_shot *shots, 
  *     (64 x 8 or 32 x 16) and x-chunk, and the dual step against the source and receiver steps as
  *     two launches.
  * The fastest choices are kept for every later launch of the context (rtmb_tuning; results do not
- * change: every variant computes the same arithmetic per point).  rtmb_autotune is the same call
- * reporting only the chunk and the step time. */
+ * change: every variant computes the same arithmetic per point).  The measurement runs the step
+ * forms without taper (those of RBC migration); the chunk it picks serves every form of the
+ * context.  rtmb_autotune is the same call reporting only the chunk and the step time. */
 typedef struct rtmb_tuning {
     uint32_t variant;     /* launch variant of the single-wavefield step (see above) */
     uint32_t chunk;       /* x planes per CTA of that step */
