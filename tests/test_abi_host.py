@@ -83,6 +83,18 @@ def test_storage_flag_combinations_are_checked_before_any_device_work():
     assert create(4, 16, 8, rtmb.FLAG_STORE_F16) == rtmb.RTMB_EINVAL    # order 8 only
     assert create(8, 17, 8, rtmb.FLAG_STORE_BF16) == rtmb.RTMB_EINVAL   # nz + 2 blen = 33: not a multiple of 8
     assert b"multiple of 8" in lib.rtmb_last_error(None)
+    assert create(8, 16, 8, rtmb.FLAG_STORE_DIFF) == rtmb.RTMB_EINVAL   # increment storage needs a 16-bit type
+    assert b"STORE_DIFF" in lib.rtmb_last_error(None)
+
+
+def test_survey_shot_list_and_partition_follow_the_reference():
+    """rtmb.survey: the reference's source grid (x outer, y inner) dealt round-robin over ranks."""
+    from rtmb import survey
+    p = dict(nx=64, ny=64, nz=32, source_count_x=2, source_count_y=3, source_distance_x=20, source_distance_y=10,
+             source_start_x=5, source_start_y=7, source_depth_z=1)
+    assert survey.shot_positions(p) == [(5, 7, 1), (5, 17, 1), (5, 27, 1), (25, 7, 1), (25, 17, 1), (25, 27, 1)]
+    assert survey.rank_shots(6, 0, 4) == [0, 4] and survey.rank_shots(6, 3, 4) == [3]
+    assert list(survey.iter_rank_positions(survey.shot_positions(p), 1, 4)) == [(1, (5, 17, 1)), (5, (25, 27, 1))]
 
 
 @pytest.mark.parametrize("nt,dt,fmin,fmax", [(120, 0.001, 5.0, 40.0), (90, 0.0012, 2.0, 30.0), (3000, 0.001, 0.0, 30.0),
