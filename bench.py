@@ -288,6 +288,28 @@ def rel_l2_dev(a, ref, ref_norm: float) -> float:
     return float(torch.linalg.vector_norm(a.double() - ref)) / (ref_norm if ref_norm > 0 else 1.0)
 
 
+def time_ctx(ctxs, fn) -> float:
+    """Device milliseconds of the work fn() enqueues on the contexts ctxs: the contexts run on one
+    torch stream for the call and the two CUDA events are recorded on that stream (a context's own
+    stream is non-blocking, so events on torch's default stream would not bracket its work)."""
+    import torch
+    ctxs = ctxs if isinstance(ctxs, (list, tuple)) else [ctxs]
+    s = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    for c in ctxs:
+        c.set_stream(s.cuda_stream)
+    try:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        fn()
+        e1.record(s)
+        s.synchronize()
+    finally:
+        for c in ctxs:
+            c.set_stream(None)
+    return e0.elapsed_time(e1)
+
+
 def compare_forms(p: dict, v2: np.ndarray, v2m: np.ndarray | None, rec_full, dev, nt_cmp: int,
                   forms=FORMS, autotune: bool = True) -> dict:
     """Per-form device time and error against the FP64 GPU oracle on the same grid, over nt_cmp
@@ -328,13 +350,8 @@ def compare_forms(p: dict, v2: np.ndarray, v2m: np.ndarray | None, rec_full, dev
         c.load_v2dt2(v2, from_host=True)
         if autotune:
             c.autotune_full()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        c.migrate_shot(sx, sy, sz, rec, img)  # one full shot, timed (buffers are allocated on first use)
-        e1.record()
-        c.sync()
-        ms = e0.elapsed_time(e1)
+        # one full shot, timed (buffers are allocated on first use)
+        ms = time_ctx(c, lambda: c.migrate_shot(sx, sy, sz, rec, img))
         c.close()
         per_sweep = ms / sweeps_cmp
         r = {"ms_per_sweep": round(per_sweep, 4), "s_per_shot": round(per_sweep * sweeps_full / 1e3, 3),
@@ -413,12 +430,7 @@ def reference_gpu_bar(args, p: dict, v: np.ndarray, rec, value: float) -> dict:
     got = torch.zeros((1, 64, 64, mp["nt"]), device=dev)
     ctx.model_shot(mp["sx"], mp["sy"], mp["sz"], got)  # warm-up: graph capture
     ctx.sync()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    ctx.model_shot(mp["sx"], mp["sy"], mp["sz"], got)
-    e1.record()
-    ctx.sync()
-    ms = e0.elapsed_time(e1)
+    ms = time_ctx(ctx, lambda: ctx.model_shot(mp["sx"], mp["sy"], mp["sz"], got))
     ctx.close()
     g = got.cpu().numpy().reshape(-1).astype(np.float64)
     r = ref_rec.astype(np.float64)
@@ -672,13 +684,8 @@ def run_batch(args) -> dict:
     if not c4:
         ctx.migrate_batch(shots, stack)  # warm-up: graph capture and instantiation
         ctx.sync()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     l0 = ctx.launches
-    e0.record()
-    ctx.migrate_batch(shots, stack)
-    e1.record()
-    ctx.sync()
-    ms_batch = e0.elapsed_time(e1)
+    ms_batch = time_ctx(ctx, lambda: ctx.migrate_batch(shots, stack))
     launches_batch = ctx.launches - l0
     pts_all = sum((s.nx + 2 * blen) * (s.ny + 2 * blen) * (snz + 2 * blen) for s in shots)
     # one by one: the single-shot driver per aperture, images stacked in FP64 (the grid's diagonal
@@ -694,12 +701,7 @@ def run_batch(args) -> dict:
         if not c4:
             c.migrate_shot_acc64(s.sx, s.sy, s.sz, s.rec, acc)
             c.sync()
-        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a0.record()
-        c.migrate_shot_acc64(s.sx, s.sy, s.sz, s.rec, acc)
-        a1.record()
-        c.sync()
-        ms_single += a0.elapsed_time(a1)
+        ms_single += time_ctx(c, lambda: c.migrate_shot_acc64(s.sx, s.sy, s.sz, s.rec, acc))
         pts += int(np.prod(c.padded_shape))
         c.close()
         del acc
@@ -754,12 +756,7 @@ def run_model(args) -> dict:
         rec = torch.zeros((1, 64, 64, ntr), device=dev)
         ctx.model_shot(p["sx"], p["sy"], p["sz"], rec)  # warm-up: graph capture
         ctx.sync()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        ctx.model_shot(p["sx"], p["sy"], p["sz"], rec)
-        e1.record()
-        ctx.sync()
-        ms = e0.elapsed_time(e1)
+        ms = time_ctx(ctx, lambda: ctx.model_shot(p["sx"], p["sy"], p["sz"], rec))
         ctx.close()
         return ms, rec.cpu().numpy()
 
@@ -809,12 +806,7 @@ def run_fmig(args) -> dict:
     for _ in range(max(1, args.warmup - 2)):
         ctx.migrate_shot_fmig(*shot, rec, img, fmin, fmax, args.fmig_nwstep)
     ctx.sync()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    ctx.migrate_shot_fmig(*shot, rec, img, fmin, fmax, args.fmig_nwstep)
-    e1.record()
-    ctx.sync()
-    ms = e0.elapsed_time(e1)
+    ms = time_ctx(ctx, lambda: ctx.migrate_shot_fmig(*shot, rec, img, fmin, fmax, args.fmig_nwstep))
     # per-kernel split (a separate run: events around every launch)
     pctx = rtmb.Context(rtmb.Params.from_input(p, flags=flags, device=0))
     pctx.load_v2dt2(rtmb.v2dt2(ve, dt), from_host=True)
@@ -890,12 +882,7 @@ def run_closure(args) -> dict:
         rec = torch.zeros((1, n // 2, n // 2, nt), device=dev)
         c.model_shot(*shot, rec)  # warm-up
         c.sync()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        c.model_shot(*shot, rec)
-        e1.record()
-        c.sync()
-        ms = e0.elapsed_time(e1)
+        ms = time_ctx(c, lambda: c.model_shot(*shot, rec))
         c.close()
         return rec, ms
 
