@@ -139,7 +139,7 @@ __device__ __forceinline__ void dual_consumer(const StepArgs &a, const StepArgs 
 #pragma unroll
     for (int k = 0; k < H; ++k) release(&pempty[k]);
 
-#pragma unroll 1
+RTMB_UNROLL_PRAGMA(RTMB_PLANE_UNROLL)
     for (int i = 0; i < n; ++i, s_in = s_in + 1 == D ? (ph_in ^= 1, 0) : s_in + 1, s_mid = s_mid + 1 == D ? 0 : s_mid + 1,
                            s_core = s_core + 1 == R ? (ph_core ^= 1, 0) : s_core + 1,
                            s_x = s_x + 1 == E ? (ph_x ^= 1, 0) : s_x + 1) {

@@ -31,6 +31,15 @@
 
 #include "stencil_common.cuh"
 
+// Unroll factor of the plane loops of the TMA and dual step kernels (compile-time tuning: the
+// x register queue shifts by one plane per iteration, and an unrolled body lets the compiler
+// rename instead of move part of it).
+#ifndef RTMB_PLANE_UNROLL
+#define RTMB_PLANE_UNROLL 1
+#endif
+#define RTMB_DO_PRAGMA(x) _Pragma(#x)
+#define RTMB_UNROLL_PRAGMA(n) RTMB_DO_PRAGMA(unroll n)
+
 namespace rtmb {
 namespace detail {
 
@@ -538,7 +547,7 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
 #pragma unroll
     for (int k = 0; k < H; ++k) release_p(k);  // planes 0 .. H-1 were only needed for the queue
 
-#pragma unroll 1
+RTMB_UNROLL_PRAGMA(RTMB_PLANE_UNROLL)
     for (int i = 0; i < n; ++i, s_in = s_in + 1 == D ? (ph_in ^= 1, 0) : s_in + 1, s_mid = s_mid + 1 == D ? 0 : s_mid + 1,
                            s_core = s_core + 1 == R ? (ph_core ^= 1, 0) : s_core + 1) {
         {
