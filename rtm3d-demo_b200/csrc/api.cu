@@ -1567,7 +1567,7 @@ int rtmb_autotune_full(rtmb_ctx *ctx, rtmb_tuning *out) {
                          p.nx > 1 && p.boundary == RTMB_BC_RBC;
     float best_dual = 1e30f;
     int best_dc = ctx->dual_chunk, best_dv = ctx->dual_variant;
-    for (int dv = 0; dv < 2 && dual_ok && !rc; ++dv) {
+    for (int dv = 0; dv < rtmb::kDualVariants && dual_ok && !rc; ++dv) {
         for (int c : cand) {
             if (rc || c > nxi) break;
             rtmb::StepArgs src = args(false), rcv = args(true);
@@ -1602,7 +1602,7 @@ int rtmb_autotune_full(rtmb_ctx *ctx, rtmb_tuning *out) {
 
 int rtmb_set_tuning(rtmb_ctx *ctx, const rtmb_tuning *t) {
     if (!ctx || !t || !t->chunk || !t->dual_chunk || t->variant >= (uint32_t)rtmb::kStepVariants ||
-        t->dual_variant >= 2u)
+        t->dual_variant >= (uint32_t)rtmb::kDualVariants)
         return fail(ctx, RTMB_EINVAL, "rtmb_set_tuning: bad tuning");
     ctx->variant = (int)t->variant;
     ctx->dual_variant = (int)t->dual_variant;

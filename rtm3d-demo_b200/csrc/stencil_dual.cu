@@ -71,12 +71,15 @@ cudaError_t launch_dual_v(const StepArgs &src, const StepArgs &rcv, bool exact, 
 
 }  // namespace
 
-// rcv.variant selects the dual step's launch variant (0: 64 x 8 tiles, 1: 32 x 16).
+// rcv.variant selects the dual step's launch variant (0: 64 x 8 tiles, 1: 32 x 16, 2 and 3: 32 x 16
+// with deeper rings).
 cudaError_t launch_dual_step(const StepArgs &src, const StepArgs &rcv, int order, bool exact, cudaStream_t s) {
     if (!dual_step_supported(src, rcv, order) || rcv.chunk <= 0) return cudaErrorInvalidValue;
     switch (rcv.variant) {
     case 0: return launch_dual_v<0>(src, rcv, exact, s);
     case 1: return launch_dual_v<1>(src, rcv, exact, s);
+    case 2: return launch_dual_v<2>(src, rcv, exact, s);
+    case 3: return launch_dual_v<3>(src, rcv, exact, s);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -23,20 +23,31 @@ constexpr int kGThreads = (kTZ / kVZ) * kDTY;  // consumer threads per wavefield
 constexpr int kDualThreads = 2 * kGThreads + 32;
 
 // Launch variants of the dual step (StepArgs::variant of the receiver arguments, picked by
-// rtmb_autotune_full): the in-plane tile, 128 consumer threads per wavefield in both.
+// rtmb_autotune_full): the in-plane tile, 128 consumer threads per wavefield in all, and the ring
+// depths (DX: P slots beyond H; R: core slots; E: exchange slots).
 //   0: 64 (z) x 8 (y); 1: 32 x 16 (a 40 x 24 halo tile for 512 points instead of 72 x 16, and
-//   z tiles of 32 cells, which waste less of a row whose length is not a multiple of 64)
+//   z tiles of 32 cells, which waste less of a row whose length is not a multiple of 64);
+//   2: 32 x 16 with P rings two planes deeper and a fourth exchange slot; 3: 32 x 16 with P rings
+//   one plane deeper, a fourth core slot and a fourth exchange slot (2 and 3: 108 KB of shared
+//   memory, still two CTAs per SM)
 template <int DV>
 struct DualTile;
 template <>
 struct DualTile<0> {
-    static constexpr int TZ = 64, TY = 8;
+    static constexpr int TZ = 64, TY = 8, DX = 4, R = 3, E = 3;
 };
 template <>
 struct DualTile<1> {
-    static constexpr int TZ = 32, TY = 16;
+    static constexpr int TZ = 32, TY = 16, DX = 4, R = 3, E = 3;
 };
-constexpr int kDualVariants = 2;
+template <>
+struct DualTile<2> {
+    static constexpr int TZ = 32, TY = 16, DX = 6, R = 3, E = 4;
+};
+template <>
+struct DualTile<3> {
+    static constexpr int TZ = 32, TY = 16, DX = 5, R = 4, E = 4;
+};
 
 struct DualMaps {
     CUtensorMap ps, pr;            // halo boxes of S and R
@@ -59,12 +70,13 @@ struct DualShape {
     static constexpr int STRIDE = ((STAGE + 31) / 32) * 32;  // 128-byte slots
     static constexpr int CORE = TZ * TY;
     static constexpr int OFF_PPR = CORE * 4, OFF_V = 2 * CORE * 4, OFF_IMG = 3 * CORE * 4, CSLOT = 4 * CORE * 4;
-    static constexpr int D = H + 4, R = 3, E = 3;
+    static constexpr int D = H + DualTile<DV>::DX, R = DualTile<DV>::R, E = DualTile<DV>::E;
     static_assert(2 * H <= D, "warm-up planes must fit in the P rings");
     static constexpr size_t RING_BYTES = (size_t)D * STRIDE * 4;
     static constexpr size_t XOFF = 2 * RING_BYTES + (size_t)R * CSLOT;  // exchange slots
     static constexpr size_t BOFF = XOFF + (size_t)E * CORE * 4;         // barriers
     static constexpr size_t SMEM = BOFF + (size_t)(4 * D + 2 * R + 2 * E) * sizeof(uint64_t);
+    static_assert(SMEM <= 113 * 1024, "two CTAs per SM");
 };
 
 // One wavefield's consumer warps.  ROLE 0: source (S), ROLE 1: receiver (R) with the image.
@@ -139,7 +151,7 @@ __device__ __forceinline__ void dual_consumer(const StepArgs &a, const StepArgs 
 #pragma unroll
     for (int k = 0; k < H; ++k) release(&pempty[k]);
 
-RTMB_UNROLL_PRAGMA(RTMB_PLANE_UNROLL)
+RTMB_UNROLL_PRAGMA(RTMB_DUAL_UNROLL)
     for (int i = 0; i < n; ++i, s_in = s_in + 1 == D ? (ph_in ^= 1, 0) : s_in + 1, s_mid = s_mid + 1 == D ? 0 : s_mid + 1,
                            s_core = s_core + 1 == R ? (ph_core ^= 1, 0) : s_core + 1,
                            s_x = s_x + 1 == E ? (ph_x ^= 1, 0) : s_x + 1) {
@@ -400,11 +412,20 @@ cudaError_t launch_dual_h(const DualMaps &maps, const DualArgs &d, bool exact, i
         return cudaGetLastError();
     };
     if (taper != kTaperNone) return cudaErrorInvalidValue;
-    if (dv == 1)
+    switch (dv) {
+    case 1:
         return exact ? run(dual_step_kernel<H, true, kTaperNone, 1>, DualShape<H, 1>::SMEM)
                      : run(dual_step_kernel<H, false, kTaperNone, 1>, DualShape<H, 1>::SMEM);
-    return exact ? run(dual_step_kernel<H, true, kTaperNone>, DualShape<H>::SMEM)
-                 : run(dual_step_kernel<H, false, kTaperNone>, DualShape<H>::SMEM);
+    case 2:
+        return exact ? run(dual_step_kernel<H, true, kTaperNone, 2>, DualShape<H, 2>::SMEM)
+                     : run(dual_step_kernel<H, false, kTaperNone, 2>, DualShape<H, 2>::SMEM);
+    case 3:
+        return exact ? run(dual_step_kernel<H, true, kTaperNone, 3>, DualShape<H, 3>::SMEM)
+                     : run(dual_step_kernel<H, false, kTaperNone, 3>, DualShape<H, 3>::SMEM);
+    default:
+        return exact ? run(dual_step_kernel<H, true, kTaperNone>, DualShape<H>::SMEM)
+                     : run(dual_step_kernel<H, false, kTaperNone>, DualShape<H>::SMEM);
+    }
 }
 
 }  // namespace detail

@@ -31,11 +31,16 @@
 
 #include "stencil_common.cuh"
 
-// Unroll factor of the plane loops of the TMA and dual step kernels (compile-time tuning: the
-// x register queue shifts by one plane per iteration, and an unrolled body lets the compiler
-// rename instead of move part of it).
+// Unroll factors of the plane loops of the single-wavefield TMA step kernel and of the dual step
+// kernel (compile-time tuning).  The x register queue shifts by one plane per iteration; an
+// unrolled body lets the compiler rename part of it instead of moving it.  Measured on a 592^3
+// shot: 3 took 4% off the exact and FP16 steps and 1.4% off the FMA forward step, but made the
+// dual step spill and run 8% slower, where 2 took 2% off.
 #ifndef RTMB_PLANE_UNROLL
-#define RTMB_PLANE_UNROLL 1
+#define RTMB_PLANE_UNROLL 3
+#endif
+#ifndef RTMB_DUAL_UNROLL
+#define RTMB_DUAL_UNROLL 2
 #endif
 #define RTMB_DO_PRAGMA(x) _Pragma(#x)
 #define RTMB_UNROLL_PRAGMA(n) RTMB_DO_PRAGMA(unroll n)
@@ -325,7 +330,7 @@ __device__ __forceinline__ void taper_tile(T *st, const float *tab, const StepAr
 // The body of one CTA: the tile (bx, by) of the (z, y) plane and x chunk bz of the volume that
 // (maps, a) describe; the stencil coefficients come from coef (for the compiler, a kernel
 // parameter at a fixed offset, so the FMAs take them straight from the constant bank).
-template <int H, bool EXACT, int TAPER, bool IMG, typename T, typename IT, bool DF = false, int V = 0>
+template <int H, bool EXACT, int TAPER, bool IMG, typename T, typename IT, bool DF = false, int V = 0, int UNR = 1>
 __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArgs &a, const StepArgs &coef, int bx,
                                               int by, int bz) {
     using S = TmaShape<H, IMG, T, IT, V>;
@@ -547,7 +552,7 @@ __device__ __forceinline__ void tma_step_body(const TmaMaps &maps, const StepArg
 #pragma unroll
     for (int k = 0; k < H; ++k) release_p(k);  // planes 0 .. H-1 were only needed for the queue
 
-RTMB_UNROLL_PRAGMA(RTMB_PLANE_UNROLL)
+RTMB_UNROLL_PRAGMA(UNR)
     for (int i = 0; i < n; ++i, s_in = s_in + 1 == D ? (ph_in ^= 1, 0) : s_in + 1, s_mid = s_mid + 1 == D ? 0 : s_mid + 1,
                            s_core = s_core + 1 == R ? (ph_core ^= 1, 0) : s_core + 1) {
         {
@@ -920,10 +925,19 @@ drain:
     if (a.err) atomicOr(a.err, 2u);
 }
 
+// Plane-loop unroll of a step kernel: RTMB_PLANE_UNROLL for order 8 without taper and without
+// increment storage (the forms it was measured on); the taper and increment forms and the batched
+// kernel, which spill registers when unrolled, keep the plain loop.
+template <int H, int TAPER, bool DF>
+struct StepUnroll {
+    static constexpr int value = (H == 4 && TAPER == kTaperNone && !DF) ? RTMB_PLANE_UNROLL : 1;
+};
+
 template <int H, bool EXACT, int TAPER, bool IMG, typename T = float, typename IT = float, bool DF = false, int V = 0>
 __global__ void __launch_bounds__(variant_threads<V>(), Variant<V>::MINB)
     tma_step_kernel(const __grid_constant__ TmaMaps maps, const __grid_constant__ StepArgs a) {
-    tma_step_body<H, EXACT, TAPER, IMG, T, IT, DF, V>(maps, a, a, blockIdx.x, blockIdx.y, blockIdx.z);
+    tma_step_body<H, EXACT, TAPER, IMG, T, IT, DF, V, StepUnroll<H, TAPER, DF>::value>(maps, a, a, blockIdx.x,
+                                                                                       blockIdx.y, blockIdx.z);
 }
 
 // Several volumes in one launch (the batched multi-shot drivers): shot s owns the linear blocks

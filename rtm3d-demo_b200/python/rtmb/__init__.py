@@ -12,7 +12,9 @@ import os
 import subprocess
 
 PKG_ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), "..", ".."))
-LIB_PATH = os.path.join(PKG_ROOT, "lib", "librtm3d_b200.so")
+# the in-tree build; RTMB_LIB names another build of the same library (for example one made with
+# other compile-time tuning: make -C rtm3d-demo_b200 NVCC="nvcc -DRTMB_PLANE_UNROLL=1" LIB=...)
+LIB_PATH = os.environ.get("RTMB_LIB") or os.path.join(PKG_ROOT, "lib", "librtm3d_b200.so")
 BIN_PATH = os.path.join(PKG_ROOT, "bin", "rtm3d_b200")
 
 RTMB_OK, RTMB_EINVAL, RTMB_ENOMEM, RTMB_ECUDA, RTMB_ENAN, RTMB_ETIMEOUT, RTMB_EIO = range(7)
