@@ -112,6 +112,13 @@ def measured_hbm_gbs() -> tuple[float, str]:
         return HBM_FALLBACK_GBS, "fallback"
 
 
+def dual_kernel_name(tuning) -> str:
+    """Kernel of the dual backward step: variants 4-7 are the merged form (every thread steps both
+    wavefields), 0-3 the split form; 5 is the default."""
+    dv = 5 if not tuning else int(tuning.get("dual_variant", 5))
+    return "dual_merged_kernel" if dv >= 4 else "dual_step_kernel"
+
+
 def ncu_traffic_per_point(kind: str):
     """DRAM bytes per grid point of one launch, from the committed ncu summary (profiles/)."""
     path = os.path.join(ROOT, "profiles", "step_kernels_ncu.md")
@@ -573,7 +580,7 @@ def run_b200(args, rank: int, world: int, local_rank: int) -> dict | None:
         "e2e": {"value": round(e2e_value, 3), "unit": "Gpt/s",
                 "h2d_bytes_per_step": int(np.prod(rec_shape) * 4), "d2h_bytes_per_step": int(np.prod(shape) * 4)},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": ("dual_step_kernel" if cat == "backward_dual" else "tma_step_kernel") +
+        "roofline": {"bound": "hbm", "kernel": (dual_kernel_name(tuning) if cat == "backward_dual" else "tma_step_kernel") +
                      f" ({cat})", "achieved": round(achieved, 1),
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "traffic": (round(tpp * n_points(p)) if tpp else None),

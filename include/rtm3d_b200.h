@@ -403,7 +403,9 @@ int rtmb_autotune_batch(rtmb_ctx *ctx, uint32_t nshots, const rtmb_shot *shots, 
  *   - where the dual-wavefield backward step applies (FP32 FMA RBC migration, order 8): its launch
  *     variant (0: 64 x 8 tiles, 1: 32 x 16, 2: 32 x 16 with two more P-ring slots and a fourth
  *     exchange slot, 3: 32 x 16 with one more P-ring slot, a fourth core slot and a fourth exchange
- *     slot) and x-chunk, and the dual step against the source and receiver steps as two launches.
+ *     slot; 4 to 7: 64 x 8, 32 x 16, 64 x 16 and 32 x 32 with every thread stepping both
+ *     wavefields) and x-chunk, and the dual step against the source and receiver steps as two
+ *     launches.
  * The fastest choices are kept for every later launch of the context (rtmb_tuning; results do not
  * change: every variant computes the same arithmetic per point).  The measurement runs the step
  * forms without taper (those of RBC migration); the chunk it picks serves every form of the
@@ -415,7 +417,7 @@ typedef struct rtmb_tuning {
     uint32_t dual_chunk;  /* x planes per CTA of the dual step */
     float ms_step;        /* forward step (ms) with the chosen variant and chunk */
     float ms_backward;    /* one backward time step (ms): the dual launch, or source + receiver steps */
-    uint32_t dual_variant;  /* launch variant of the dual step (0 .. 3, see above) */
+    uint32_t dual_variant;  /* launch variant of the dual step (0 .. 7, see above) */
 } rtmb_tuning;
 int rtmb_autotune_full(rtmb_ctx *ctx, rtmb_tuning *out);
 /* Applies a tuning (for example one measured earlier on the same geometry). */

@@ -399,8 +399,9 @@ void rtmb::driver::init_geometry(rtmb_ctx *ctx) {
     const int nxi = ctx->nxe - 2 * ctx->h, nyi = ctx->nye - 2 * ctx->h;
     const int tiles = ((ctx->nze + rtmb::kTZ - 1) / rtmb::kTZ) * ((nyi + rtmb::kTY - 1) / rtmb::kTY);
     ctx->chunk = pick_chunk(nxi > 0 ? nxi : 1, tiles > 0 ? tiles : 1);
-    const int tiles8 = ((ctx->nze + rtmb::kTZ - 1) / rtmb::kTZ) * ((nyi + 7) / 8);  // the dual step's 64 x 8 tiles
-    ctx->dual_chunk = pick_chunk(nxi > 0 ? nxi : 1, tiles8 > 0 ? tiles8 : 1);
+    // the default dual step (variant 5): 32 x 16 tiles, two CTAs per SM like the 64 x 8 split form
+    const int tiles_dual = ((ctx->nze + 31) / 32) * ((nyi + 15) / 16);
+    ctx->dual_chunk = pick_chunk(nxi > 0 ? nxi : 1, tiles_dual > 0 ? tiles_dual : 1);
     rtmb_stencil_coefs(p.stencil_order, p.dx, p.dy, p.dz, ctx->coefs);
 }
 

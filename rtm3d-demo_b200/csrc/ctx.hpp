@@ -26,10 +26,10 @@ struct rtmb_ctx {
     float *d_upb = nullptr;      // [nt][nxe][nye][h] (HBC)
     float *d_rec = nullptr, *d_img = nullptr;  // staging for the host-buffer forms
     int chunk = 0;
-    int dual_chunk = 0;  // x planes per CTA of the dual-wavefield backward step (64 x 8 tiles)
+    int dual_chunk = 0;  // x planes per CTA of the dual-wavefield backward step
     int variant = 0;     // launch variant of the TMA step kernel (rtmb_autotune_full)
     int use_dual = -1;   // -1: the default rule; 0 / 1: the autotuner's choice
-    int dual_variant = 0;  // launch variant (tile) of the dual backward step
+    int dual_variant = 5;  // launch variant of the dual backward step (5: merged form, 32 x 16 tiles)
     int batch_group = 12;  // shots per launch of rtmb_migrate_batch (rtmb_autotune_batch)
     uint64_t launches = 0;
     // storage forms (RTMB_FLAG_STORE_*): element type of d_w, one scale record per stored level

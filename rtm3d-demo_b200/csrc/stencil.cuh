@@ -116,7 +116,7 @@ struct StepArgs {
 void variant_tile(int variant, int *tz, int *ty);
 constexpr int kStepVariants = 4;
 // launch variants of the dual backward step (in-plane tile and ring depths, StepArgs::variant)
-constexpr int kDualVariants = 4;
+constexpr int kDualVariants = 8;
 // Shots per launch of the batched step kernel (their arguments travel as kernel parameters).
 constexpr int kMaxBatchShots = 24;
 

@@ -72,7 +72,7 @@ cudaError_t launch_dual_v(const StepArgs &src, const StepArgs &rcv, bool exact, 
 }  // namespace
 
 // rcv.variant selects the dual step's launch variant (0: 64 x 8 tiles, 1: 32 x 16, 2 and 3: 32 x 16
-// with deeper rings).
+// with deeper rings, 4 to 7: the merged form on 64 x 8, 32 x 16, 64 x 16 and 32 x 32 tiles).
 cudaError_t launch_dual_step(const StepArgs &src, const StepArgs &rcv, int order, bool exact, cudaStream_t s) {
     if (!dual_step_supported(src, rcv, order) || rcv.chunk <= 0) return cudaErrorInvalidValue;
     switch (rcv.variant) {
@@ -80,6 +80,10 @@ cudaError_t launch_dual_step(const StepArgs &src, const StepArgs &rcv, int order
     case 1: return launch_dual_v<1>(src, rcv, exact, s);
     case 2: return launch_dual_v<2>(src, rcv, exact, s);
     case 3: return launch_dual_v<3>(src, rcv, exact, s);
+    case 4: return launch_dual_v<4>(src, rcv, exact, s);
+    case 5: return launch_dual_v<5>(src, rcv, exact, s);
+    case 6: return launch_dual_v<6>(src, rcv, exact, s);
+    case 7: return launch_dual_v<7>(src, rcv, exact, s);
     default: return cudaErrorInvalidValue;
     }
 }
