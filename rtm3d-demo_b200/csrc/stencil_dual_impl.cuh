@@ -496,18 +496,6 @@ __device__ __forceinline__ void dual_lap(const float *s, const float4 *q, int ty
     }
 }
 
-// the new level of one point (the single-wavefield kernel's two arithmetic forms)
-template <bool EXACT>
-__device__ __forceinline__ float dual_update(float v, float lap, float p, float pp) {
-    if (EXACT) {
-        const float two_p = 2.f * p;
-        const float d = two_p - pp;
-        const float vl = v * lap;
-        return d + vl;
-    }
-    return fmaf(v, lap, 2.f * p - pp);
-}
-
 template <int H, bool EXACT, int DV>
 __device__ __forceinline__ void dual_merged_consumer(const StepArgs &as, const StepArgs &a, const float *ring_s,
                                                      const float *ring_r, const unsigned char *cring, uint64_t *pfull,
@@ -618,8 +606,8 @@ RTMB_UNROLL_PRAGMA(RTMB_MERGED_UNROLL)
 #pragma unroll
             for (int e = 0; e < kVZ; ++e) {
                 const bool v = (vmask >> e) & 1u;
-                const float ns = dual_update<EXACT>(get(vv, e), lap_s[e], get(qcs, e), get(pps, e));
-                float nr = dual_update<EXACT>(get(vv, e), lap_r[e], get(qcr, e), get(ppr, e));
+                const float ns = step_update<EXACT>(get(vv, e), lap_s[e], get(qcs, e), get(pps, e));
+                float nr = step_update<EXACT>(get(vv, e), lap_r[e], get(qcr, e), get(ppr, e));
                 if (e == rec_e && rec_p) nr = a.rec_mode == kRecOverwrite ? rec_v : nr + rec_v;
                 const float os = v ? ns : get(pps, e);
                 const float orr = v ? nr : get(ppr, e);

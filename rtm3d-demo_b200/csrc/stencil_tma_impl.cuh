@@ -110,6 +110,20 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
 
 __device__ __forceinline__ float4 ld_f4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 
+// The new level of one point in the two arithmetic forms of the FP32 step: exact (every product and
+// sum rounded on its own, the reference CPU order) or one FMA.  Used by the kernels that restate the
+// step body (the merged dual step, the two-row step).
+template <bool EXACT>
+__device__ __forceinline__ float step_update(float v, float lap, float p, float pp) {
+    if (EXACT) {
+        const float two_p = 2.f * p;
+        const float d = two_p - pp;
+        const float vl = v * lap;
+        return d + vl;
+    }
+    return fmaf(v, lap, 2.f * p - pp);
+}
+
 // Barrier 1 over the NT consumer threads only (the producer warp never joins it).
 template <int NT>
 __device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory"); }
