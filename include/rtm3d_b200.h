@@ -398,10 +398,8 @@ int rtmb_autotune_batch(rtmb_ctx *ctx, uint32_t nshots, const rtmb_shot *shots, 
  * launches per candidate):
  *   - the single-wavefield step (forward form plus imaging form) for every launch variant -- the
  *     in-plane tile (0: 64 z x 16 y, 1: 32 x 32, 2: 64 x 8 at three CTAs per SM, 3: 64 x 16 with
- *     shallower load rings, 4: 64 x 16 with two y rows per thread, for the steps without image,
- *     receivers or border save, the others running variant 3) -- and every x-chunk length (x planes
- *     per CTA, 8 .. 256).  Variants 1-4 exist for the FP32 forms without taper at stencil order 8;
- *     other forms tune the chunk only;
+ *     shallower load rings) -- and every x-chunk length (x planes per CTA, 8 .. 256).  Variants 1-3
+ *     exist for the FP32 forms without taper at stencil order 8; other forms tune the chunk only;
  *   - where the dual-wavefield backward step applies (FP32 FMA RBC migration, order 8): its launch
  *     variant (0: 64 x 8 tiles, 1: 32 x 16, 2: 32 x 16 with two more P-ring slots and a fourth
  *     exchange slot, 3: 32 x 16 with one more P-ring slot, a fourth core slot and a fourth exchange

@@ -9,7 +9,6 @@
 
 #include "stencil.cuh"
 #include "stencil_tma_impl.cuh"
-#include "stencil_rows_impl.cuh"
 
 namespace rtmb {
 namespace detail {
@@ -95,56 +94,11 @@ cudaError_t tma_dispatch_v(const StepArgs &a, bool exact, cudaStream_t s, bool *
     return detail::launch_tma_h<H>(maps, a, exact, a.taper_mode, a.img != nullptr, grid, s);
 }
 
-// Variant 4: the two-row kernel (stencil_rows_impl.cuh), for the steps it covers: FP32, order 8, no
-// taper, no image, no receivers, no upper-border save or taper side buffer (the forward and
-// backward-source steps of RBC migration).  Not used: *used stays false.
-cudaError_t rows_dispatch(const StepArgs &a, bool exact, cudaStream_t s, bool *used) {
-    using S = detail::RowsShape;
-    *used = false;
-    auto enc = tensor_map_encoder();
-    if (!enc) return cudaSuccess;
-    const int nxi = a.nxe - 2 * S::H, nyi = a.nye - 2 * S::H;
-    const dim3 grid((a.nze + S::TZ - 1) / S::TZ, (nyi + S::TY - 1) / S::TY, (nxi + a.chunk - 1) / a.chunk);
-    detail::TmaMaps maps;
-    std::memset(&maps, 0, sizeof maps);
-    if (!(encode(enc, &maps.p, a.P, a, S::SPITCH, S::SROWS) && encode(enc, &maps.pp, a.PP, a, S::TZ, S::TY) &&
-          encode(enc, &maps.v, a.V, a, S::TZ, S::TY)))
-        return cudaSuccess;
-    *used = true;
-    static unsigned long long attr_done[2] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    auto kern = exact ? detail::tma_rows_kernel<true> : detail::tma_rows_kernel<false>;
-    const unsigned long long bit = 1ull << (dev & 63);
-    if (!(attr_done[exact ? 1 : 0] & bit)) {
-        const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
-        if (e != cudaSuccess) return e;
-        attr_done[exact ? 1 : 0] |= bit;
-    }
-    kern<<<grid, detail::kRowsThreads, S::SMEM, s>>>(maps, a);
-    return cudaGetLastError();
-}
-
-bool rows_form(const StepArgs &a) {
-    return a.store == kStoreF32 && !a.img && !a.img64 && a.rec_mode == kRecNone && a.upb_mode == kUpbNone &&
-           !a.quirk_out && !a.diff && a.taper_mode == kTaperNone && !a.tw;
-}
-
 // The launch variants (tile shape, ring depths) serve the FP32 forms without taper at order 8; the
-// others run variant 0.  Variant 4 (two rows per thread) covers the forward-type steps; the other
-// steps of a context tuned to it run variant 3, the same tile with one row per thread.
+// others run variant 0.
 template <int H>
 cudaError_t tma_dispatch(const StepArgs &a, bool exact, cudaStream_t s, bool *used) {
-    int v = (H == 4 && a.taper_mode == kTaperNone && !a.tw) ? a.variant : 0;
-    if (v == 4) {
-        if (rows_form(a)) {
-            const cudaError_t e = rows_dispatch(a, exact, s, used);
-            if (*used || e != cudaSuccess) return e;
-        }
-        StepArgs b = a;  // the one-row kernel on the same tile
-        b.variant = 3;
-        return tma_dispatch_v<H, 3>(b, exact, s, used);
-    }
+    const int v = (H == 4 && a.taper_mode == kTaperNone && !a.tw) ? a.variant : 0;
     switch (v) {
     case 0: return tma_dispatch_v<H, 0>(a, exact, s, used);
     case 1: return tma_dispatch_v<H, 1>(a, exact, s, used);
@@ -204,7 +158,6 @@ void variant_tile(int variant, int *tz, int *ty) {
     case 1: *tz = detail::Variant<1>::TZ; *ty = detail::Variant<1>::TY; break;
     case 2: *tz = detail::Variant<2>::TZ; *ty = detail::Variant<2>::TY; break;
     case 3: *tz = detail::Variant<3>::TZ; *ty = detail::Variant<3>::TY; break;
-    case 4: *tz = detail::RowsShape::TZ; *ty = detail::RowsShape::TY; break;
     default: *tz = detail::Variant<0>::TZ; *ty = detail::Variant<0>::TY; break;
     }
 }

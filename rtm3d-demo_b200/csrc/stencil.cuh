@@ -114,7 +114,7 @@ struct StepArgs {
 
 // In-plane tile (z, y) of a launch variant of the TMA step kernel (stencil_tma_impl.cuh: Variant).
 void variant_tile(int variant, int *tz, int *ty);
-constexpr int kStepVariants = 5;
+constexpr int kStepVariants = 4;
 // launch variants of the dual backward step (in-plane tile and ring depths, StepArgs::variant)
 constexpr int kDualVariants = 8;
 // Shots per launch of the batched step kernel (their arguments travel as kernel parameters).

@@ -111,8 +111,8 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
 __device__ __forceinline__ float4 ld_f4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 
 // The new level of one point in the two arithmetic forms of the FP32 step: exact (every product and
-// sum rounded on its own, the reference CPU order) or one FMA.  Used by the kernels that restate the
-// step body (the merged dual step, the two-row step).
+// sum rounded on its own, the reference CPU order) or one FMA.  Used by the merged dual step, which
+// restates the step body for two wavefields.
 template <bool EXACT>
 __device__ __forceinline__ float step_update(float v, float lap, float p, float pp) {
     if (EXACT) {
