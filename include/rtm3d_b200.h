@@ -90,8 +90,8 @@ typedef enum rtmb_boundary {
  * as ONE launch (both wavefields and the image in one pass over the grid: 36 instead of 44 bytes per
  * point) when stencil_order is 8 and rows are 16-byte aligned; same results as two launches (no
  * reference counterpart: the reference runs them as separate operators).  This flag keeps the two
- * launches.  The exact form and HBC migration (whose receiver steps taper the upper border) keep
- * two launches: there one launch gained nothing or lost. */
+ * launches.  HBC migration (whose receiver steps taper the upper border) keeps two launches: there
+ * one launch lost. */
 #define RTMB_FLAG_NO_DUAL       0x200u
 /* Modeling (every face tapered) and HBC migration (the upper border tapered) keep the wavefields
  * tapered in HBM between time steps: each step stores T(u) of its new level instead of u, so the
@@ -400,7 +400,7 @@ int rtmb_autotune_batch(rtmb_ctx *ctx, uint32_t nshots, const rtmb_shot *shots, 
  *     in-plane tile (0: 64 z x 16 y, 1: 32 x 32, 2: 64 x 8 at three CTAs per SM, 3: 64 x 16 with
  *     shallower load rings) -- and every x-chunk length (x planes per CTA, 8 .. 256).  Variants 1-3
  *     exist for the FP32 forms without taper at stencil order 8; other forms tune the chunk only;
- *   - where the dual-wavefield backward step applies (FP32 FMA RBC migration, order 8): its launch
+ *   - where the dual-wavefield backward step applies (FP32 RBC migration, order 8): its launch
  *     variant (0: 64 x 8 tiles, 1: 32 x 16, 2: 32 x 16 with two more P-ring slots and a fourth
  *     exchange slot, 3: 32 x 16 with one more P-ring slot, a fourth core slot and a fourth exchange
  *     slot; 4 to 7: 64 x 8, 32 x 16, 64 x 16 and 32 x 32 with every thread stepping both

@@ -902,10 +902,11 @@ int migrate_impl(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const flo
     rcv.store = ctx->store;
     rcv.inj_dev = st ? ctx->d_inj : nullptr;
     const int rmode = (p.flags & RTMB_FLAG_RCV_ADD) ? rtmb::kRecAdd : rtmb::kRecOverwrite;
-    // FP32 FMA form: the source and receiver steps of one time step in one launch (RBC: with the
-    // upper taper of HBC the two launches measured faster, 1.83 against 2.99 ms at 592^3)
-    const bool dual = !st && !exact(ctx) && p.stencil_order == 8 && tma_ok(ctx) && !(p.flags & RTMB_FLAG_NO_DUAL) &&
-                      p.nx > 1 && !hbc && ctx->use_dual != 0;
+    // FP32 forms: the source and receiver steps of one time step in one launch unless the autotuner
+    // measured two launches faster (RBC: with the upper taper of HBC the two launches measured
+    // faster, 1.83 against 2.99 ms at 592^3)
+    const bool dual = !st && p.stencil_order == 8 && tma_ok(ctx) && !(p.flags & RTMB_FLAG_NO_DUAL) && p.nx > 1 &&
+                      !hbc && ctx->use_dual != 0;
     for (int it = (int)p.nt - 1; it >= 0; --it) {
         if (dual && it < (int)p.nt - 2) {
             src.P = s_cur; src.PP = s_prev; src.it = it;
@@ -1564,7 +1565,7 @@ int rtmb_autotune_full(rtmb_ctx *ctx, rtmb_tuning *out) {
             return e != cudaSuccess ? e : rtmb::launch_step(ai, order, exact(ctx), ctx->stream, tma_ok(ctx));
         }, &two);
     }
-    const bool dual_ok = !rc && !st && !exact(ctx) && order == 8 && tma_ok(ctx) && !(p.flags & RTMB_FLAG_NO_DUAL) &&
+    const bool dual_ok = !rc && !st && order == 8 && tma_ok(ctx) && !(p.flags & RTMB_FLAG_NO_DUAL) &&
                          p.nx > 1 && p.boundary == RTMB_BC_RBC;
     float best_dual = 1e30f;
     int best_dc = ctx->dual_chunk, best_dv = ctx->dual_variant;
@@ -1578,7 +1579,7 @@ int rtmb_autotune_full(rtmb_ctx *ctx, rtmb_tuning *out) {
             rcv.variant = dv;
             if (!rtmb::dual_step_supported(src, rcv, order)) break;
             float t = 0.f;
-            if ((rc = time_launches(ctx, e0, e1, [&] { return rtmb::launch_dual_step(src, rcv, order, false, ctx->stream); },
+            if ((rc = time_launches(ctx, e0, e1, [&] { return rtmb::launch_dual_step(src, rcv, order, exact(ctx), ctx->stream); },
                                     &t)))
                 break;
             if (t < best_dual) { best_dual = t; best_dc = c; best_dv = dv; }

@@ -237,9 +237,9 @@ def test_autotune_picks_a_chunk_and_keeps_results(cuda, oracle):
 
 @pytest.mark.parametrize("bc", ["hbc", "rbc"])
 def test_dual_backward_step_matches_two_launches(cuda, oracle, bc):
-    """In the FMA form the RBC backward source and receiver steps run as one dual-wavefield launch
-    by default; it gives the two-launch result (RTMB_FLAG_NO_DUAL) bit for bit.  The exact form
-    and HBC migration keep two launches."""
+    """In both FP32 forms the RBC backward source and receiver steps run as one dual-wavefield launch
+    by default; it gives the two-launch result (RTMB_FLAG_NO_DUAL) bit for bit.  HBC migration keeps
+    two launches."""
     import torch
     case = CASES["mid"]
     p = oracle_params(case)
@@ -247,7 +247,7 @@ def test_dual_backward_step_matches_two_launches(cuda, oracle, bc):
                                                case["dt"]))
     v2 = oracle.v2dt2(oracle.extend_init_borders(layered_model(case), case["blen"], bc, seed=7), case["dt"])
     out = {}
-    for flags in (rtmb.FLAG_FAST_FMA, rtmb.FLAG_FAST_FMA | rtmb.FLAG_NO_DUAL, 0):
+    for flags in (rtmb.FLAG_FAST_FMA, rtmb.FLAG_FAST_FMA | rtmb.FLAG_NO_DUAL, 0, rtmb.FLAG_NO_DUAL):
         ctx = ctx_for(case, bc, flags)
         ctx.load_v2dt2(v2, from_host=True)
         img = torch.zeros(ctx.padded_shape, dtype=torch.float32, device=cuda)
@@ -255,6 +255,9 @@ def test_dual_backward_step_matches_two_launches(cuda, oracle, bc):
         ctx.migrate_shot(case["sx"], case["sy"], case["sz"], dev(rec, cuda), img)
         ctx.sync()
         out[flags] = (host(img), ctx.profile_read()["backward_dual"]["launches"])
-    fma, two, exact = out[rtmb.FLAG_FAST_FMA], out[rtmb.FLAG_FAST_FMA | rtmb.FLAG_NO_DUAL], out[0]
-    assert fma[1] == (case["nt"] - 2 if bc == "rbc" else 0) and two[1] == 0 and exact[1] == 0
+    fma, two, exact, exact_two = (out[rtmb.FLAG_FAST_FMA], out[rtmb.FLAG_FAST_FMA | rtmb.FLAG_NO_DUAL], out[0],
+                                  out[rtmb.FLAG_NO_DUAL])
+    n_dual = case["nt"] - 2 if bc == "rbc" else 0
+    assert fma[1] == n_dual and two[1] == 0 and exact[1] == n_dual and exact_two[1] == 0
     assert bitexact(fma[0], two[0])
+    assert bitexact(exact[0], exact_two[0])
