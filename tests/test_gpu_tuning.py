@@ -59,6 +59,38 @@ def test_every_launch_variant_gives_the_same_image(cuda, oracle, mid_inputs, for
                 assert bitexact(got, want), (variant, chunk, dual, dv)
 
 
+@pytest.fixture(scope="module")
+def golden_inputs(oracle):
+    case = CASES["golden"]
+    p = oracle_params(case)
+    rec, _ = oracle.model_shot(p, oracle.v2dt2(oracle.extend_init_borders(layered_model(case), case["blen"], "abc"),
+                                               case["dt"]))
+    v2 = oracle.v2dt2(oracle.extend_init_borders(layered_model(case), case["blen"], "rbc", seed=7), case["dt"])
+    return case, v2, rec
+
+
+@pytest.mark.parametrize("form", ["exact", "fma"])
+@pytest.mark.parametrize("rcv", ["overwrite", "add"])
+def test_launch_variants_on_partial_tiles(cuda, oracle, golden_inputs, form, rcv):
+    """The small case's padded grid (40 x 36 x 44, 28 computed y rows) leaves every tile shape of
+    both step kernels partly outside the grid in y and z.  Every launch variant, and every dual step
+    variant against the two launches (RTMB_FLAG_NO_DUAL), gives the same image bit for bit, with the
+    receivers overwriting the receiver wavefield (the reference's injection) or added to it
+    (RTMB_FLAG_RCV_ADD); the exact form with overwriting receivers is also the oracle's image."""
+    case, v2, rec = golden_inputs
+    flags = (0 if form == "exact" else rtmb.FLAG_FAST_FMA) | (rtmb.FLAG_RCV_ADD if rcv == "add" else 0)
+    want, _ = _migrate(cuda, case, v2, rec, flags | rtmb.FLAG_NO_DUAL)
+    if form == "exact" and rcv == "overwrite":
+        ref, rc = oracle.migrate(oracle_params(case), v2, rec, "rbc")
+        assert rc == 0 and bitexact(want, ref)
+    for variant in range(4):
+        for chunk in (8, 48):
+            for dual, dv in ((0, 0),) + tuple((1, dv) for dv in range(8)):
+                t = dict(variant=variant, chunk=chunk, dual=dual, dual_chunk=chunk, dual_variant=dv)
+                got, _ = _migrate(cuda, case, v2, rec, flags, tuning=t)
+                assert bitexact(got, want), (variant, chunk, dual, dv)
+
+
 def test_autotune_full_keeps_results(cuda, mid_inputs):
     case, v2, rec = mid_inputs
     want, _ = _migrate(cuda, case, v2, rec, rtmb.FLAG_FAST_FMA)
