@@ -119,6 +119,18 @@ def dual_kernel_name(tuning) -> str:
     return "dual_merged_kernel" if dv >= 4 else "dual_step_kernel"
 
 
+def dual_bytes_per_point(tuning, nt: int) -> float:
+    """Algorithmic bytes per grid point of a dual backward step, averaged over a shot's nt - 2 dual
+    launches: 36 (read S, S_prev, R, R_prev, v2dt2 and IMG, write S_new, R_new and IMG); the merged
+    form pairs its launches on the image, so the first of a pair moves 28 (no image) and the second
+    36, an odd last launch 36."""
+    n = max(nt - 2, 1)
+    if dual_kernel_name(tuning) != "dual_merged_kernel":
+        return 36.0
+    skip = n // 2 if n % 2 == 0 else (n - 1) // 2
+    return (28.0 * skip + 36.0 * (n - skip)) / n
+
+
 def ncu_traffic_per_point(kind: str):
     """DRAM bytes per grid point of one launch, from the committed ncu summary (profiles/)."""
     path = os.path.join(ROOT, "profiles", "step_kernels_ncu.md")
@@ -553,7 +565,8 @@ def run_b200(args, rank: int, world: int, local_rank: int) -> dict | None:
     # roofline of the dominant kernel (largest summed device time)
     peak, peak_kind = measured_hbm_gbs()
     cat = max(("forward", "backward_source", "backward_receiver", "backward_dual"), key=lambda k: prof[k]["ms"])
-    bpp = {"forward": 16, "backward_source": 16, "backward_receiver": 28, "backward_dual": 36}[cat]
+    bpp = {"forward": 16, "backward_source": 16, "backward_receiver": 28, "backward_dual": dual_bytes_per_point(
+        tuning, p["nt"])}[cat]
     per_launch_ms = prof[cat]["ms"] / max(prof[cat]["launches"], 1)
     bytes_launch = bpp * n_points(p)
     achieved = bytes_launch / (per_launch_ms * 1e-3) / 1e9

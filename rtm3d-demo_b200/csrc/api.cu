@@ -907,6 +907,21 @@ int migrate_impl(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const flo
     // faster, 1.83 against 2.99 ms at 592^3)
     const bool dual = !st && p.stencil_order == 8 && tma_ok(ctx) && !(p.flags & RTMB_FLAG_NO_DUAL) && p.nx > 1 &&
                       !hbc && ctx->use_dual != 0;
+    // the merged dual step pairs its launches on the image: the first of a pair leaves its product
+    // S_new R_new to the second, which adds both in the order two separate steps would (the image
+    // is read and written every other step).  Only where every dual step of the loop is a merged
+    // launch; an odd last step reads and writes the image itself.
+    bool dual_geometry_ok = false;  // the dual step's conditions hold for every step of the loop
+    if (dual && p.nt > 2) {
+        rtmb::StepArgs s0 = src, r0 = rcv;
+        s0.P = s_cur; s0.PP = s_prev;
+        r0.P = rP; r0.PP = rPP; r0.ps = nullptr;
+        set_receivers(r0, ctx, rmode, const_cast<float *>(rec), 0);
+        r0.chunk = ctx->dual_chunk;
+        r0.variant = ctx->dual_variant;
+        dual_geometry_ok = rtmb::dual_step_supported(s0, r0, (int)p.stencil_order);
+    }
+    const bool pair_img = dual && ctx->dual_variant >= 4 && dual_geometry_ok;
     for (int it = (int)p.nt - 1; it >= 0; --it) {
         if (dual && it < (int)p.nt - 2) {
             src.P = s_cur; src.PP = s_prev; src.it = it;
@@ -916,17 +931,22 @@ int migrate_impl(rtmb_ctx *ctx, uint32_t sx, uint32_t sy, uint32_t sz, const flo
             set_receivers(rcv, ctx, rmode, const_cast<float *>(rec), it);
             rcv.chunk = ctx->dual_chunk;
             rcv.variant = ctx->dual_variant;
+            const int j = (int)p.nt - 3 - it;  // index of this dual step, from 0
+            rcv.img_pair = !pair_img ? 0 : (j % 2 == 1 ? 2 : (it > 0 ? 1 : 0));
             if (rtmb::dual_step_supported(src, rcv, (int)p.stencil_order)) {
                 LAUNCH_CAT(RTMB_PROF_BACKWARD_DUAL,
                            rtmb::launch_dual_step(src, rcv, (int)p.stencil_order, exact(ctx), ctx->stream));
                 rcv.chunk = ctx->chunk;
                 rcv.variant = ctx->variant;
+                rcv.img_pair = 0;
                 std::swap(s_cur, s_prev);
                 std::swap(rP, rPP);
                 continue;
             }
+            if (pair_img) return fail(ctx, RTMB_EINVAL, "dual step no longer supported in a paired loop");
             rcv.chunk = ctx->chunk;
             rcv.variant = ctx->variant;
+            rcv.img_pair = 0;
         }
         if (it == (int)p.nt - 2) {
             s_cur = sP;

@@ -110,6 +110,11 @@ struct StepArgs {
     // launch variant of the TMA step kernel (tile shape and ring depths, 0 = default): taken by the
     // FP32 forms without taper at order 8, ignored elsewhere
     int variant;
+    // image pairing of the merged dual step (receiver arguments): 0 the image is read and written
+    // (img += S_new R_new); 1 this step's product is left to the next launch (no image traffic);
+    // 2 the previous step's product, S R of this step's input levels, is added first:
+    // img = (img + S R) + S_new R_new, the same FP32 sequence as two steps of mode 0
+    int img_pair;
 };
 
 // In-plane tile (z, y) of a launch variant of the TMA step kernel (stencil_tma_impl.cuh: Variant).

@@ -75,6 +75,7 @@ cudaError_t launch_dual_v(const StepArgs &src, const StepArgs &rcv, bool exact, 
 // with deeper rings, 4 to 7: the merged form on 64 x 8, 32 x 16, 64 x 16 and 32 x 32 tiles).
 cudaError_t launch_dual_step(const StepArgs &src, const StepArgs &rcv, int order, bool exact, cudaStream_t s) {
     if (!dual_step_supported(src, rcv, order) || rcv.chunk <= 0) return cudaErrorInvalidValue;
+    if (rcv.img_pair != 0 && (rcv.variant < 4 || rcv.img_pair > 2)) return cudaErrorInvalidValue;  // merged form only
     switch (rcv.variant) {
     case 0: return launch_dual_v<0>(src, rcv, exact, s);
     case 1: return launch_dual_v<1>(src, rcv, exact, s);

@@ -531,6 +531,7 @@ __device__ __forceinline__ void dual_merged_consumer(const StepArgs &as, const S
         }
     }
     const size_t row_off = (size_t)y * a.nze + z0;
+    const bool img_io = a.img_pair != 1;  // this launch reads and writes the image
     float *PPs = as.PP + row_off;
     float *PPr = a.PP + row_off;
     const int col = ZH + tz * kVZ;
@@ -598,7 +599,8 @@ RTMB_UNROLL_PRAGMA(RTMB_MERGED_UNROLL)
         const float4 pps = ld_f4(reinterpret_cast<const float *>(ct) + ccol);
         const float4 ppr = ld_f4(reinterpret_cast<const float *>(ct + S::OFF_PPR) + ccol);
         const float4 vv = ld_f4(reinterpret_cast<const float *>(ct + S::OFF_V) + ccol);
-        const float4 im4 = ld_f4(reinterpret_cast<const float *>(ct + S::OFF_IMG) + ccol);
+        float4 im4 = vv;
+        if (img_io) im4 = ld_f4(reinterpret_cast<const float *>(ct + S::OFF_IMG) + ccol);
         release(&cempty[s_core]);
         if (row_ok) {
             const float4 qcs = qs[H], qcr = qr[H];
@@ -618,11 +620,14 @@ RTMB_UNROLL_PRAGMA(RTMB_MERGED_UNROLL)
             }
             *reinterpret_cast<float4 *>(PPs + (size_t)x * plane) = outs;
             *reinterpret_cast<float4 *>(PPr + (size_t)x * plane) = outr;
-            if (imask) {
+            if (imask && img_io) {
                 float4 im;
+                const float4 pcs = qs[H], pcr = qr[H];  // this step's input levels: the previous step's output
 #pragma unroll
                 for (int e = 0; e < kVZ; ++e) {
-                    const float acc = get(im4, e) + get(outs, e) * get(outr, e);
+                    float acc = get(im4, e);
+                    if (a.img_pair == 2) acc = acc + get(pcs, e) * get(pcr, e);
+                    acc = acc + get(outs, e) * get(outr, e);
                     put(im, e, ((imask >> e) & 1u) ? acc : get(im4, e));
                 }
                 *reinterpret_cast<float4 *>(a.img + row_off + (size_t)x * plane) = im;
@@ -667,6 +672,7 @@ __global__ void __launch_bounds__((DualTile<DV>::TZ / kVZ) * DualTile<DV>::TY + 
     }
     __syncthreads();
 
+    const bool img_io = a.img_pair != 1;  // this launch reads and writes the image
     if (tid >= MT) {
         // producer: the S and R planes k onto one barrier, then the core tiles of output plane k - 2H
         if (tid != MT) return;
@@ -683,11 +689,11 @@ __global__ void __launch_bounds__((DualTile<DV>::TZ / kVZ) * DualTile<DV>::TY + 
                 const int i = k - 2 * H, cs = i % R;
                 if (i >= R && !(ok = mbar_wait_producer(&cempty[cs], ((i / R) + 1) & 1))) break;
                 unsigned char *dst = cring + cs * CSLOT;
-                mbar_expect_tx(&cfull[cs], CSLOT);
+                mbar_expect_tx(&cfull[cs], img_io ? CSLOT : S::OFF_IMG);
                 tma_load_3d(dst, &maps.pps, &cfull[cs], zt0, yt0, xc0 + i);
                 tma_load_3d(dst + S::OFF_PPR, &maps.ppr, &cfull[cs], zt0, yt0, xc0 + i);
                 tma_load_3d(dst + S::OFF_V, &maps.v, &cfull[cs], zt0, yt0, xc0 + i);
-                tma_load_3d(dst + S::OFF_IMG, &maps.img, &cfull[cs], zt0, yt0, xc0 + i);
+                if (img_io) tma_load_3d(dst + S::OFF_IMG, &maps.img, &cfull[cs], zt0, yt0, xc0 + i);
                 c_issued = i + 1;
             }
         }
