@@ -366,14 +366,20 @@ class Context:
         return int(c.value), float(ms.value)
 
     def autotune_full(self) -> dict:
-        """Picks the launch variant (tile shape, ring depths), the x-chunk lengths and the dual
-        backward step or two launches for this context; returns the rtmb_tuning fields."""
+        """Picks the launch variant (tile shape, ring depths), the x-chunk lengths, the dual backward
+        step's variant (split or merged form, tile, ring depths) and the dual step or two launches
+        for this context; returns the rtmb_tuning fields."""
         t = Tuning()
         self._check(self.L.rtmb_autotune_full(self.h, C.byref(t)))
         return t.as_dict()
 
+    # the library's own choice for a field the caller leaves out (dual_variant 5: the merged dual step)
+    TUNING_DEFAULTS = {"dual_variant": 5}
+
     def set_tuning(self, t: dict) -> None:
-        tt = Tuning(**{k: t.get(k, 0) for k, _ in Tuning._fields_})
+        """Applies rtmb_tuning fields (as autotune_full returns them); a missing field is 0, except
+        dual_variant, which keeps the library's default."""
+        tt = Tuning(**{k: t.get(k, self.TUNING_DEFAULTS.get(k, 0)) for k, _ in Tuning._fields_})
         self._check(self.L.rtmb_set_tuning(self.h, C.byref(tt)))
 
     def set_chunk(self, chunk: int):
