@@ -2,7 +2,8 @@
 // reconstructed source wavefield S and the back-propagated receiver wavefield R one step and adds
 // S_new * R_new to the image, which the separate launches do in two passes (the source step, then
 // the receiver step reading S_new back from HBM).  Per point it moves 36 bytes instead of 16 + 28:
-// v2dt2 is read once and S_new never leaves the chip for the image.
+// v2dt2 is read once and S_new never leaves the chip for the image.  The merged form can also pair
+// consecutive launches on the image (StepArgs::img_pair): 28 + 36 bytes per point for two steps.
 //
 // Same arithmetic per point as the single-wavefield kernel (stencil_tma_impl.cuh), so results are
 // bit-identical to the two launches, in both arithmetic forms.
